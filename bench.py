@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Throughput of the dense-stereo hot path on the full-HD configuration:
+1920x1080 rectified u8 pair, D = 256, Birchfield-Tomasi cost, 8-path SGM
+(P1 = 10, P2 = 120), WTA + left-right check (threshold 1).
+
+One step = one stereo frame through tdv_stereo_sgm.  Prints one JSON line.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm (default): `value` is frames/s with the pair already in HBM, timed
+per step with CUDA events on the launch stream, L2 flushed (256 MiB write)
+between steps; `e2e` is the same through the public API with the pair copied
+from pinned host memory and the disparity map copied back inside the timed
+region.  Under torchrun every rank processes its own frames (weak scaling, no
+collective on the data path); the time is the max over ranks.
+
+Reference arm (--impl reference): the reference's CPU path restated in C++
+(the oracle: BT cost + SemiGlobalCPU with its table and start-assign
+recurrence + WTACPU) on all host threads, each step a band of rows of the
+same frame sized so the run stays within a few minutes; rank 0 only.
+"""
+import argparse
+import datetime
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H, D = 1920, 1080, 256
+P1, P2, PATHS, LR = 10.0, 120.0, 8, 1
+METRIC = "1080p D=256 8-path SGM fps"
+UNIT = "frames/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--frames", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def config(extra=None):
+    c = {"workload": f"BT + SGM-{PATHS} + WTA + LR, {W}x{H}, D={D}", "width": W, "height": H,
+         "max_disp": D, "paths": PATHS, "p1": P1, "p2": P2, "lr_threshold": LR,
+         "l2": "flushed between timed steps (256 MiB write)",
+         "inputs": "seeded synthetic video frames (moving rectangles over a slanted plane)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for ln in fh:
+                parts = [x.strip() for x in ln.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        mx = max((float(r[2]) for r in rows if r[2].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------- CPU arms
+def cpu_reference_run(steps, warmup, budget_s=150.0):
+    """Times the oracle's restatement of the reference CPU path on bands of a
+    full-HD frame; returns (frames/s, description, threads)."""
+    import numpy as np
+
+    import oracle
+    from thundervision_b200 import synthetic
+    threads = os.cpu_count() or 1
+    L, R, _, _ = synthetic.VideoStream(seed=0).frame(0)
+    Lf, Rf = oracle.u8_to_f32(L), oracle.u8_to_f32(R)
+
+    def band(h):
+        t0 = time.perf_counter()
+        C = oracle.bt_cost(Lf[:h], Rf[:h], D, layout=oracle.LAYOUT_REF_WHD)
+        oracle.sgm(C, Lf[:h], P1, P2, paths=PATHS, table=oracle.TABLE_REF,
+                   semantics=oracle.SEM_REF_CPU, layout=oracle.LAYOUT_REF_WHD, threads=threads,
+                   want_S=False)
+        return time.perf_counter() - t0
+
+    t_probe = band(32)
+    per_row = t_probe / 32
+    total_steps = max(1, steps + warmup)
+    h = int(max(16, min(H, (budget_s / total_steps) / per_row)))
+    for _ in range(warmup):
+        band(h)
+    ts = [band(h) for _ in range(steps)]
+    t = sum(ts) / len(ts)
+    fps = (h / H) / t
+    desc = (f"rows 0..{h - 1} of a {W}x{H} frame ({h / H:.3f} frame) per step, D={D}, {PATHS} paths,"
+            f" reference CPU semantics (start-assign, stale-end table), {threads} threads;"
+            f" frames/s scaled by rows")
+    return fps, desc, threads
+
+
+def cpu_baseline_sample(budget_s=20.0):
+    fps, desc, threads = cpu_reference_run(1, 0, budget_s=budget_s)
+    return {"value": fps, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    fps, desc, threads = cpu_reference_run(args.steps, args.warmup)
+    line = {"metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 / fps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference", "config": config(),
+            "cpu_baseline": {"value": fps, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ ours
+def alg_bytes(name):
+    """Algorithmic HBM bytes of one launch of a fused kernel at this size:
+    the u16 aggregation volume (256 disparities = 512 B per pixel) read and/or
+    written once, plus the 16-byte BT planes of both images once."""
+    pix = W * H
+    s_vol = pix * 256 * 2
+    planes = 2 * pix * 16
+    if name == "fused_prep":
+        return 2 * pix + planes
+    if name.startswith("fused_pass_V+"):
+        return s_vol + planes
+    if name.endswith("_wta"):
+        return s_vol + planes + 3 * pix * 2
+    return 2 * s_vol + planes
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from thundervision_b200 import api, synthetic
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    ctx = api.Context(local)
+    ctx.reserve(W, H, D)
+
+    vs = synthetic.VideoStream(seed=1000 + rank)
+    host_frames = [vs.frame(t)[:2] for t in range(args.frames)]
+    dev_frames = [(torch.from_numpy(l).to(dev), torch.from_numpy(r).to(dev)) for l, r in host_frames]
+    pinned = [(torch.from_numpy(l).pin_memory(), torch.from_numpy(r).pin_memory())
+              for l, r in host_frames]
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    st = torch.cuda.current_stream()
+
+    def step(i):
+        l, r = dev_frames[i % len(dev_frames)]
+        return ctx.stereo_sgm(l, r, D, P1, P2, paths=PATHS, lr=LR)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timed region, per-kernel events inside the ABI ----
+    import ctypes
+
+    from thundervision_b200 import _lib
+    lib = _lib.lib()
+    lib.tdv_ctx_enable_timing(ctx.handle, 1)
+    kbuf = (ctypes.c_float * 64)()
+    ksum, kcnt = {}, {}
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    total_ms = 0.0
+    launches = 0
+    for i in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        step(i)
+        e1.record(st)
+        n = lib.tdv_ctx_timings(ctx.handle, kbuf, 64)
+        for j in range(n):
+            nm = lib.tdv_ctx_timing_name(ctx.handle, j).decode()
+            ksum[nm] = ksum.get(nm, 0.0) + kbuf[j]
+            kcnt[nm] = kcnt.get(nm, 0) + 1
+        launches += n
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    lib.tdv_ctx_enable_timing(ctx.handle, 0)
+
+    # ---- end-to-end through the public API, host buffers ----
+    host_out = torch.empty((H, W), dtype=torch.uint16).pin_memory()
+    dl = torch.empty((H, W), dtype=torch.uint8, device=dev)
+    dr = torch.empty((H, W), dtype=torch.uint8, device=dev)
+    e2e_ms = 0.0
+    for i in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        pl, pr = pinned[i % len(pinned)]
+        e0.record(st)
+        dl.copy_(pl, non_blocking=True)
+        dr.copy_(pr, non_blocking=True)
+        out = ctx.stereo_sgm(dl, dr, D, P1, P2, paths=PATHS, lr=LR)
+        host_out.copy_(out["disp"], non_blocking=True)
+        e1.record(st)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+
+    t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    total_ms, e2e_ms = float(t[0]), float(t[1])
+    if rank != 0:
+        ctx.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    frames = args.steps * world
+    fps = frames / (total_ms / 1000.0)
+    e2e_fps = frames / (e2e_ms / 1000.0)
+    cells = W * H * D * PATHS
+    # dominant kernel: largest total device time
+    dom = max(ksum, key=lambda k: ksum[k])
+    avg_ms = ksum[dom] / kcnt[dom]
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg_bytes(dom) / (avg_ms / 1000.0) / 1e9
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "fused_traffic_1080p_d256.json")))
+        traffic = tr.get("per_launch_bytes", {}).get(dom)
+    except OSError:
+        pass
+    kernels = {k: {"launches": kcnt[k], "avg_ms": ksum[k] / kcnt[k],
+                   "share": ksum[k] / sum(ksum.values())} for k in sorted(ksum)}
+    frame_alg = W * H * D * 4 * (PATHS + 3) + W * H * (2 * 1 + 2)
+    line = {
+        "metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": config({"parallelism": f"replicas x{world}, frames sharded by rank"}),
+        "gcells_per_s": cells * fps / 1e9,
+        "e2e": {"value": e2e_fps, "unit": UNIT, "h2d_bytes_per_step": 2 * W * H,
+                "d2h_bytes_per_step": 2 * W * H},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks
+                     else "fallback 6.65 TB/s"},
+        "frame_roofline": {"model": "stage-interface bytes W*H*D*4*(P+3)+W*H*4 per frame",
+                           "achieved_gbs": frame_alg * fps / world / 1e9,
+                           "frac": frame_alg * fps / world / 1e9 / peak},
+        "kernels": kernels,
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample()
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

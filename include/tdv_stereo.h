@@ -1,0 +1,183 @@
+/*
+ * tdv_stereo.h -- C ABI of the B200 (sm_100a) dense-stereo hot path:
+ * matching-cost DSI -> SGM / DP aggregation -> WTA disparity reduction.
+ *
+ * Every entry point takes plain device pointers and sizes, runs asynchronously
+ * on the caller's CUDA stream (NULL = legacy default stream) and returns a
+ * tdv_status; nothing is thrown across the ABI.  The reference (ThunderVision's
+ * LibThunderVision) reaches the same stages through free C++ functions with no
+ * extern "C"; each declaration below names the reference function it replaces
+ * (paths relative to the ThunderVision root; tdvision/ =
+ * LibThunderVision/src/tdvision/).  INTEGRATION.md shows the reference-side
+ * adapters.
+ *
+ * Conventions
+ *   - Images are single-channel, row-major, device memory: u8 or f32, with a
+ *     row pitch in elements and an intensity scale (intensity = value*scale;
+ *     scale 1/255 is the reference's [0,1] domain, tdvision/misc.cpp:31-32).
+ *   - Cost / aggregation volumes ("DSI") keep the disparity axis contiguous.
+ *     TDV_LAYOUT_REF_WHD is the reference layout, offset ((x*H)+y)*D+d with a
+ *     row pitch of D elements (tdvision/dsimem.cpp:34-35, dsimemutil.h:6);
+ *     TDV_LAYOUT_HWD is ((y*W)+x)*D+d.
+ *   - Cells with x-d < 0 hold +INF (tdvision/birchfieldcost.cu:52).
+ *   - Disparity outputs are W*H arrays: uint16 disparity (0xFFFF = rejected by
+ *     the left-right check) and/or float d/D, the reference's output format
+ *     (tdvision/wtacpu.cpp:35-36).
+ */
+#ifndef TDV_STEREO_H
+#define TDV_STEREO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TDV_ABI_VERSION 1
+
+typedef struct tdv_ctx tdv_ctx;
+typedef void* tdv_stream; /* a cudaStream_t */
+
+/* Replaces the reference's exception convention (CUException thrown by
+ * CUerrExp, tdvision/cuerr.hpp:73-78, cuerr.cpp:6-15). */
+typedef enum {
+    TDV_OK = 0,
+    TDV_ERR_INVALID_ARG = 1,
+    TDV_ERR_UNSUPPORTED = 2,
+    TDV_ERR_OOM = 3,
+    TDV_ERR_CUDA = 4,
+    TDV_ERR_TIMEOUT = 5,
+    TDV_ERR_BAD_WORK = 6
+} tdv_status;
+
+typedef enum { TDV_LAYOUT_REF_WHD = 0, TDV_LAYOUT_HWD = 1 } tdv_layout;
+typedef enum { TDV_F32 = 0, TDV_U16 = 1, TDV_U8 = 2, TDV_F64 = 3 } tdv_dtype;
+
+typedef struct {
+    const void* ptr;  /* device */
+    int32_t width, height;
+    int32_t pitch;    /* elements between rows, >= width */
+    int32_t dtype;    /* TDV_U8 or TDV_F32 */
+    float scale;      /* intensity = value * scale */
+} tdv_image;
+
+typedef struct {
+    void* ptr;        /* device, dense, no padding between pixels */
+    int32_t width, height, depth;
+    int32_t layout;   /* tdv_layout */
+    int32_t dtype;    /* TDV_F32 (TDV_F64 accepted by the soft-SGM calls) */
+} tdv_volume;
+
+typedef struct {
+    uint16_t* disp;       /* W*H disparity, may be NULL */
+    float* disp_norm;     /* W*H d/D (reference format), may be NULL */
+    uint16_t* disp_right; /* W*H right-view disparity, may be NULL */
+    int32_t lr_threshold; /* < 0: no left-right check; else reject |dL-dR|>thr */
+} tdv_disparity;
+
+/* ---- matching cost --------------------------------------------------- */
+typedef enum { TDV_COST_BT = 0, TDV_COST_SSD = 1, TDV_COST_NCC = 2 } tdv_cost_kind;
+
+typedef struct {
+    int32_t kind;   /* tdv_cost_kind */
+    int32_t radius; /* SSD/NCC window radius: SSD 3 = the reference's 7x7
+                       (tdvision/ssd.cu:11-13), NCC 1 = its 3x3
+                       (tdvision/crosscorrelation.cu:17-18); ignored for BT */
+} tdv_cost_params;
+
+/* Fills the cost DSI `out` (F32, either layout) from a rectified pair.
+ * Replaces BirchfieldCostRun (tdvision/birchfieldcost.cu:194-212),
+ * SSDDevRun (tdvision/ssd.cu:79-114) and CrossCorrelationDevRun
+ * (tdvision/crosscorrelation.cu:53-76), i.e. the updateImpl of
+ * AbstractMatchingCost (tdvision/matchingcost.hpp:48-49). */
+tdv_status tdv_cost(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right,
+                    const tdv_cost_params* params, tdv_volume* out, tdv_stream stream);
+
+/* ---- semi-global aggregation ----------------------------------------- */
+typedef enum {
+    TDV_SEM_STANDARD = 0, /* S += C at path starts, previous = C, full min over d */
+    TDV_SEM_REF_CPU = 1,  /* tdvision/semiglobalcpu.cpp:56-126 as written */
+    TDV_SEM_REF_GPU = 2   /* tdvision/semiglobal.cu:283-466 without its race */
+} tdv_sgm_semantics;
+typedef enum { TDV_TABLE_FULL = 0, TDV_TABLE_REF = 1 } tdv_path_table;
+typedef enum { TDV_P2_CONST = 0, TDV_P2_ADJUST = 1 } tdv_p2_mode;
+
+typedef struct {
+    float p1, p2;      /* penalties (reference: 30/255, 150/255,
+                          tdvision/semiglobalcpu.cpp:36-37) */
+    int32_t p2_mode;   /* tdv_p2_mode: ADJUST = P2/|I(p)-I(p-r)| */
+    int32_t paths;     /* 8, or 4 (horizontal + vertical) */
+    int32_t table;     /* tdv_path_table: REF = the reference's SGPaths as built
+                          by tdvision/semiglobal.cu:57-230 */
+    int32_t semantics; /* tdv_sgm_semantics */
+} tdv_sgm_params;
+
+/* Aggregates a cost DSI and reduces it to disparities (fused WTA, optional
+ * left-right check).  `guide` is the intensity image for P2_ADJUST (may be
+ * NULL otherwise).  `aggreg` (optional, F32, same layout as `cost`) receives
+ * the aggregated volume.  Replaces SemiGlobalDevRun
+ * (tdvision/semiglobal.cu:474-521) and SemiGlobalCPU::updateImpl
+ * (tdvision/semiglobalcpu.cpp:173-230). */
+tdv_status tdv_sgm(tdv_ctx* ctx, const tdv_volume* cost, const tdv_image* guide,
+                   const tdv_sgm_params* params, tdv_volume* aggreg, tdv_disparity* out,
+                   tdv_stream stream);
+
+/* Winner-take-all over a DSI, lowest d on ties.  Replaces WTARunDev
+ * (tdvision/wta.cu:90-100) and WTACPU::wta (tdvision/wtacpu.cpp:14-39). */
+tdv_status tdv_wta(tdv_ctx* ctx, const tdv_volume* vol, tdv_disparity* out, tdv_stream stream);
+
+/* Dynamic-programming scanline matcher over a cost DSI.  Replaces
+ * DynamicProgDevRun (tdvision/dynamicprog.cu:106-122). */
+tdv_status tdv_dp_scanline(tdv_ctx* ctx, const tdv_volume* cost, tdv_disparity* out,
+                           tdv_stream stream);
+
+/* SSD window + WTA fused, no DSI.  Replaces FastWTADevRun
+ * (tdvision/fastwta.cu:57-83). */
+tdv_status tdv_fast_wta(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right,
+                        int32_t max_disp, int32_t radius, tdv_disparity* out, tdv_stream stream);
+
+/* Birchfield-Tomasi cost recomputed inside the aggregation, no cost DSI:
+ * the role of SemiGlobalLabDevRun (tdvision/semiglobal_lab.cu:232-282) with
+ * the reference's cost and recurrence.  Integer-domain inputs (u8, scale 1,
+ * P1/P2 multiples of 1/2, STANDARD, FULL, P2_CONST, D <= 256) take the fused
+ * 16-bit path; anything else runs tdv_cost + tdv_sgm on context scratch. */
+tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right,
+                          int32_t max_disp, const tdv_sgm_params* params, tdv_disparity* out,
+                          tdv_stream stream);
+
+/* ---- context ---------------------------------------------------------- */
+typedef void* (*tdv_alloc_fn)(size_t bytes, void* user);
+typedef void (*tdv_free_fn)(void* ptr, void* user);
+
+/* Creates a context bound to `device`; no CUDA call is made until first use.
+ * A context owns scratch (aggregation volumes, path tables); use one per host
+ * thread.  Replaces the per-stage scratch of SemiGlobalDev / DynamicProgDev
+ * (tdvision/semiglobaldev.hpp:19-21, dynamicprogdev.hpp:14-15). */
+tdv_status tdv_ctx_create(int32_t device, tdv_ctx** out);
+void tdv_ctx_destroy(tdv_ctx* ctx);
+/* Replaces the device allocator for scratch (default cudaMalloc/cudaFree). */
+tdv_status tdv_ctx_set_allocator(tdv_ctx* ctx, tdv_alloc_fn alloc, tdv_free_fn release,
+                                 void* user);
+/* Pre-sizes scratch for pairs up to W x H x D so later calls do not allocate. */
+tdv_status tdv_ctx_reserve(tdv_ctx* ctx, int32_t width, int32_t height, int32_t max_disp);
+const char* tdv_last_error_string(const tdv_ctx* ctx);
+/* Per-kernel timing: when enabled, every kernel a call launches is bracketed
+ * by CUDA events on the call's stream; tdv_ctx_timings then returns (after the
+ * stream has been synchronised) the device milliseconds of each launch of the
+ * most recent call and tdv_ctx_timing_name its kernel name.  This replaces the
+ * reference's CudaBenchmarker around each stage update
+ * (tdvision/benchmark.cpp:7-31, matchingcost.cpp:35-42). */
+tdv_status tdv_ctx_enable_timing(tdv_ctx* ctx, int32_t enable);
+int32_t tdv_ctx_timings(tdv_ctx* ctx, float* ms_out, int32_t max_entries);
+const char* tdv_ctx_timing_name(const tdv_ctx* ctx, int32_t index);
+const char* tdv_status_string(tdv_status status);
+int32_t tdv_version(void);
+/* Bytes of a dense W x H x D volume of `dtype`. */
+size_t tdv_volume_bytes(int32_t width, int32_t height, int32_t depth, int32_t dtype);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TDV_STEREO_H */

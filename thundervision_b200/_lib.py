@@ -1,0 +1,122 @@
+"""ctypes binding of the C ABI declared in include/tdv_stereo.h.
+
+The shared library ``libtdvb200.so`` is built in-tree by
+``thundervision_b200/csrc/Makefile``; nothing here falls back to another
+implementation: if the library is missing or a call fails, an exception is
+raised (the reference's stages throw ``CUException``, tdvision/cuerr.hpp:73-78).
+"""
+import ctypes
+import os
+import subprocess
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtdvb200.so")
+CSRC = os.path.join(_HERE, "csrc")
+
+TDV_OK, TDV_ERR_INVALID_ARG, TDV_ERR_UNSUPPORTED, TDV_ERR_OOM = 0, 1, 2, 3
+TDV_ERR_CUDA, TDV_ERR_TIMEOUT, TDV_ERR_BAD_WORK = 4, 5, 6
+LAYOUT_REF_WHD, LAYOUT_HWD = 0, 1
+F32, U16, U8, F64 = 0, 1, 2, 3
+COST_BT, COST_SSD, COST_NCC = 0, 1, 2
+SEM_STANDARD, SEM_REF_CPU, SEM_REF_GPU = 0, 1, 2
+TABLE_FULL, TABLE_REF = 0, 1
+P2_CONST, P2_ADJUST = 0, 1
+
+# every symbol include/tdv_stereo.h declares
+EXPORTS = [
+    "tdv_cost", "tdv_sgm", "tdv_wta", "tdv_dp_scanline", "tdv_fast_wta", "tdv_stereo_sgm",
+    "tdv_ctx_create", "tdv_ctx_destroy", "tdv_ctx_set_allocator", "tdv_ctx_reserve",
+    "tdv_last_error_string", "tdv_status_string", "tdv_version", "tdv_volume_bytes",
+    "tdv_ctx_enable_timing", "tdv_ctx_timings", "tdv_ctx_timing_name",
+]
+
+
+class tdv_image(ctypes.Structure):
+    _fields_ = [("ptr", ctypes.c_void_p), ("width", ctypes.c_int32), ("height", ctypes.c_int32),
+                ("pitch", ctypes.c_int32), ("dtype", ctypes.c_int32), ("scale", ctypes.c_float)]
+
+
+class tdv_volume(ctypes.Structure):
+    _fields_ = [("ptr", ctypes.c_void_p), ("width", ctypes.c_int32), ("height", ctypes.c_int32),
+                ("depth", ctypes.c_int32), ("layout", ctypes.c_int32), ("dtype", ctypes.c_int32)]
+
+
+class tdv_disparity(ctypes.Structure):
+    _fields_ = [("disp", ctypes.c_void_p), ("disp_norm", ctypes.c_void_p),
+                ("disp_right", ctypes.c_void_p), ("lr_threshold", ctypes.c_int32)]
+
+
+class tdv_cost_params(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("radius", ctypes.c_int32)]
+
+
+class tdv_sgm_params(ctypes.Structure):
+    _fields_ = [("p1", ctypes.c_float), ("p2", ctypes.c_float), ("p2_mode", ctypes.c_int32),
+                ("paths", ctypes.c_int32), ("table", ctypes.c_int32), ("semantics", ctypes.c_int32)]
+
+
+ALLOC_FN = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
+FREE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p)
+
+_lib = None
+
+
+def build(force=False):
+    """Compile libtdvb200.so for sm_100a (nvcc cross-compiles without a GPU)."""
+    if force:
+        subprocess.check_call(["make", "-s", "-C", CSRC, "clean"])
+    subprocess.check_call(["make", "-s", "-C", CSRC])
+
+
+def _declare(lib):
+    P = ctypes.POINTER
+    vp = ctypes.c_void_p
+    st = ctypes.c_int
+    sig = {
+        "tdv_cost": (st, [vp, P(tdv_image), P(tdv_image), P(tdv_cost_params), P(tdv_volume), vp]),
+        "tdv_sgm": (st, [vp, P(tdv_volume), P(tdv_image), P(tdv_sgm_params), P(tdv_volume),
+                         P(tdv_disparity), vp]),
+        "tdv_wta": (st, [vp, P(tdv_volume), P(tdv_disparity), vp]),
+        "tdv_dp_scanline": (st, [vp, P(tdv_volume), P(tdv_disparity), vp]),
+        "tdv_fast_wta": (st, [vp, P(tdv_image), P(tdv_image), ctypes.c_int32, ctypes.c_int32,
+                              P(tdv_disparity), vp]),
+        "tdv_stereo_sgm": (st, [vp, P(tdv_image), P(tdv_image), ctypes.c_int32, P(tdv_sgm_params),
+                                P(tdv_disparity), vp]),
+        "tdv_ctx_create": (st, [ctypes.c_int32, P(vp)]),
+        "tdv_ctx_destroy": (None, [vp]),
+        "tdv_ctx_set_allocator": (st, [vp, ALLOC_FN, FREE_FN, vp]),
+        "tdv_ctx_reserve": (st, [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+        "tdv_last_error_string": (ctypes.c_char_p, [vp]),
+        "tdv_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+        "tdv_version": (ctypes.c_int32, []),
+        "tdv_ctx_enable_timing": (st, [vp, ctypes.c_int32]),
+        "tdv_ctx_timings": (ctypes.c_int32, [vp, P(ctypes.c_float), ctypes.c_int32]),
+        "tdv_ctx_timing_name": (ctypes.c_char_p, [vp, ctypes.c_int32]),
+        "tdv_volume_bytes": (ctypes.c_size_t, [ctypes.c_int32] * 4),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+
+
+def lib():
+    """The loaded C-ABI library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                "libtdvb200.so not built: run thundervision_b200._lib.build() (or make -C "
+                "thundervision_b200/csrc)")
+        l = ctypes.CDLL(LIB_PATH)
+        _declare(l)
+        _lib = l
+    return _lib
+
+
+class TdvError(RuntimeError):
+    """A non-OK tdv_status (the reference raises tdv::CUException)."""
+
+    def __init__(self, status, message):
+        self.status = status
+        super().__init__(f"{lib().tdv_status_string(status).decode()}: {message}")

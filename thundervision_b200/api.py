@@ -1,0 +1,199 @@
+"""Python front end of the C ABI on torch CUDA tensors.
+
+Images are (H, W) uint8 or float32 CUDA tensors (row stride may exceed W);
+cost / aggregation volumes are float32 CUDA tensors shaped (H, W, D) for the
+HWD layout or (W, H, D) for the reference layout ((x*H)+y)*D+d
+(tdvision/dsimem.cpp:34-35).  Every call runs on torch's current stream.
+Disparities come back as uint16 (0xFFFF = rejected by the left-right check)
+and, on request, float32 d/D -- the reference's output format
+(tdvision/wtacpu.cpp:35-36).
+"""
+import ctypes
+
+import torch
+
+from . import _lib as L
+
+_LAYOUTS = {"hwd": L.LAYOUT_HWD, "ref": L.LAYOUT_REF_WHD, "whd": L.LAYOUT_REF_WHD}
+_COSTS = {"bt": L.COST_BT, "ssd": L.COST_SSD, "ncc": L.COST_NCC}
+_SEMS = {"standard": L.SEM_STANDARD, "ref_cpu": L.SEM_REF_CPU, "ref_gpu": L.SEM_REF_GPU}
+_TABLES = {"full": L.TABLE_FULL, "ref": L.TABLE_REF}
+_P2 = {"const": L.P2_CONST, "adjust": L.P2_ADJUST}
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _image(t, scale=1.0):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("images must be CUDA tensors")
+    if t.dim() != 2 or t.stride(1) != 1:
+        raise ValueError("images must be (H, W) with unit column stride")
+    if t.dtype == torch.uint8:
+        dt = L.U8
+    elif t.dtype == torch.float32:
+        dt = L.F32
+    else:
+        raise TypeError("images must be uint8 or float32")
+    return L.tdv_image(t.data_ptr(), t.shape[1], t.shape[0], t.stride(0), dt, float(scale))
+
+
+def _volume(t, layout):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float32:
+        raise TypeError("volumes must be float32 CUDA tensors")
+    if t.dim() != 3 or not t.is_contiguous():
+        raise ValueError("volumes must be contiguous 3-d tensors")
+    lay = _LAYOUTS[layout]
+    if lay == L.LAYOUT_HWD:
+        H, W, D = t.shape
+    else:
+        W, H, D = t.shape
+    return L.tdv_volume(t.data_ptr(), W, H, D, lay, L.F32)
+
+
+def _vol_dims(t, layout):
+    if _LAYOUTS[layout] == L.LAYOUT_HWD:
+        H, W, D = t.shape
+    else:
+        W, H, D = t.shape
+    return W, H, D
+
+
+class Context:
+    """Owns a tdv_ctx (scratch buffers, path schedules) for one device."""
+
+    def __init__(self, device=None):
+        if device is None:
+            device = torch.cuda.current_device()
+        self.device = int(device)
+        h = ctypes.c_void_p()
+        st = L.lib().tdv_ctx_create(self.device, ctypes.byref(h))
+        if st != L.TDV_OK:
+            raise L.TdvError(st, "tdv_ctx_create")
+        self.handle = h
+        self._keep = []
+
+    def close(self):
+        if self.handle:
+            L.lib().tdv_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, status):
+        if status != L.TDV_OK:
+            msg = L.lib().tdv_last_error_string(self.handle).decode()
+            raise L.TdvError(status, msg)
+
+    def reserve(self, W, H, D):
+        self.check(L.lib().tdv_ctx_reserve(self.handle, W, H, D))
+
+    def set_allocator(self, alloc, release, user=None):
+        a, r = L.ALLOC_FN(alloc), L.FREE_FN(release)
+        self._keep += [a, r]
+        self.check(L.lib().tdv_ctx_set_allocator(self.handle, a, r, user))
+
+    # ---- outputs --------------------------------------------------------
+    def _outputs(self, W, H, dev, norm, right, lr):
+        disp = torch.empty((H, W), dtype=torch.uint16, device=dev)
+        dn = torch.empty((H, W), dtype=torch.float32, device=dev) if norm else None
+        dr = torch.empty((H, W), dtype=torch.uint16, device=dev) if right else None
+        o = L.tdv_disparity(disp.data_ptr(), dn.data_ptr() if dn is not None else None,
+                            dr.data_ptr() if dr is not None else None,
+                            -1 if lr is None else int(lr))
+        return o, disp, dn, dr
+
+    @staticmethod
+    def _result(disp, dn, dr):
+        out = {"disp": disp}
+        if dn is not None:
+            out["disp_norm"] = dn
+        if dr is not None:
+            out["disp_right"] = dr
+        return out
+
+    # ---- stages ---------------------------------------------------------
+    def cost(self, left, right, max_disp, kind="bt", radius=None, layout="hwd", scale=1.0,
+             out=None):
+        """Matching-cost DSI (BirchfieldCostRun / SSDDevRun / CrossCorrelationDevRun)."""
+        if radius is None:
+            radius = {"bt": 0, "ssd": 3, "ncc": 1}[kind]
+        H = min(left.shape[0], right.shape[0])
+        W = min(left.shape[1], right.shape[1])
+        if out is None:
+            shape = (H, W, max_disp) if _LAYOUTS[layout] == L.LAYOUT_HWD else (W, H, max_disp)
+            out = torch.empty(shape, dtype=torch.float32, device=left.device)
+        li, ri = _image(left, scale), _image(right, scale)
+        vol = _volume(out, layout)
+        p = L.tdv_cost_params(_COSTS[kind], radius)
+        self.check(L.lib().tdv_cost(self.handle, ctypes.byref(li), ctypes.byref(ri), ctypes.byref(p),
+                                    ctypes.byref(vol), _stream()))
+        return out
+
+    def sgm(self, cost, p1, p2, guide=None, guide_scale=1.0, p2_mode="const", paths=8,
+            table="full", semantics="standard", layout="hwd", lr=None, norm=False, right=False,
+            aggreg=None):
+        """SGM aggregation + WTA (SemiGlobalDevRun / SemiGlobalCPU::updateImpl)."""
+        W, H, D = _vol_dims(cost, layout)
+        cv = _volume(cost, layout)
+        gi = _image(guide, guide_scale) if guide is not None else None
+        prm = L.tdv_sgm_params(p1, p2, _P2[p2_mode], paths, _TABLES[table], _SEMS[semantics])
+        av = _volume(aggreg, layout) if aggreg is not None else None
+        o, disp, dn, dr = self._outputs(W, H, cost.device, norm, right, lr)
+        self.check(L.lib().tdv_sgm(self.handle, ctypes.byref(cv),
+                                   ctypes.byref(gi) if gi is not None else None, ctypes.byref(prm),
+                                   ctypes.byref(av) if av is not None else None, ctypes.byref(o),
+                                   _stream()))
+        return self._result(disp, dn, dr)
+
+    def wta(self, vol, layout="hwd", norm=False, lr=None, right=False):
+        """Winner-take-all (WTARunDev / WTACPU::wta)."""
+        W, H, D = _vol_dims(vol, layout)
+        v = _volume(vol, layout)
+        o, disp, dn, dr = self._outputs(W, H, vol.device, norm, right, lr)
+        self.check(L.lib().tdv_wta(self.handle, ctypes.byref(v), ctypes.byref(o), _stream()))
+        return self._result(disp, dn, dr)
+
+    def dp(self, cost, layout="hwd", norm=False):
+        """Dynamic-programming scanline matcher (DynamicProgDevRun)."""
+        W, H, D = _vol_dims(cost, layout)
+        v = _volume(cost, layout)
+        o, disp, dn, dr = self._outputs(W, H, cost.device, norm, False, None)
+        self.check(L.lib().tdv_dp_scanline(self.handle, ctypes.byref(v), ctypes.byref(o), _stream()))
+        return self._result(disp, dn, dr)
+
+    def fast_wta(self, left, right, max_disp, radius=3, scale=1.0, norm=False):
+        """SSD window + WTA without a DSI (FastWTADevRun)."""
+        H, W = left.shape
+        li, ri = _image(left, scale), _image(right, scale)
+        o, disp, dn, dr = self._outputs(W, H, left.device, norm, False, None)
+        self.check(L.lib().tdv_fast_wta(self.handle, ctypes.byref(li), ctypes.byref(ri), max_disp,
+                                        radius, ctypes.byref(o), _stream()))
+        return self._result(disp, dn, dr)
+
+    def stereo_sgm(self, left, right, max_disp, p1, p2, paths=8, p2_mode="const", table="full",
+                   semantics="standard", scale=1.0, lr=None, norm=False, right_disp=False):
+        """BT + SGM + WTA with the cost recomputed inside the aggregation."""
+        H, W = left.shape
+        li, ri = _image(left, scale), _image(right, scale)
+        prm = L.tdv_sgm_params(p1, p2, _P2[p2_mode], paths, _TABLES[table], _SEMS[semantics])
+        o, disp, dn, dr = self._outputs(W, H, left.device, norm, right_disp, lr)
+        self.check(L.lib().tdv_stereo_sgm(self.handle, ctypes.byref(li), ctypes.byref(ri), max_disp,
+                                          ctypes.byref(prm), ctypes.byref(o), _stream()))
+        return self._result(disp, dn, dr)
+
+
+_default = {}
+
+
+def default_context(device=None):
+    if device is None:
+        device = torch.cuda.current_device()
+    if device not in _default:
+        _default[device] = Context(device)
+    return _default[device]

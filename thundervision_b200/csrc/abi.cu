@@ -1,0 +1,518 @@
+// Host side of the C ABI: argument validation, context scratch, dispatch.
+// Every entry point validates its arguments before touching CUDA, returns a
+// tdv_status and records a message retrievable with tdv_last_error_string.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "tdv_internal.hpp"
+
+using tdv::ImgArg;
+using tdv::VolArg;
+
+namespace {
+
+constexpr int kMaxSide = 16384;
+
+tdv_status fail(tdv_ctx* ctx, tdv_status s, const char* fmt, ...) {
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        ctx->last_error = buf;
+    }
+    return s;
+}
+
+#define TDV_CUDA(call)                                                                     \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(ctx, TDV_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+#define TDV_TRY(expr)                     \
+    do {                                  \
+        tdv_status s_ = (expr);           \
+        if (s_ != TDV_OK) return s_;      \
+    } while (0)
+
+// Makes ctx->device current for the duration of a call and restores the
+// caller's device afterwards.
+struct DeviceScope {
+    int prev = -1;
+    bool changed = false;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceScope(int dev) {
+        err = cudaGetDevice(&prev);
+        if (err == cudaSuccess && prev != dev) {
+            err = cudaSetDevice(dev);
+            changed = err == cudaSuccess;
+        }
+    }
+    ~DeviceScope() {
+        if (changed) cudaSetDevice(prev);
+    }
+};
+
+#define TDV_DEVICE_SCOPE(ctx)                                                                \
+    DeviceScope dscope_((ctx)->device);                                                      \
+    if (dscope_.err != cudaSuccess)                                                          \
+        return fail(ctx, TDV_ERR_CUDA, "selecting device %d: %s", (ctx)->device,             \
+                    cudaGetErrorString(dscope_.err))
+
+tdv_status check_image(tdv_ctx* ctx, const tdv_image* im, const char* name) {
+    if (!im) return fail(ctx, TDV_ERR_INVALID_ARG, "%s: null image", name);
+    if (!im->ptr) return fail(ctx, TDV_ERR_INVALID_ARG, "%s: null data pointer", name);
+    if (im->width <= 0 || im->height <= 0 || im->width > kMaxSide || im->height > kMaxSide)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "%s: bad size %dx%d", name, im->width, im->height);
+    if (im->pitch < im->width)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "%s: pitch %d < width %d", name, im->pitch, im->width);
+    if (im->dtype != TDV_U8 && im->dtype != TDV_F32)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "%s: dtype must be TDV_U8 or TDV_F32", name);
+    if (!std::isfinite(im->scale)) return fail(ctx, TDV_ERR_INVALID_ARG, "%s: scale not finite", name);
+    return TDV_OK;
+}
+
+tdv_status check_volume(tdv_ctx* ctx, const tdv_volume* v, const char* name) {
+    if (!v) return fail(ctx, TDV_ERR_INVALID_ARG, "%s: null volume", name);
+    if (!v->ptr) return fail(ctx, TDV_ERR_INVALID_ARG, "%s: null data pointer", name);
+    if (v->width <= 0 || v->height <= 0 || v->depth <= 0 || v->width > kMaxSide ||
+        v->height > kMaxSide)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "%s: bad size %dx%dx%d", name, v->width, v->height,
+                    v->depth);
+    if (v->layout != TDV_LAYOUT_REF_WHD && v->layout != TDV_LAYOUT_HWD)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "%s: bad layout %d", name, v->layout);
+    if (v->dtype != TDV_F32) return fail(ctx, TDV_ERR_INVALID_ARG, "%s: dtype must be TDV_F32", name);
+    return TDV_OK;
+}
+
+tdv_status check_out(tdv_ctx* ctx, const tdv_disparity* o) {
+    if (!o) return fail(ctx, TDV_ERR_INVALID_ARG, "null disparity output");
+    if (!o->disp && !o->disp_norm && !o->disp_right)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "disparity output: all pointers null");
+    return TDV_OK;
+}
+
+tdv_status check_params(tdv_ctx* ctx, const tdv_sgm_params* p) {
+    if (!p) return fail(ctx, TDV_ERR_INVALID_ARG, "null sgm params");
+    if (!std::isfinite(p->p1) || !std::isfinite(p->p2))
+        return fail(ctx, TDV_ERR_INVALID_ARG, "penalties must be finite");
+    if (p->p2_mode != TDV_P2_CONST && p->p2_mode != TDV_P2_ADJUST)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "bad p2_mode %d", p->p2_mode);
+    if (p->paths != 4 && p->paths != 8) return fail(ctx, TDV_ERR_INVALID_ARG, "paths must be 4 or 8");
+    if (p->table != TDV_TABLE_FULL && p->table != TDV_TABLE_REF)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "bad table %d", p->table);
+    if (p->semantics < TDV_SEM_STANDARD || p->semantics > TDV_SEM_REF_GPU)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "bad semantics %d", p->semantics);
+    return TDV_OK;
+}
+
+// Scratch buffers grow on demand; growing waits for the device first because
+// work already queued may still read the old buffer.
+tdv_status ensure(tdv_ctx* ctx, tdv_ctx::Buf& b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.bytes >= bytes) return TDV_OK;
+    if (b.ptr) {
+        cudaDeviceSynchronize();
+        if (ctx->release) ctx->release(b.ptr, ctx->alloc_user);
+        else cudaFree(b.ptr);
+        b.ptr = nullptr;
+        b.bytes = 0;
+    }
+    void* p = nullptr;
+    if (ctx->alloc) {
+        p = ctx->alloc(bytes, ctx->alloc_user);
+    } else if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        p = nullptr;
+    }
+    if (!p) return fail(ctx, TDV_ERR_OOM, "allocating %zu bytes of scratch failed", bytes);
+    b.ptr = p;
+    b.bytes = bytes;
+    return TDV_OK;
+}
+
+void release_buf(tdv_ctx* ctx, tdv_ctx::Buf& b) {
+    if (!b.ptr) return;
+    if (ctx->release) ctx->release(b.ptr, ctx->alloc_user);
+    else cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+}
+
+cudaStream_t S(tdv_stream s) { return (cudaStream_t)s; }
+
+tdv_status ensure_schedule(tdv_ctx* ctx, int W, int H, int table, int paths, cudaStream_t st) {
+    tdv::PassSchedule& sc = ctx->sched;
+    if (sc.W == W && sc.H == H && sc.table == table && sc.paths == paths && sc.d_walks) return TDV_OK;
+    tdv::PassSchedule fresh;
+    if (!tdv::build_schedule(W, H, table, paths, fresh))
+        return fail(ctx, TDV_ERR_BAD_WORK, "path table for %dx%d has a walk outside the image", W, H);
+    TDV_TRY(ensure(ctx, ctx->sched_buf, fresh.walks.size() * sizeof(tdv::Walk)));
+    sc = std::move(fresh);
+    sc.d_walks = (tdv::Walk*)ctx->sched_buf.ptr;
+    TDV_CUDA(cudaMemcpyAsync(sc.d_walks, sc.walks.data(), sc.walks.size() * sizeof(tdv::Walk),
+                             cudaMemcpyHostToDevice, st));
+    // the host vector is the copy source: keep it until the copy has run
+    TDV_CUDA(cudaStreamSynchronize(st));
+    return TDV_OK;
+}
+
+tdv_status run_sgm(tdv_ctx* ctx, const tdv_volume* cost, const tdv_image* guide,
+                   const tdv_sgm_params* p, tdv_volume* aggreg, tdv_disparity* out, cudaStream_t st) {
+    const int W = cost->width, H = cost->height, D = cost->depth;
+    VolArg C = tdv::make_vol(*cost);
+    VolArg Sv;
+    if (aggreg) {
+        Sv = tdv::make_vol(*aggreg);
+    } else {
+        TDV_TRY(ensure(ctx, ctx->agg, (size_t)W * H * D * sizeof(float)));
+        tdv_volume tmp = *cost;
+        tmp.ptr = ctx->agg.ptr;
+        Sv = tdv::make_vol(tmp);
+    }
+    TDV_TRY(ensure_schedule(ctx, W, H, p->table, p->paths, st));
+    tdv::SgmArgs a;
+    a.C = C;
+    a.S = Sv;
+    a.has_guide = guide ? 1 : 0;
+    if (guide) a.guide = tdv::make_img(*guide);
+    else memset(&a.guide, 0, sizeof(a.guide));
+    a.p1 = p->p1;
+    a.p2 = p->p2;
+    a.p2_adjust = p->p2_mode == TDV_P2_ADJUST;
+    a.sem = p->semantics;
+    TDV_CUDA(tdv::launch_sgm_passes(a, ctx->sched, st, &ctx->timer));
+    uint16_t* disp = out->disp;
+    if (!disp && (out->lr_threshold >= 0 || out->disp_right)) {
+        TDV_TRY(ensure(ctx, ctx->misc, (size_t)W * H * sizeof(uint16_t)));
+        disp = (uint16_t*)ctx->misc.ptr;
+    }
+    TDV_CUDA(tdv::launch_wta(Sv, disp, out->disp_norm, st, &ctx->timer));
+    if (out->lr_threshold >= 0 || out->disp_right)
+        TDV_CUDA(tdv::launch_lr(Sv, disp, out->disp_norm, out->disp_right,
+                                out->lr_threshold >= 0 ? out->lr_threshold : 0x7FFFFFFF, st,
+                                &ctx->timer));
+    return TDV_OK;
+}
+
+bool is_half_multiple(float v) { return v >= 0.0f && v <= 4096.0f && std::floor(2.0f * v) == 2.0f * v; }
+
+}  // namespace
+
+namespace tdv {
+
+VolArg make_vol(const tdv_volume& v) {
+    VolArg a;
+    a.ptr = v.ptr;
+    a.W = v.width;
+    a.H = v.height;
+    a.D = v.depth;
+    if (v.layout == TDV_LAYOUT_REF_WHD) {
+        a.sx = (long long)v.height * v.depth;
+        a.sy = v.depth;
+    } else {
+        a.sx = v.depth;
+        a.sy = (long long)v.width * v.depth;
+    }
+    return a;
+}
+
+ImgArg make_img(const tdv_image& im) {
+    ImgArg a;
+    a.ptr = im.ptr;
+    a.W = im.width;
+    a.H = im.height;
+    a.pitch = im.pitch;
+    a.u8 = im.dtype == TDV_U8 ? 1 : 0;
+    a.scale = im.scale;
+    return a;
+}
+
+}  // namespace tdv
+
+extern "C" {
+
+int32_t tdv_version(void) { return TDV_ABI_VERSION; }
+
+const char* tdv_status_string(tdv_status s) {
+    switch (s) {
+        case TDV_OK: return "ok";
+        case TDV_ERR_INVALID_ARG: return "invalid argument";
+        case TDV_ERR_UNSUPPORTED: return "unsupported";
+        case TDV_ERR_OOM: return "out of memory";
+        case TDV_ERR_CUDA: return "cuda error";
+        case TDV_ERR_TIMEOUT: return "timeout";
+        case TDV_ERR_BAD_WORK: return "bad work item";
+    }
+    return "unknown status";
+}
+
+size_t tdv_volume_bytes(int32_t W, int32_t H, int32_t D, int32_t dtype) {
+    if (W <= 0 || H <= 0 || D <= 0) return 0;
+    size_t e = dtype == TDV_F64 ? 8 : dtype == TDV_F32 ? 4 : dtype == TDV_U16 ? 2 : 1;
+    return (size_t)W * H * D * e;
+}
+
+tdv_status tdv_ctx_create(int32_t device, tdv_ctx** out) {
+    if (!out) return TDV_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (device < 0) return TDV_ERR_INVALID_ARG;
+    tdv_ctx* c = new (std::nothrow) tdv_ctx;
+    if (!c) return TDV_ERR_OOM;
+    c->device = device;
+    *out = c;
+    return TDV_OK;
+}
+
+void tdv_ctx_destroy(tdv_ctx* ctx) {
+    if (!ctx) return;
+    const bool any = ctx->agg.ptr || ctx->cost.ptr || ctx->planes.ptr || ctx->codes.ptr ||
+                     ctx->misc.ptr || ctx->sched_buf.ptr;
+    if (any) {
+        DeviceScope ds(ctx->device);
+        cudaDeviceSynchronize();
+        release_buf(ctx, ctx->agg);
+        release_buf(ctx, ctx->cost);
+        release_buf(ctx, ctx->planes);
+        release_buf(ctx, ctx->codes);
+        release_buf(ctx, ctx->misc);
+        release_buf(ctx, ctx->sched_buf);
+    }
+    if (!ctx->timer.ev.empty()) {
+        DeviceScope ds(ctx->device);
+        for (cudaEvent_t e : ctx->timer.ev) cudaEventDestroy(e);
+    }
+    delete ctx;
+}
+
+tdv_status tdv_ctx_set_allocator(tdv_ctx* ctx, tdv_alloc_fn alloc, tdv_free_fn release, void* user) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    if ((alloc == nullptr) != (release == nullptr))
+        return fail(ctx, TDV_ERR_INVALID_ARG, "allocator and release must be set together");
+    if (ctx->agg.ptr || ctx->cost.ptr || ctx->planes.ptr || ctx->codes.ptr || ctx->misc.ptr ||
+        ctx->sched_buf.ptr)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "allocator must be set before any scratch exists");
+    ctx->alloc = alloc;
+    ctx->release = release;
+    ctx->alloc_user = user;
+    return TDV_OK;
+}
+
+tdv_status tdv_ctx_reserve(tdv_ctx* ctx, int32_t W, int32_t H, int32_t D) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    if (W <= 0 || H <= 0 || D <= 0 || W > kMaxSide || H > kMaxSide)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "bad reserve size %dx%dx%d", W, H, D);
+    if (!ctx->alloc) {
+        TDV_DEVICE_SCOPE(ctx);
+        TDV_TRY(ensure(ctx, ctx->planes, tdv::fused_plane_bytes(W, H)));
+        if (D <= tdv::kMaxDispSgm) TDV_TRY(ensure(ctx, ctx->agg, tdv::fused_agg_bytes(W, H, D)));
+        TDV_TRY(ensure(ctx, ctx->misc, (size_t)W * H * sizeof(uint16_t)));
+        return TDV_OK;
+    }
+    TDV_TRY(ensure(ctx, ctx->planes, tdv::fused_plane_bytes(W, H)));
+    if (D <= tdv::kMaxDispSgm) TDV_TRY(ensure(ctx, ctx->agg, tdv::fused_agg_bytes(W, H, D)));
+    TDV_TRY(ensure(ctx, ctx->misc, (size_t)W * H * sizeof(uint16_t)));
+    return TDV_OK;
+}
+
+tdv_status tdv_ctx_enable_timing(tdv_ctx* ctx, int32_t enable) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    ctx->timer.on = enable != 0;
+    ctx->timer.n = 0;
+    ctx->timer.names.clear();
+    return TDV_OK;
+}
+
+int32_t tdv_ctx_timings(tdv_ctx* ctx, float* ms, int32_t max_entries) {
+    if (!ctx || !ctx->timer.on || ctx->timer.n < 2) return 0;
+    tdv::Timer& t = ctx->timer;
+    DeviceScope ds(ctx->device);
+    if (cudaEventSynchronize(t.ev[t.n - 1]) != cudaSuccess) return 0;
+    const int n = t.n - 1;
+    for (int i = 0; i < n && i < max_entries && ms; i++)
+        if (cudaEventElapsedTime(&ms[i], t.ev[i], t.ev[i + 1]) != cudaSuccess) ms[i] = -1.0f;
+    return n;
+}
+
+const char* tdv_ctx_timing_name(const tdv_ctx* ctx, int32_t i) {
+    if (!ctx || i < 0 || i >= (int32_t)ctx->timer.names.size()) return "";
+    return ctx->timer.names[i].c_str();
+}
+
+const char* tdv_last_error_string(const tdv_ctx* ctx) {
+    if (!ctx) return "null context";
+    return ctx->last_error.c_str();
+}
+
+tdv_status tdv_cost(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right,
+                    const tdv_cost_params* params, tdv_volume* out, tdv_stream stream) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    TDV_TRY(check_image(ctx, left, "left"));
+    TDV_TRY(check_image(ctx, right, "right"));
+    TDV_TRY(check_volume(ctx, out, "out"));
+    if (!params) return fail(ctx, TDV_ERR_INVALID_ARG, "null cost params");
+    if (params->kind < TDV_COST_BT || params->kind > TDV_COST_NCC)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "bad cost kind %d", params->kind);
+    if (params->kind != TDV_COST_BT && (params->radius < 0 || params->radius > 15))
+        return fail(ctx, TDV_ERR_INVALID_ARG, "window radius %d outside [0,15]", params->radius);
+    // The reference sizes the DSI to the smaller of the two images
+    // (tdvision/matchingcost.cpp:20-24).
+    const int W = std::min(left->width, right->width), H = std::min(left->height, right->height);
+    if (out->width != W || out->height != H)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "out volume %dx%d != min image size %dx%d", out->width,
+                    out->height, W, H);
+    TDV_DEVICE_SCOPE(ctx);
+    ctx->timer.begin(S(stream));
+    TDV_CUDA(tdv::launch_cost(tdv::make_img(*left), tdv::make_img(*right), params->kind,
+                              params->radius, tdv::make_vol(*out), S(stream), &ctx->timer));
+    return TDV_OK;
+}
+
+tdv_status tdv_sgm(tdv_ctx* ctx, const tdv_volume* cost, const tdv_image* guide,
+                   const tdv_sgm_params* params, tdv_volume* aggreg, tdv_disparity* out,
+                   tdv_stream stream) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    TDV_TRY(check_volume(ctx, cost, "cost"));
+    TDV_TRY(check_params(ctx, params));
+    TDV_TRY(check_out(ctx, out));
+    if (cost->depth > tdv::kMaxDispSgm)
+        return fail(ctx, TDV_ERR_UNSUPPORTED, "SGM supports D <= %d (got %d)", tdv::kMaxDispSgm,
+                    cost->depth);
+    if (params->p2_mode == TDV_P2_ADJUST && !guide)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "P2_ADJUST needs a guide image");
+    if (guide) {
+        TDV_TRY(check_image(ctx, guide, "guide"));
+        if (guide->width < cost->width || guide->height < cost->height)
+            return fail(ctx, TDV_ERR_INVALID_ARG, "guide smaller than the cost volume");
+    }
+    if (aggreg) {
+        TDV_TRY(check_volume(ctx, aggreg, "aggreg"));
+        if (aggreg->width != cost->width || aggreg->height != cost->height ||
+            aggreg->depth != cost->depth || aggreg->layout != cost->layout)
+            return fail(ctx, TDV_ERR_INVALID_ARG, "aggreg must match the cost volume's size and layout");
+        if (aggreg->ptr == cost->ptr) return fail(ctx, TDV_ERR_INVALID_ARG, "aggreg aliases cost");
+    }
+    TDV_DEVICE_SCOPE(ctx);
+    ctx->timer.begin(S(stream));
+    return run_sgm(ctx, cost, guide, params, aggreg, out, S(stream));
+}
+
+tdv_status tdv_wta(tdv_ctx* ctx, const tdv_volume* vol, tdv_disparity* out, tdv_stream stream) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    TDV_TRY(check_volume(ctx, vol, "vol"));
+    TDV_TRY(check_out(ctx, out));
+    if (out->lr_threshold >= 0 || out->disp_right) {
+        if (!out->disp) return fail(ctx, TDV_ERR_INVALID_ARG, "left-right check needs out->disp");
+    }
+    TDV_DEVICE_SCOPE(ctx);
+    VolArg V = tdv::make_vol(*vol);
+    ctx->timer.begin(S(stream));
+    TDV_CUDA(tdv::launch_wta(V, out->disp, out->disp_norm, S(stream), &ctx->timer));
+    if (out->lr_threshold >= 0 || out->disp_right)
+        TDV_CUDA(tdv::launch_lr(V, out->disp, out->disp_norm, out->disp_right,
+                                out->lr_threshold >= 0 ? out->lr_threshold : 0x7FFFFFFF, S(stream),
+                                &ctx->timer));
+    return TDV_OK;
+}
+
+tdv_status tdv_dp_scanline(tdv_ctx* ctx, const tdv_volume* cost, tdv_disparity* out,
+                           tdv_stream stream) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    TDV_TRY(check_volume(ctx, cost, "cost"));
+    TDV_TRY(check_out(ctx, out));
+    if (cost->depth > tdv::kMaxDispWide)
+        return fail(ctx, TDV_ERR_UNSUPPORTED, "DP supports D <= %d (got %d)", tdv::kMaxDispWide,
+                    cost->depth);
+    if (out->lr_threshold >= 0 || out->disp_right)
+        return fail(ctx, TDV_ERR_UNSUPPORTED, "DP has no left-right check");
+    TDV_DEVICE_SCOPE(ctx);
+    const size_t cb = (size_t)cost->width * cost->height * cost->depth;
+    TDV_TRY(ensure(ctx, ctx->codes, cb));
+    ctx->timer.begin(S(stream));
+    TDV_CUDA(tdv::launch_dp(tdv::make_vol(*cost), out->disp, out->disp_norm, ctx->codes.ptr, cb,
+                            S(stream), &ctx->timer));
+    return TDV_OK;
+}
+
+tdv_status tdv_fast_wta(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right, int32_t D,
+                        int32_t radius, tdv_disparity* out, tdv_stream stream) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    TDV_TRY(check_image(ctx, left, "left"));
+    TDV_TRY(check_image(ctx, right, "right"));
+    TDV_TRY(check_out(ctx, out));
+    if (D <= 0 || D > 65535) return fail(ctx, TDV_ERR_INVALID_ARG, "bad max_disp %d", D);
+    if (radius < 0 || radius > 15) return fail(ctx, TDV_ERR_INVALID_ARG, "bad radius %d", radius);
+    if (out->lr_threshold >= 0 || out->disp_right)
+        return fail(ctx, TDV_ERR_UNSUPPORTED, "fast WTA has no left-right check");
+    if (left->width != right->width || left->height != right->height)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "left and right images differ in size");
+    TDV_DEVICE_SCOPE(ctx);
+    ctx->timer.begin(S(stream));
+    TDV_CUDA(tdv::launch_fast_wta(tdv::make_img(*left), tdv::make_img(*right), D, radius, out->disp,
+                                  out->disp_norm, S(stream), &ctx->timer));
+    return TDV_OK;
+}
+
+tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right, int32_t D,
+                          const tdv_sgm_params* params, tdv_disparity* out, tdv_stream stream) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    TDV_TRY(check_image(ctx, left, "left"));
+    TDV_TRY(check_image(ctx, right, "right"));
+    TDV_TRY(check_params(ctx, params));
+    TDV_TRY(check_out(ctx, out));
+    if (D <= 0 || D > tdv::kMaxDispSgm)
+        return fail(ctx, TDV_ERR_UNSUPPORTED, "SGM supports 1 <= D <= %d (got %d)", tdv::kMaxDispSgm, D);
+    if (left->width != right->width || left->height != right->height)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "left and right images differ in size");
+    const int W = left->width, H = left->height;
+    ctx->timer.begin(S(stream));
+    const bool fused = left->dtype == TDV_U8 && right->dtype == TDV_U8 && left->scale == 1.0f &&
+                       right->scale == 1.0f && params->semantics == TDV_SEM_STANDARD &&
+                       params->table == TDV_TABLE_FULL && params->p2_mode == TDV_P2_CONST &&
+                       is_half_multiple(params->p1) && is_half_multiple(params->p2) &&
+                       2.0f * params->p2 <= 2560.0f && W >= 1 && H >= 1;
+    TDV_DEVICE_SCOPE(ctx);
+    if (fused) {
+        TDV_TRY(ensure(ctx, ctx->planes, tdv::fused_plane_bytes(W, H)));
+        TDV_TRY(ensure(ctx, ctx->agg, tdv::fused_agg_bytes(W, H, D)));
+        tdv::FusedArgs a;
+        a.L = tdv::make_img(*left);
+        a.R = tdv::make_img(*right);
+        a.W = W;
+        a.H = H;
+        a.D = D;
+        a.p1h = (int)(2.0f * params->p1);
+        a.p2h = (int)(2.0f * params->p2);
+        a.paths = params->paths;
+        a.disp = out->disp;
+        a.disp_norm = out->disp_norm;
+        a.disp_right = out->disp_right;
+        a.lr_thr = out->lr_threshold >= 0 ? out->lr_threshold : (out->disp_right ? 0x7FFFFFFF : -1);
+        a.planes = ctx->planes.ptr;
+        a.agg = ctx->agg.ptr;
+        TDV_CUDA(tdv::launch_fused(a, S(stream), &ctx->timer));
+        return TDV_OK;
+    }
+    // general path: BT cost DSI into scratch, then the float aggregation
+    TDV_TRY(ensure(ctx, ctx->cost, (size_t)W * H * D * sizeof(float)));
+    tdv_volume cv;
+    cv.ptr = ctx->cost.ptr;
+    cv.width = W;
+    cv.height = H;
+    cv.depth = D;
+    cv.layout = TDV_LAYOUT_HWD;
+    cv.dtype = TDV_F32;
+    TDV_CUDA(tdv::launch_cost(tdv::make_img(*left), tdv::make_img(*right), TDV_COST_BT, 0,
+                              tdv::make_vol(cv), S(stream), &ctx->timer));
+    return run_sgm(ctx, &cv, left, params, nullptr, out, S(stream));
+}
+
+}  // extern "C"

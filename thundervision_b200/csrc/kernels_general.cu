@@ -1,0 +1,450 @@
+// General (float32, any layout) kernels of the stage chain:
+//   cost DSI writers  (BT / SSD / NCC)
+//   SGM aggregation passes over a scheduled walk list (REF_CPU / REF_GPU /
+//     STANDARD semantics, constant or intensity-adjusted P2)
+//   WTA, left-right check, DP scanline, fused SSD+WTA.
+// Float arithmetic uses explicit round-to-nearest intrinsics wherever the
+// compiler could otherwise contract a multiply and an add, so each expression
+// rounds exactly as the C++ oracle (built with -ffp-contract=off) does.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include <cstdint>
+
+#include "tdv_internal.hpp"
+
+namespace tdv {
+
+namespace {
+
+__device__ __forceinline__ float img_at(const ImgArg& im, int x, int y) {
+    x = min(max(x, 0), im.W - 1);
+    y = min(max(y, 0), im.H - 1);
+    const size_t o = (size_t)y * im.pitch + x;
+    if (im.u8) return __fmul_rn((float)((const uint8_t*)im.ptr)[o], im.scale);
+    return __fmul_rn(((const float*)im.ptr)[o], im.scale);
+}
+
+// Birchfield-Tomasi dissimilarity, tdvision/birchfieldcost.cu:14-39.
+__device__ float bt_cell(const ImgArg& L, const ImgArg& R, int x, int y, int d) {
+    const float lI = img_at(L, x, y);
+    const float rI = img_at(R, x - d, y);
+    const float laI = __fmul_rn(0.5f, __fadd_rn(lI, img_at(L, x - 1, y)));
+    const float lbI = __fmul_rn(0.5f, __fadd_rn(lI, img_at(L, x + 1, y)));
+    const float raI = __fmul_rn(0.5f, __fadd_rn(rI, img_at(R, x - d - 1, y)));
+    const float rbI = __fmul_rn(0.5f, __fadd_rn(rI, img_at(R, x - d + 1, y)));
+    const float lImi = fminf(laI, fminf(lbI, lI));
+    const float lIma = fmaxf(laI, fmaxf(lbI, lI));
+    const float rImi = fminf(raI, fminf(rbI, rI));
+    const float rIma = fmaxf(raI, fmaxf(rbI, rI));
+    const float a = fmaxf(0.0f, fmaxf(__fsub_rn(lI, rIma), __fsub_rn(rImi, lI)));
+    const float b = fmaxf(0.0f, fmaxf(__fsub_rn(rI, lIma), __fsub_rn(lImi, rI)));
+    return __fadd_rn(0.0f, fminf(a, b));
+}
+
+// Window SSD, rows then columns, tdvision/ssd.cu:15-29.
+__device__ float ssd_cell(const ImgArg& L, const ImgArg& R, int x, int y, int d, int r) {
+    float sum = 0.0f;
+    for (int row = -r; row <= r; row++)
+        for (int col = -r; col <= r; col++) {
+            const float df = __fsub_rn(img_at(L, x + col, y + row), img_at(R, x + col - d, y + row));
+            sum = __fadd_rn(sum, __fmul_rn(df, df));
+        }
+    return sum;
+}
+
+// Un-centred normalised cross-correlation, tdvision/crosscorrelation.cu:11-28.
+__device__ float ncc_cell(const ImgArg& L, const ImgArg& R, int x, int y, int d, int r) {
+    float dom = 0.0f, ls = 0.0f, rs = 0.0f;
+    for (int row = -r; row <= r; row++)
+        for (int col = -r; col <= r; col++) {
+            const float lv = img_at(L, x + col, y + row);
+            const float rv = img_at(R, x + col - d, y + row);
+            dom = __fadd_rn(dom, __fmul_rn(lv, rv));
+            ls = __fadd_rn(ls, __fmul_rn(lv, lv));
+            rs = __fadd_rn(rs, __fmul_rn(rv, rv));
+        }
+    return __fsub_rn(1.0f, __fdiv_rn(dom, __fsqrt_rn(__fmul_rn(ls, rs))));
+}
+
+// One thread per cell in memory order (disparity fastest), so the DSI stores
+// are fully coalesced whatever the layout.
+__global__ void cost_kernel(ImgArg L, ImgArg R, int kind, int radius, VolArg out, int xmajor) {
+    const size_t n = (size_t)out.W * out.H * out.D;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int d = (int)(i % out.D);
+        const size_t p = i / out.D;
+        int x, y;
+        if (xmajor) { y = (int)(p % out.H); x = (int)(p / out.H); }
+        else { x = (int)(p % out.W); y = (int)(p / out.W); }
+        float v;
+        if (kind == TDV_COST_NCC) v = (d < x + 1) ? ncc_cell(L, R, x, y, d, radius) : CUDART_INF_F;
+        else if (x - d < 0) v = CUDART_INF_F;
+        else if (kind == TDV_COST_BT) v = bt_cell(L, R, x, y, d);
+        else v = ssd_cell(L, R, x, y, d, radius);
+        ((float*)out.ptr)[i] = v;
+    }
+}
+
+// Order-preserving float -> uint32 map for warp reductions with redux.sync;
+// NaN maps above +INF, so a minimum ignores NaN like fminf.
+__device__ __forceinline__ uint32_t ford(float f) {
+    const uint32_t u = __float_as_uint(f);
+    if (f != f) return 0xFFFFFFFFu;
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float fdeord(uint32_t o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
+}
+
+__device__ __forceinline__ float smin(float a, float b) { return (b < a) ? b : a; }
+
+// One warp per walk; lane l holds disparities [l*NPL, l*NPL+NPL).
+template <int NPL>
+__global__ void __launch_bounds__(128) sgm_pass_kernel(SgmArgs a, const Walk* __restrict__ walks,
+                                                       int nwalks, int dx, int dy, int first) {
+    const int lane = threadIdx.x & 31;
+    const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    if (w >= nwalks) return;
+    const Walk wk = walks[w];
+    const int D = a.C.D;
+    const int d0 = lane * NPL;
+    const bool refcpu = a.sem == TDV_SEM_REF_CPU;
+    const bool refgpu = a.sem == TDV_SEM_REF_GPU;
+    const int mlim = refcpu ? D - 1 : D;  // REF_CPU scans {sentinel, L(0..D-2)}
+    const float* C = (const float*)a.C.ptr;
+    float* S = (float*)a.S.ptr;
+
+    int x = wk.sx, y = wk.sy;
+    float L[NPL], c[NPL];
+    {
+        const float* cp = C + x * a.C.sx + y * a.C.sy;
+        float* sp = S + x * a.S.sx + y * a.S.sy;
+        uint32_t mo = 0xFFFFFFFFu;
+#pragma unroll
+        for (int j = 0; j < NPL; j++) {
+            const int d = d0 + j;
+            c[j] = d < D ? cp[d] : CUDART_INF_F;
+            if (d < mlim) mo = min(mo, ford(c[j]));
+            if (d < D) {
+                if (refcpu || first) {
+                    sp[d] = c[j];
+                } else {
+                    float acc = sp[d];
+                    for (int k = 0; k < wk.mult; k++) acc = __fadd_rn(acc, c[j]);
+                    sp[d] = acc;
+                }
+            }
+            L[j] = (refgpu && d < D) ? __fadd_rn(c[j], a.p1) : c[j];
+        }
+        // minimum over d with fminf semantics starting from +INF: NaN ignored,
+        // no candidate -> +INF
+        mo = __reduce_min_sync(0xFFFFFFFFu, mo);
+        float m = mo == 0xFFFFFFFFu ? CUDART_INF_F : fdeord(mo);
+        float lastI = a.has_guide ? img_at(a.guide, x, y) : 0.0f;
+
+        for (int t = 1; t < wk.len; t++) {
+            x += dx;
+            y += dy;
+            const float* cq = C + x * a.C.sx + y * a.C.sy;
+            float* sq = S + x * a.S.sx + y * a.S.sy;
+#pragma unroll
+            for (int j = 0; j < NPL; j++) {
+                const int d = d0 + j;
+                c[j] = d < D ? cq[d] : CUDART_INF_F;
+            }
+            float p2a = a.p2;
+            if (a.p2_adjust) {
+                const float I = img_at(a.guide, x, y);
+                p2a = __fdiv_rn(a.p2, fabsf(__fsub_rn(I, lastI)));
+                lastI = I;
+            }
+            const float mp2 = __fadd_rn(m, p2a);
+            float up = __shfl_up_sync(0xFFFFFFFFu, L[NPL - 1], 1);
+            float dn = __shfl_down_sync(0xFFFFFFFFu, L[0], 1);
+            if (lane == 0) up = CUDART_INF_F;
+            if (lane == 31) dn = CUDART_INF_F;
+            float Ln[NPL];
+            uint32_t mn_o = 0xFFFFFFFFu;
+#pragma unroll
+            for (int j = 0; j < NPL; j++) {
+                const int d = d0 + j;
+                const float lm = j > 0 ? L[j - 1] : up;
+                const float lp = j < NPL - 1 ? L[j + 1] : dn;
+                const float b = __fadd_rn(lm, a.p1);
+                const float e = __fadd_rn(lp, a.p1);
+                float mn;
+                if (refcpu) mn = smin(L[j], smin(b, smin(e, mp2)));
+                else mn = fminf(L[j], fminf(b, fminf(e, mp2)));
+                float v = __fsub_rn(__fadd_rn(c[j], mn), m);
+                if (d >= D) v = CUDART_INF_F;
+                Ln[j] = v;
+                if (d < mlim) mn_o = min(mn_o, ford(v));
+                if (d < D) {
+                    if (first) {
+                        sq[d] = v;
+                    } else {
+                        float acc = sq[d];
+                        for (int k = 0; k < wk.mult; k++) acc = __fadd_rn(acc, v);
+                        sq[d] = acc;
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NPL; j++) L[j] = Ln[j];
+            mn_o = __reduce_min_sync(0xFFFFFFFFu, mn_o);
+            m = mn_o == 0xFFFFFFFFu ? CUDART_INF_F : fdeord(mn_o);
+        }
+    }
+}
+
+template <int NPL>
+cudaError_t run_passes(const SgmArgs& a, const PassSchedule& sch, cudaStream_t st, Timer* tm) {
+    const int wpb = 4;
+    for (size_t p = 0; p < sch.passes.size(); p++) {
+        const Pass& ps = sch.passes[p];
+        const int nw = (int)ps.count;
+        const int blocks = (nw + wpb - 1) / wpb;
+        sgm_pass_kernel<NPL><<<blocks, wpb * 32, 0, st>>>(a, sch.d_walks + ps.first, nw, ps.dx, ps.dy,
+                                                          p == 0 ? 1 : 0);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (tm) tm->mark("sgm_pass");
+    }
+    return cudaSuccess;
+}
+
+__device__ __forceinline__ void argmin_merge(uint32_t& vo, int& vd, uint32_t o2, int d2) {
+    if (o2 < vo || (o2 == vo && d2 < vd)) { vo = o2; vd = d2; }
+}
+
+// Winner-take-all, one warp per pixel, strict '<' so the lowest d wins ties
+// (tdvision/wtacpu.cpp:14-39); NaN never wins; no finite value -> d = 0.
+__global__ void wta_kernel(VolArg V, uint16_t* disp, float* disp_norm) {
+    const int lane = threadIdx.x & 31;
+    const size_t npix = (size_t)V.W * V.H;
+    const float* base = (const float*)V.ptr;
+    for (size_t p = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < npix;
+         p += ((size_t)gridDim.x * blockDim.x) >> 5) {
+        const int x = (int)(p % V.W), y = (int)(p / V.W);
+        const float* vp = base + x * V.sx + y * V.sy;
+        uint32_t bo = ford(CUDART_INF_F);
+        int bd = 0x7FFFFFFF;
+        for (int d = lane; d < V.D; d += 32) {
+            const float v = vp[d];
+            if (v < CUDART_INF_F) argmin_merge(bo, bd, ford(v), d);
+        }
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            const uint32_t o2 = __shfl_xor_sync(0xFFFFFFFFu, bo, s);
+            const int d2 = __shfl_xor_sync(0xFFFFFFFFu, bd, s);
+            argmin_merge(bo, bd, o2, d2);
+        }
+        if (lane == 0) {
+            const int d = bd == 0x7FFFFFFF ? 0 : bd;
+            if (disp) disp[p] = (uint16_t)d;
+            if (disp_norm) disp_norm[p] = __fdiv_rn((float)d, (float)V.D);
+        }
+    }
+}
+
+// Left-right check, one block per row.  dR(xr) = argmin_d S(xr+d, y, d) over
+// xr+d < W; a left pixel is rejected (0xFFFF, d/D = -1) when x-dL < 0 or
+// |dL - dR(x-dL)| > thr.
+__global__ void lr_kernel(VolArg S, uint16_t* dispL, float* disp_norm, uint16_t* dispR, int thr) {
+    extern __shared__ uint16_t sdr[];
+    const int y = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const float* base = (const float*)S.ptr;
+    for (int xr = warp; xr < S.W; xr += nw) {
+        uint32_t bo = ford(CUDART_INF_F);
+        int bd = 0x7FFFFFFF;
+        for (int d = lane; d < S.D && xr + d < S.W; d += 32) {
+            const float v = base[(xr + d) * S.sx + y * S.sy + d];
+            if (v < CUDART_INF_F) argmin_merge(bo, bd, ford(v), d);
+        }
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            const uint32_t o2 = __shfl_xor_sync(0xFFFFFFFFu, bo, s);
+            const int d2 = __shfl_xor_sync(0xFFFFFFFFu, bd, s);
+            argmin_merge(bo, bd, o2, d2);
+        }
+        if (lane == 0) {
+            const uint16_t d = (uint16_t)(bd == 0x7FFFFFFF ? 0 : bd);
+            sdr[xr] = d;
+            if (dispR) dispR[(size_t)y * S.W + xr] = d;
+        }
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < S.W; x += blockDim.x) {
+        const size_t o = (size_t)y * S.W + x;
+        const int dl = dispL[o];
+        const int xr = x - dl;
+        if (xr < 0 || abs(dl - (int)sdr[xr]) > thr) {
+            dispL[o] = 0xFFFF;
+            if (disp_norm) disp_norm[o] = -1.0f;
+        }
+    }
+}
+
+// DP scanline, one warp per row (tdvision/dynamicprogcpu.cpp:13-62 recurrence,
+// tdvision/dynamicprog.cu:68-101 backtrack).  Choice codes (1 byte per cell,
+// -1/0/+1 stored as 0/1/2) go to scratch in [y][x][d] order.
+template <int NPL>
+__global__ void __launch_bounds__(128) dp_kernel(VolArg C, uint8_t* codes, uint16_t* disp,
+                                                 float* disp_norm) {
+    const int lane = threadIdx.x & 31;
+    const int y = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    if (y >= C.H) return;
+    const int D = C.D, W = C.W;
+    const int d0 = lane * NPL;
+    const float* base = (const float*)C.ptr;
+    uint8_t* crow = codes + (size_t)y * W * D;
+    float A[NPL];
+#pragma unroll
+    for (int j = 0; j < NPL; j++) {
+        const int d = d0 + j;
+        A[j] = d < D ? base[y * C.sy + d] : CUDART_INF_F;
+        if (d < D) crow[d] = 1;
+    }
+    for (int x = 1; x < W; x++) {
+        const float* cp = base + x * C.sx + y * C.sy;
+        float up = __shfl_up_sync(0xFFFFFFFFu, A[NPL - 1], 1);
+        float dn = __shfl_down_sync(0xFFFFFFFFu, A[0], 1);
+        if (lane == 0) up = CUDART_INF_F;
+        if (lane == 31) dn = CUDART_INF_F;
+        float An[NPL];
+#pragma unroll
+        for (int j = 0; j < NPL; j++) {
+            const int d = d0 + j;
+            const float c1 = j > 0 ? A[j - 1] : up;
+            const float c2 = A[j];
+            const float c3 = (j < NPL - 1 ? A[j + 1] : dn);
+            float m;
+            uint8_t code;
+            if (c1 < c2 && c1 < c3) { m = c1; code = 0; }
+            else if (c2 < c3) { m = c2; code = 1; }
+            else { m = c3; code = 2; }
+            if (d < D) {
+                An[j] = __fadd_rn(cp[d], m);
+                crow[(size_t)x * D + d] = code;
+            } else {
+                An[j] = CUDART_INF_F;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NPL; j++) A[j] = An[j];
+    }
+    // argmin of the last column, strict '<' from d = 0
+    uint32_t bo = 0xFFFFFFFFu;
+    int bd = 0x7FFFFFFF;
+#pragma unroll
+    for (int j = 0; j < NPL; j++) {
+        const int d = d0 + j;
+        if (d < D) argmin_merge(bo, bd, ford(A[j]), d);
+    }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        const uint32_t o2 = __shfl_xor_sync(0xFFFFFFFFu, bo, s);
+        const int d2 = __shfl_xor_sync(0xFFFFFFFFu, bd, s);
+        argmin_merge(bo, bd, o2, d2);
+    }
+    // The reference seeds its minimum with d = 0 of the last column and only a
+    // strictly smaller value replaces it, so a NaN there pins d = 0.
+    const bool nan0 = __shfl_sync(0xFFFFFFFFu, A[0] != A[0] ? 1 : 0, 0) != 0;
+    __syncwarp();
+    if (lane == 0) {
+        int z = (bd == 0x7FFFFFFF || nan0) ? 0 : bd;
+        for (int x = W - 1; x >= 0; x--) {
+            const int nz = z + (int)crow[(size_t)x * D + z] - 1;
+            if (nz >= 0 && nz < D) z = nz;
+            const size_t o = (size_t)y * W + x;
+            if (disp) disp[o] = (uint16_t)z;
+            if (disp_norm) disp_norm[o] = __fdiv_rn((float)z, (float)D);
+        }
+    }
+}
+
+// SSD window + argmin fused (tdvision/fastwta.cu:32-53), one thread per pixel.
+__global__ void fast_wta_kernel(ImgArg L, ImgArg R, int D, int r, uint16_t* disp, float* disp_norm) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= L.W || y >= L.H) return;
+    float best = CUDART_INF_F;
+    int bd = 0;
+    const int nd = min(D, x + 1);
+    for (int d = 0; d < nd; d++) {
+        const float v = ssd_cell(L, R, x, y, d, r);
+        if (v < best) { best = v; bd = d; }
+    }
+    const size_t o = (size_t)y * L.W + x;
+    if (disp) disp[o] = (uint16_t)bd;
+    if (disp_norm) disp_norm[o] = __fdiv_rn((float)bd, (float)D);
+}
+
+int grid_for(size_t n, int block) {
+    size_t g = (n + block - 1) / block;
+    if (g > (size_t)148 * 64) g = (size_t)148 * 64;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+}  // namespace
+
+cudaError_t launch_cost(const ImgArg& L, const ImgArg& R, int kind, int radius, const VolArg& out,
+                        cudaStream_t st, Timer* tm) {
+    const size_t n = (size_t)out.W * out.H * out.D;
+    const int xmajor = out.sx > out.sy ? 1 : 0;
+    cost_kernel<<<grid_for(n, 256), 256, 0, st>>>(L, R, kind, radius, out, xmajor);
+    if (tm) tm->mark("cost");
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sgm_passes(const SgmArgs& a, const PassSchedule& sch, cudaStream_t st, Timer* tm) {
+    const int D = a.C.D;
+    if (D <= 32) return run_passes<1>(a, sch, st, tm);
+    if (D <= 64) return run_passes<2>(a, sch, st, tm);
+    if (D <= 128) return run_passes<4>(a, sch, st, tm);
+    return run_passes<8>(a, sch, st, tm);
+}
+
+cudaError_t launch_wta(const VolArg& V, uint16_t* disp, float* disp_norm, cudaStream_t st, Timer* tm) {
+    const size_t npix = (size_t)V.W * V.H;
+    wta_kernel<<<grid_for(npix * 32, 256), 256, 0, st>>>(V, disp, disp_norm);
+    if (tm) tm->mark("wta");
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lr(const VolArg& S, uint16_t* dispL, float* disp_norm, uint16_t* dispR, int thr,
+                      cudaStream_t st, Timer* tm) {
+    lr_kernel<<<S.H, 256, S.W * sizeof(uint16_t), st>>>(S, dispL, disp_norm, dispR, thr);
+    if (tm) tm->mark("lr_check");
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dp(const VolArg& C, uint16_t* disp, float* disp_norm, void* codes,
+                      size_t codes_bytes, cudaStream_t st, Timer* tm) {
+    (void)codes_bytes;
+    const int blocks = (C.H + 3) / 4;
+    const int D = C.D;
+    uint8_t* cd = (uint8_t*)codes;
+    if (D <= 32) dp_kernel<1><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+    else if (D <= 64) dp_kernel<2><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+    else if (D <= 128) dp_kernel<4><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+    else if (D <= 256) dp_kernel<8><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+    else if (D <= 512) dp_kernel<16><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+    else dp_kernel<32><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+    if (tm) tm->mark("dp_scanline");
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fast_wta(const ImgArg& L, const ImgArg& R, int D, int radius, uint16_t* disp,
+                            float* disp_norm, cudaStream_t st, Timer* tm) {
+    dim3 blk(16, 16), grd((L.W + 15) / 16, (L.H + 15) / 16);
+    fast_wta_kernel<<<grd, blk, 0, st>>>(L, R, D, radius, disp, disp_norm);
+    if (tm) tm->mark("fast_wta");
+    return cudaGetLastError();
+}
+
+}  // namespace tdv

@@ -1,0 +1,159 @@
+// Internal declarations shared by the C-ABI host code and the kernel files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/tdv_stereo.h"
+
+namespace tdv {
+
+// Largest disparity range handled by the SGM / WTA kernels (8 values per lane
+// of one warp for fp32 paths = 256, the reference's SG_MAX_DISP,
+// tdvision/semiglobal.cu:44; the DP and WTA kernels take up to 1024).
+constexpr int kMaxDispSgm = 256;
+constexpr int kMaxDispWide = 1024;
+
+// One walk of an aggregation pass: start cell, number of cells, and how many
+// identical walks the reference table issues back to back (REF tables repeat
+// some reverse diagonals).
+struct Walk {
+    int32_t sx, sy, len, mult;
+};
+
+// An ordered aggregation pass: all walks share one direction and touch
+// disjoint cells, so they run concurrently while every cell still sees the
+// reference's per-cell order of updates.
+struct Pass {
+    int dx, dy;
+    size_t first, count;  // range in the device walk array
+};
+
+struct PassSchedule {
+    int W = 0, H = 0, table = -1, paths = 0;
+    std::vector<Pass> passes;
+    std::vector<Walk> walks;  // host copy
+    Walk* d_walks = nullptr;  // device copy (ctx scratch)
+};
+
+// Optional per-kernel timing: events recorded on the launch stream before the
+// first and after every kernel of one ABI call.
+struct Timer {
+    bool on = false;
+    std::vector<cudaEvent_t> ev;
+    std::vector<std::string> names;
+    int n = 0;
+    cudaStream_t st = nullptr;
+    void begin(cudaStream_t s) {
+        if (!on) return;
+        n = 0;
+        names.clear();
+        st = s;
+        rec();
+    }
+    void mark(const char* name) {
+        if (!on) return;
+        names.emplace_back(name);
+        rec();
+    }
+    void rec() {
+        if (n >= (int)ev.size()) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return;
+            ev.push_back(e);
+        }
+        cudaEventRecord(ev[n++], st);
+    }
+};
+
+// Builds the reference's path table (tdvision/semiglobal.cu:57-230) or its
+// corrected FULL variant and schedules it into passes; see paths.cpp.
+// Returns false (and schedules nothing usable) if a walk leaves the image.
+bool build_schedule(int W, int H, int table, int paths, PassSchedule& out);
+
+}  // namespace tdv
+
+struct tdv_ctx {
+    int device = 0;
+    bool device_set = false;
+    std::string last_error;
+    tdv_alloc_fn alloc = nullptr;
+    tdv_free_fn release = nullptr;
+    void* alloc_user = nullptr;
+
+    // scratch buffers, grown on demand
+    struct Buf {
+        void* ptr = nullptr;
+        size_t bytes = 0;
+    };
+    Buf agg;      // aggregation volume
+    Buf cost;     // cost DSI for tdv_stereo_sgm's general path
+    Buf planes;   // fused path: left/right BT planes
+    Buf codes;    // DP choice codes
+    Buf misc;     // small per-call scratch
+
+    tdv::PassSchedule sched;
+    Buf sched_buf;
+    tdv::Timer timer;
+};
+
+namespace tdv {
+
+// ---- kernel launchers (defined in the .cu kernel files) ----------------
+
+struct ImgArg {
+    const void* ptr;
+    int W, H, pitch;
+    int u8;  // 1: uint8, 0: float
+    float scale;
+};
+
+struct VolArg {
+    void* ptr;
+    int W, H, D;
+    long long sx, sy;  // element strides of the pixel (x, y)
+};
+
+VolArg make_vol(const tdv_volume& v);
+ImgArg make_img(const tdv_image& im);
+
+cudaError_t launch_cost(const ImgArg& L, const ImgArg& R, int kind, int radius, const VolArg& out,
+                        cudaStream_t st, Timer* tm);
+
+struct SgmArgs {
+    VolArg C, S;
+    ImgArg guide;
+    int has_guide;
+    float p1, p2;
+    int p2_adjust, sem;
+};
+cudaError_t launch_sgm_passes(const SgmArgs& a, const PassSchedule& sch, cudaStream_t st, Timer* tm);
+cudaError_t launch_wta(const VolArg& V, uint16_t* disp, float* disp_norm, cudaStream_t st, Timer* tm);
+cudaError_t launch_lr(const VolArg& S, uint16_t* dispL, float* disp_norm, uint16_t* dispR,
+                      int thr, cudaStream_t st, Timer* tm);
+cudaError_t launch_dp(const VolArg& C, uint16_t* disp, float* disp_norm, void* codes_scratch,
+                      size_t codes_bytes, cudaStream_t st, Timer* tm);
+cudaError_t launch_fast_wta(const ImgArg& L, const ImgArg& R, int D, int radius, uint16_t* disp,
+                            float* disp_norm, cudaStream_t st, Timer* tm);
+
+// Fused integer-domain BT + SGM + WTA (+ left-right check).
+struct FusedArgs {
+    ImgArg L, R;
+    int W, H, D;
+    int p1h, p2h;  // penalties in half-units (2*P)
+    int paths;
+    uint16_t* disp;
+    float* disp_norm;
+    uint16_t* disp_right;
+    int lr_thr;
+    void* planes;  // 2 * W*H*16 bytes
+    void* agg;     // W*H*Dp*2 bytes
+};
+size_t fused_agg_bytes(int W, int H, int D);
+size_t fused_plane_bytes(int W, int H);
+cudaError_t launch_fused(const FusedArgs& a, cudaStream_t st, Timer* tm);
+
+}  // namespace tdv
