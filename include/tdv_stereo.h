@@ -162,6 +162,10 @@ tdv_status tdv_ctx_set_allocator(tdv_ctx* ctx, tdv_alloc_fn alloc, tdv_free_fn r
 /* Pre-sizes scratch for pairs up to W x H x D so later calls do not allocate. */
 tdv_status tdv_ctx_reserve(tdv_ctx* ctx, int32_t width, int32_t height, int32_t max_disp);
 const char* tdv_last_error_string(const tdv_ctx* ctx);
+/* Synchronises `stream` and returns the error status kernels of this
+ * context recorded on the device (TDV_ERR_TIMEOUT when a bounded wait inside
+ * a kernel ran out), clearing it; TDV_OK if none. */
+tdv_status tdv_ctx_device_status(tdv_ctx* ctx, tdv_stream stream);
 /* Per-kernel timing: when enabled, every kernel a call launches is bracketed
  * by CUDA events on the call's stream; tdv_ctx_timings then returns (after the
  * stream has been synchronised) the device milliseconds of each launch of the

@@ -27,7 +27,7 @@ EXPORTS = [
     "tdv_cost", "tdv_sgm", "tdv_wta", "tdv_dp_scanline", "tdv_fast_wta", "tdv_stereo_sgm",
     "tdv_ctx_create", "tdv_ctx_destroy", "tdv_ctx_set_allocator", "tdv_ctx_reserve",
     "tdv_last_error_string", "tdv_status_string", "tdv_version", "tdv_volume_bytes",
-    "tdv_ctx_enable_timing", "tdv_ctx_timings", "tdv_ctx_timing_name",
+    "tdv_ctx_enable_timing", "tdv_ctx_timings", "tdv_ctx_timing_name", "tdv_ctx_device_status",
 ]
 
 
@@ -92,6 +92,7 @@ def _declare(lib):
         "tdv_ctx_enable_timing": (st, [vp, ctypes.c_int32]),
         "tdv_ctx_timings": (ctypes.c_int32, [vp, P(ctypes.c_float), ctypes.c_int32]),
         "tdv_ctx_timing_name": (ctypes.c_char_p, [vp, ctypes.c_int32]),
+        "tdv_ctx_device_status": (st, [vp, vp]),
         "tdv_volume_bytes": (ctypes.c_size_t, [ctypes.c_int32] * 4),
     }
     for name, (res, args) in sig.items():

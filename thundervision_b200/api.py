@@ -90,6 +90,10 @@ class Context:
             msg = L.lib().tdv_last_error_string(self.handle).decode()
             raise L.TdvError(status, msg)
 
+    def device_status(self):
+        """Synchronise and raise if a kernel recorded an error (e.g. a timed-out wait)."""
+        self.check(L.lib().tdv_ctx_device_status(self.handle, _stream()))
+
     def reserve(self, W, H, D):
         self.check(L.lib().tdv_ctx_reserve(self.handle, W, H, D))
 

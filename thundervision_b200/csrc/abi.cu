@@ -149,6 +149,14 @@ void release_buf(tdv_ctx* ctx, tdv_ctx::Buf& b) {
 
 cudaStream_t S(tdv_stream s) { return (cudaStream_t)s; }
 
+// The device error word is allocated (and zeroed) once per context.
+tdv_status ensure_err(tdv_ctx* ctx, cudaStream_t st) {
+    if (ctx->err.ptr) return TDV_OK;
+    TDV_TRY(ensure(ctx, ctx->err, 16));
+    TDV_CUDA(cudaMemsetAsync(ctx->err.ptr, 0, 16, st));
+    return TDV_OK;
+}
+
 tdv_status ensure_schedule(tdv_ctx* ctx, int W, int H, int table, int paths, cudaStream_t st) {
     tdv::PassSchedule& sc = ctx->sched;
     if (sc.W == W && sc.H == H && sc.table == table && sc.paths == paths && sc.d_walks) return TDV_OK;
@@ -275,7 +283,7 @@ tdv_status tdv_ctx_create(int32_t device, tdv_ctx** out) {
 void tdv_ctx_destroy(tdv_ctx* ctx) {
     if (!ctx) return;
     const bool any = ctx->agg.ptr || ctx->cost.ptr || ctx->planes.ptr || ctx->codes.ptr ||
-                     ctx->misc.ptr || ctx->sched_buf.ptr;
+                     ctx->misc.ptr || ctx->sched_buf.ptr || ctx->err.ptr;
     if (any) {
         DeviceScope ds(ctx->device);
         cudaDeviceSynchronize();
@@ -285,6 +293,7 @@ void tdv_ctx_destroy(tdv_ctx* ctx) {
         release_buf(ctx, ctx->codes);
         release_buf(ctx, ctx->misc);
         release_buf(ctx, ctx->sched_buf);
+        release_buf(ctx, ctx->err);
     }
     if (!ctx->timer.ev.empty()) {
         DeviceScope ds(ctx->device);
@@ -345,6 +354,20 @@ int32_t tdv_ctx_timings(tdv_ctx* ctx, float* ms, int32_t max_entries) {
 const char* tdv_ctx_timing_name(const tdv_ctx* ctx, int32_t i) {
     if (!ctx || i < 0 || i >= (int32_t)ctx->timer.names.size()) return "";
     return ctx->timer.names[i].c_str();
+}
+
+tdv_status tdv_ctx_device_status(tdv_ctx* ctx, tdv_stream stream) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    if (!ctx->err.ptr) return TDV_OK;
+    TDV_DEVICE_SCOPE(ctx);
+    int v = 0;
+    TDV_CUDA(cudaMemcpyAsync(&v, ctx->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
+    TDV_CUDA(cudaStreamSynchronize(S(stream)));
+    if (v != 0) {
+        TDV_CUDA(cudaMemsetAsync(ctx->err.ptr, 0, sizeof(int), S(stream)));
+        return fail(ctx, (tdv_status)v, "a kernel reported %s", tdv_status_string((tdv_status)v));
+    }
+    return TDV_OK;
 }
 
 const char* tdv_last_error_string(const tdv_ctx* ctx) {
@@ -498,6 +521,8 @@ tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* 
         a.lr_thr = out->lr_threshold >= 0 ? out->lr_threshold : (out->disp_right ? 0x7FFFFFFF : -1);
         a.planes = ctx->planes.ptr;
         a.agg = ctx->agg.ptr;
+        TDV_TRY(ensure_err(ctx, S(stream)));
+        a.err = (int*)ctx->err.ptr;
         TDV_CUDA(tdv::launch_fused(a, S(stream), &ctx->timer));
         return TDV_OK;
     }

@@ -4,7 +4,7 @@
 //
 // Exactness.  In this domain every BT cost is a multiple of 1/2 in [0, 255]
 // and every path cost L = C + min(...) - m' lies in [0, 255 + P2], so all
-// quantities are small multiples of 1/2.  The kernel carries them as unsigned
+// quantities are small multiples of 1/2.  The kernels carry them as unsigned
 // 16-bit "half-units" (2x the value), two disparities per 32-bit register.
 // Integer arithmetic on these is exact, so the result is bit-identical to the
 // float32 recurrence of the reference (tdvision/semiglobalcpu.cpp:104-122)
@@ -14,14 +14,27 @@
 // every invalid S in [8*BIG, 8*(BIG + P2h)] <= 65535, above any valid S.
 //
 // Data flow per frame (8 paths):
-//   prep : BT planes for both images (I, half-sample min, half-sample max).
-//   pass : V+ V- D1+ D1- D2+ D2- H+ H-, one warp per path line; lanes own
-//          consecutive disparities; d-1/d+1 neighbours by byte permutes plus
-//          one shuffle each way; min over d by redux.sync.  The first pass
-//          stores S, the middle ones read-modify-write it, the last (H-)
-//          reads it, finishes S in registers and reduces it to the disparity
-//          (and the right-view disparity for the left-right check) without
-//          storing it.  S lives in HBM as [y][x][d] u16, 64*PPL d per pixel.
+//   prep : BT planes of both images (I, half-sample min, half-sample max in
+//          half-units).  The right plane stores, at pixel x, the values of x
+//          and x-1 so the disparity pair (d, d+1) of left column x reads one
+//          16-byte entry; rows are padded with one 16-byte slot after every 8
+//          entries so that lanes reading entries 8 apart hit distinct banks.
+//   pass : V+ V- D1+ D1- D2+ D2- H+ H-.  Lanes own consecutive disparity
+//          pairs; d-1/d+1 neighbours by byte permutes plus one shuffle each
+//          way; u16x2 min/max; min over d by redux.sync.  The aggregation
+//          volume S ([y][x][64*PPL] u16 in HBM) is stored by the first pass,
+//          read-modify-written by the middle ones and read by the last (H-),
+//          which finishes S in registers and reduces it to disparities (WTA,
+//          right-view disparity, left-right check) without storing it.
+//   Vertical and diagonal passes run row-synchronous blocks: G warps own G
+//   adjacent path lines and advance one image row per step; per row one
+//   thread issues TMA bulk copies (cp.async.bulk) of the S chunk, the left
+//   plane entries and the shared right-plane segment into a ring of shared
+//   memory slots completed by mbarriers.  Horizontal passes give each warp a
+//   row, an S ring and a sliding window of right-plane chunks, also filled by
+//   TMA bulk copies.  Every mbarrier wait is bounded; a wait that runs out
+//   records TDV_ERR_TIMEOUT, waits (bounded) for its copies in flight and
+//   returns.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -32,14 +45,28 @@ namespace tdv {
 
 namespace {
 
-constexpr int kWarps = 4;   // warps (= path lines) per block
-constexpr int kLook = 4;    // S loads issued this many steps ahead
-constexpr int kRing = 256;  // right-disparity ring per warp (>= max D)
+constexpr int kMaxG = 16;       // warps per block, vertical/diagonal passes
+constexpr int kRowSlots = 6;    // ring depth (rows), vertical/diagonal passes
+constexpr int kMaxGH = 8;       // warps per block, horizontal passes
+constexpr int kHSlots = 8;      // S ring depth (steps), horizontal passes
+constexpr int kChunk = 64;      // right-plane entries per horizontal refill
+constexpr int kChunkSlots = 8;  // resident chunks per horizontal warp
+constexpr int kLookC = 2;       // chunks fetched ahead of need
+constexpr int kRing = 256;      // right-disparity ring per warp (>= max D)
+constexpr uint32_t kSpin = 1u << 22;
+constexpr int kGroupBytes = 9 * 16;
+constexpr int kChunkBytes = (kChunk / 8) * kGroupBytes;
+constexpr uint32_t FULL = 0xFFFFFFFFu;
 
 struct __align__(16) Plane {
     uint32_t i, mn, mx, pad;
 };
 
+__host__ __device__ inline int padded_len(int W) { return 9 * ((W + 7) / 8); }
+__device__ __forceinline__ int ppos(int e) { return e + (e >> 3); }
+__host__ __device__ inline int align128(int v) { return (v + 127) & ~127; }
+
+// ---------------------------------------------------------------- PTX
 __device__ __forceinline__ uint32_t vmin2(uint32_t a, uint32_t b) {
     uint32_t r;
     asm("min.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
@@ -50,11 +77,51 @@ __device__ __forceinline__ uint32_t vmax2(uint32_t a, uint32_t b) {
     asm("max.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
     return r;
 }
-__device__ __forceinline__ uint32_t hi_lo(uint32_t a, uint32_t b) {
-    // (hi16(a), lo16(b)) as (lo, hi) of the result
-    return __byte_perm(a, b, 0x5432);
+// (hi16(a), lo16(b)) as (lo, hi) of the result
+__device__ __forceinline__ uint32_t hi_lo(uint32_t a, uint32_t b) { return __byte_perm(a, b, 0x5432); }
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+// 1-D TMA bulk copy global -> shared, completion counted on `bar`.
+__device__ __forceinline__ void tma_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for phase `parity` of `bar`; false when the bound runs out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t it = 0; it < kSpin; it++)
+        if (mbar_try(bar, parity)) return true;
+    return false;
 }
 
+// ---------------------------------------------------------------- planes
 __device__ __forceinline__ int u8_at(const ImgArg& im, int x, int y) {
     x = min(max(x, 0), im.W - 1);
     y = min(max(y, 0), im.H - 1);
@@ -73,7 +140,7 @@ __device__ __forceinline__ void bt_triple(const ImgArg& im, int x, int y, uint32
     mx = max(2 * v, max(a, b));
 }
 
-__global__ void prep_kernel(ImgArg L, ImgArg R, Plane* LP, Plane* RP, int W, int H) {
+__global__ void prep_kernel(ImgArg L, ImgArg R, Plane* LP, Plane* RPp, int W, int H, int Wp) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= W) return;
@@ -85,8 +152,6 @@ __global__ void prep_kernel(ImgArg L, ImgArg R, Plane* LP, Plane* RP, int W, int
     lp.mx = mx * 0x10001u;
     lp.pad = 0;
     LP[(size_t)y * W + x] = lp;
-    // right plane at xr packs (value at xr, value at xr-1): the pair of
-    // disparities (d, d+1) seen from left column x reads RP[x-d].
     uint32_t j2, jn, jx, k2, kn, kx;
     bt_triple(R, x, y, j2, jn, jx);
     bt_triple(R, max(x - 1, 0), y, k2, kn, kx);
@@ -95,99 +160,67 @@ __global__ void prep_kernel(ImgArg L, ImgArg R, Plane* LP, Plane* RP, int W, int
     rp.mn = jn | (kn << 16);
     rp.mx = jx | (kx << 16);
     rp.pad = 0;
-    RP[(size_t)y * W + x] = rp;
+    RPp[(size_t)y * Wp + x + (x >> 3)] = rp;
 }
 
 struct FK {
     const Plane* LP;
-    const Plane* RP;
-    uint32_t* S;  // pairs
-    int W, H, D, Dp2;  // Dp2 = u32 pairs per pixel
+    const Plane* RPp;  // padded rows of Wp entries
+    uint32_t* S;       // aggregation volume, u16 pairs
+    int W, H, D, Dp2, Wp;
     uint32_t P1P1, P2P2, BIGBIG;
     uint16_t* disp;
     float* disp_norm;
     uint16_t* disp_right;
     int lr_thr;
+    int* err;
 };
 
-__device__ __forceinline__ void walk_geom(int i, int dx, int dy, int W, int H, int& sx, int& sy,
-                                          int& len) {
-    if (dy == 0) {
-        sy = i;
-        sx = dx > 0 ? 0 : W - 1;
-        len = W;
-        return;
-    }
-    if (dx == 0) {
-        sx = i;
-        sy = dy > 0 ? 0 : H - 1;
-        len = H;
-        return;
-    }
-    const int ye = dy > 0 ? 0 : H - 1;
-    const int xe = dx > 0 ? 0 : W - 1;
-    if (i < W) {
-        sx = i;
-        sy = ye;
-    } else {
-        sx = xe;
-        sy = ye + dy * (i - W + 1);
-    }
-    const int nx = dx > 0 ? W - sx : sx + 1;
-    const int ny = dy > 0 ? H - sy : sy + 1;
-    len = min(nx, ny);
-}
-
+// ---------------------------------------------------------------- compute
 template <int PPL>
 struct Vec;
 template <>
 struct Vec<1> {
-    static __device__ __forceinline__ void ld(const uint32_t* p, uint32_t* v) { v[0] = __ldcs(p); }
     static __device__ __forceinline__ void st(uint32_t* p, const uint32_t* v) { __stcs(p, v[0]); }
+    static __device__ __forceinline__ void lds(const uint32_t* p, uint32_t* v) { v[0] = p[0]; }
 };
 template <>
 struct Vec<2> {
-    static __device__ __forceinline__ void ld(const uint32_t* p, uint32_t* v) {
-        const uint2 t = __ldcs((const uint2*)p);
-        v[0] = t.x;
-        v[1] = t.y;
-    }
     static __device__ __forceinline__ void st(uint32_t* p, const uint32_t* v) {
         __stcs((uint2*)p, make_uint2(v[0], v[1]));
+    }
+    static __device__ __forceinline__ void lds(const uint32_t* p, uint32_t* v) {
+        const uint2 t = *(const uint2*)p;
+        v[0] = t.x;
+        v[1] = t.y;
     }
 };
 template <>
 struct Vec<4> {
-    static __device__ __forceinline__ void ld(const uint32_t* p, uint32_t* v) {
-        const uint4 t = __ldcs((const uint4*)p);
+    static __device__ __forceinline__ void st(uint32_t* p, const uint32_t* v) {
+        __stcs((uint4*)p, make_uint4(v[0], v[1], v[2], v[3]));
+    }
+    static __device__ __forceinline__ void lds(const uint32_t* p, uint32_t* v) {
+        const uint4 t = *(const uint4*)p;
         v[0] = t.x;
         v[1] = t.y;
         v[2] = t.z;
         v[3] = t.w;
     }
-    static __device__ __forceinline__ void st(uint32_t* p, const uint32_t* v) {
-        __stcs((uint4*)p, make_uint4(v[0], v[1], v[2], v[3]));
-    }
 };
 
-// BT costs (half-units) of this lane's disparity pairs at left pixel (x, y).
-template <int PPL>
-__device__ __forceinline__ void bt_pairs(const FK& k, int x, int y, int base, uint32_t* c) {
-    const uint4 lp = __ldg((const uint4*)&k.LP[(size_t)y * k.W + x]);
-    const Plane* rrow = k.RP + (size_t)y * k.W;
-    const int lim = min(x + 1, k.D);  // valid d < lim
-#pragma unroll
-    for (int q = 0; q < PPL; q++) {
-        const int d = base + 2 * q;
-        const int xr = max(x - d, 0);
-        const uint4 rp = __ldg((const uint4*)&rrow[xr]);
-        // .x = I, .y = half-sample min, .z = half-sample max
-        const uint32_t A = vmax2(lp.x, rp.y) - vmin2(lp.x, rp.z);
-        const uint32_t B = vmax2(rp.x, lp.y) - vmin2(rp.x, lp.z);
-        uint32_t v = vmin2(A, B);
-        if (d + 1 >= lim) v = (d < lim) ? ((v & 0xFFFFu) | (k.BIGBIG & 0xFFFF0000u)) : k.BIGBIG;
-        c[q] = v;
-    }
+// BT of one disparity pair from a left entry and a right entry.
+__device__ __forceinline__ uint32_t bt_pair(const uint4& lp, const uint4& rp) {
+    // .x = I, .y = half-sample min, .z = half-sample max
+    const uint32_t A = vmax2(lp.x, rp.y) - vmin2(lp.x, rp.z);
+    const uint32_t B = vmax2(rp.x, lp.y) - vmin2(rp.x, lp.z);
+    return vmin2(A, B);
+}
+
+// Invalid halves (d > x or d >= D) carry BIG.
+__device__ __forceinline__ uint32_t mask_pair(uint32_t v, int d, int lim, uint32_t BIGBIG) {
+    if (d + 1 >= lim) v = (d < lim) ? ((v & 0xFFFFu) | (BIGBIG & 0xFFFF0000u)) : BIGBIG;
+    return v;
 }
 
 template <int PPL>
@@ -196,143 +229,352 @@ __device__ __forceinline__ uint32_t warp_min_pairs(const uint32_t* L) {
 #pragma unroll
     for (int q = 1; q < PPL; q++) t = vmin2(t, L[q]);
     t = min(t & 0xFFFFu, t >> 16);
-    return __reduce_min_sync(0xFFFFFFFFu, t);
+    return __reduce_min_sync(FULL, t);
 }
 
-// MODE 0: first pass (store S); 1: middle pass (S += L); 2: last pass (final
-// S -> WTA, optional left-right check; only launched for H-).
-template <int PPL, int MODE>
-__global__ void __launch_bounds__(kWarps * 32) fused_pass(FK k, int dx, int dy, int nwalks) {
-    extern __shared__ uint32_t smem[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int walk = blockIdx.x * kWarps + warp;
-    if (walk >= nwalks) return;
-    int sx, sy, len;
-    walk_geom(walk, dx, dy, k.W, k.H, sx, sy, len);
-    const int base = lane * 2 * PPL;
+// One step of the min-plus recurrence for this lane's pairs.
+template <int PPL>
+__device__ __forceinline__ void recur(const uint32_t* L, uint32_t m, const uint32_t* c, uint32_t* Ln,
+                                      int lane, const FK& k) {
+    const uint32_t MM = m * 0x10001u;
+    const uint32_t MP2 = MM + k.P2P2;
+    uint32_t up = __shfl_up_sync(FULL, L[PPL - 1], 1);
+    uint32_t dn = __shfl_down_sync(FULL, L[0], 1);
+    if (lane == 0) up = k.BIGBIG;
+    if (lane == 31) dn = k.BIGBIG;
+#pragma unroll
+    for (int q = 0; q < PPL; q++) {
+        const uint32_t lm = hi_lo(q > 0 ? L[q - 1] : up, L[q]);
+        const uint32_t lp = hi_lo(L[q], q < PPL - 1 ? L[q + 1] : dn);
+        uint32_t tv = vmin2(lm, lp) + k.P1P1;
+        tv = vmin2(vmin2(tv, L[q]), MP2);
+        Ln[q] = tv + c[q] - MM;
+    }
+}
 
-    const bool lr = MODE == 2 && k.lr_thr >= 0;
-    uint32_t* ring = smem + warp * kRing;
-    uint16_t* rowL = (uint16_t*)(smem + kWarps * kRing) + (size_t)warp * 2 * k.W;
-    uint16_t* rowR = rowL + k.W;
-    if (lr) {
-        for (int i = lane; i < kRing; i += 32) ring[i] = 0xFFFFFFFFu;
-        __syncwarp();
+// ---------------------------------------------- vertical / diagonal passes
+// A path line is x = kp + s*y (s = dx*dy); the block owns lines
+// j0 .. j0+G-1 (kp = kmin + j) and walks rows in the pass direction dy.
+template <int PPL, int MODE>
+__global__ void __launch_bounds__(kMaxG * 32, 1)
+    vd_pass(FK k, int s, int dy, int kmin, int nlines, int G, int nslots) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int SB = 128 * PPL;
+    constexpr int DSPAN = 64 * PPL;
+    const int NRG = (G + DSPAN) / 8 + 2;
+    const int offL = G * SB, offR = offL + G * 16;
+    const int slotBytes = align128(offR + NRG * kGroupBytes);
+    uint64_t* bars = (uint64_t*)smem;
+    unsigned char* slots = smem + 128;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int j0 = blockIdx.x * G;
+    const int Gb = min(G, nlines - j0);
+    const int kf = kmin + j0;
+    int ylo, yhi;
+    if (s == 0) {
+        ylo = 0;
+        yhi = k.H - 1;
+    } else if (s > 0) {
+        ylo = max(0, -(kf + Gb - 1));
+        yhi = min(k.H - 1, k.W - 1 - kf);
+    } else {
+        ylo = max(0, kf - k.W + 1);
+        yhi = min(k.H - 1, kf + Gb - 1);
+    }
+    const int nrows = yhi - ylo + 1;
+    if (nrows <= 0) return;  // uniform for the block
+
+    auto row_of = [&](int i) { return dy > 0 ? ylo + i : yhi - i; };
+    auto issue = [&](int i) {
+        const int y = row_of(i);
+        const int xf = kf + s * y;
+        const int xlo = max(xf, 0), xhi = min(xf + Gb, k.W);
+        const int npx = xhi - xlo;
+        const int g0 = max(0, xlo - DSPAN + 2) >> 3, g1 = (xhi - 1) >> 3;
+        unsigned char* base = slots + (i % nslots) * slotBytes;
+        const uint32_t bar = smem_u32(&bars[i % nslots]);
+        const uint32_t sb = MODE != 0 ? (uint32_t)npx * SB : 0u;
+        const uint32_t lb = (uint32_t)npx * 16;
+        const uint32_t rb = (uint32_t)(g1 - g0 + 1) * kGroupBytes;
+        mbar_expect_tx(bar, sb + lb + rb);
+        if (MODE != 0)
+            tma_load(smem_u32(base + (xlo - xf) * SB), k.S + ((size_t)y * k.W + xlo) * k.Dp2, sb, bar);
+        tma_load(smem_u32(base + offL + (xlo - xf) * 16), k.LP + (size_t)y * k.W + xlo, lb, bar);
+        tma_load(smem_u32(base + offR), k.RPp + (size_t)y * k.Wp + 9 * g0, rb, bar);
+    };
+
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < nslots; b++) mbar_init(smem_u32(&bars[b]), 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    int issued = 0;
+    if (threadIdx.x == 0) {
+        for (; issued < nslots && issued < nrows; issued++) issue(issued);
     }
 
-    uint32_t L[PPL], c[PPL], s[PPL];
-    uint32_t sb[kLook][PPL];
-    auto sptr = [&](int t) -> uint32_t* {
-        const int x = sx + t * dx, y = sy + t * dy;
-        return k.S + ((size_t)y * k.W + x) * k.Dp2 + lane * PPL;
+    const int kp = kf + warp;
+    const bool has_line = warp < Gb;
+    const int base_d = lane * 2 * PPL;
+    bool started = false, ok = true;
+    uint32_t L[PPL], m = 0;
+
+    for (int i = 0; i < nrows; i++) {
+        const int slot = i % nslots;
+        ok = ok && mbar_wait(smem_u32(&bars[slot]), (uint32_t)(i / nslots) & 1u);
+        const int y = row_of(i);
+        const int xf = kf + s * y;
+        const int x = kp + s * y;
+        if (ok && has_line && x >= 0 && x < k.W) {
+            const unsigned char* base = slots + slot * slotBytes;
+            const uint4 lp = *(const uint4*)(base + offL + (x - xf) * 16);
+            const int g0 = max(0, max(xf, 0) - DSPAN + 2) >> 3;
+            const Plane* rseg = (const Plane*)(base + offR);
+            const int lim = min(x + 1, k.D);
+            uint32_t c[PPL], Ln[PPL];
+#pragma unroll
+            for (int q = 0; q < PPL; q++) {
+                const int d = base_d + 2 * q;
+                const int e = max(x - d, 0);
+                const uint4 rp = *(const uint4*)&rseg[ppos(e) - 9 * g0];
+                c[q] = mask_pair(bt_pair(lp, rp), d, lim, k.BIGBIG);
+            }
+            if (!started) {
+#pragma unroll
+                for (int q = 0; q < PPL; q++) Ln[q] = c[q];
+                started = true;
+            } else {
+                recur<PPL>(L, m, c, Ln, lane, k);
+            }
+            uint32_t* sg = k.S + ((size_t)y * k.W + x) * k.Dp2 + lane * PPL;
+            if (MODE == 0) {
+                Vec<PPL>::st(sg, Ln);
+            } else {
+                uint32_t sv[PPL];
+                Vec<PPL>::lds((const uint32_t*)(base + (x - xf) * SB) + lane * PPL, sv);
+#pragma unroll
+                for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
+                Vec<PPL>::st(sg, sv);
+            }
+#pragma unroll
+            for (int q = 0; q < PPL; q++) L[q] = Ln[q];
+            m = warp_min_pairs<PPL>(L);
+        }
+        // every thread is done with this slot: refill it with row i + nslots
+        if (__syncthreads_or(ok ? 0 : 1)) {
+            if (threadIdx.x == 0) {
+                atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
+                for (int r = i + 1; r < issued; r++)
+                    mbar_wait(smem_u32(&bars[r % nslots]), (uint32_t)(r / nslots) & 1u);
+                mbar_wait(smem_u32(&bars[slot]), (uint32_t)(i / nslots) & 1u);
+            }
+            return;
+        }
+        if (threadIdx.x == 0 && issued < nrows) {
+            fence_proxy_async();
+            issue(issued);
+            issued++;
+        }
+    }
+}
+
+// ------------------------------------------------------ horizontal passes
+// One warp per image row, walking x in direction dx.  MODE 1: S += L;
+// MODE 2: final S -> WTA (+ right-view disparity and left-right check).
+template <int PPL, int MODE>
+__global__ void __launch_bounds__(kMaxGH * 32, 1) h_pass(FK k, int dx, int GH, int warp_bytes) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int SB = 128 * PPL;
+    constexpr int DSPAN = 64 * PPL;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y = blockIdx.x * GH + warp;
+    if (y >= k.H) return;  // warps are independent: no block-wide barrier below
+    unsigned char* wbase = smem + (size_t)warp * warp_bytes;
+    uint64_t* sbar = (uint64_t*)wbase;  // kHSlots barriers
+    uint64_t* cbar = sbar + kHSlots;    // kChunkSlots barriers
+    unsigned char* sring = wbase + 128;
+    unsigned char* cring = sring + kHSlots * SB;
+    uint32_t* lrring = (uint32_t*)(cring + kChunkSlots * kChunkBytes);
+    uint16_t* rowL = (uint16_t*)(lrring + kRing);
+    uint16_t* rowR = rowL + k.W;
+    const bool lr = MODE == 2 && k.lr_thr >= 0;
+
+    const int W = k.W;
+    const int x0 = dx > 0 ? 0 : W - 1;
+    const int nch = (W + kChunk - 1) / kChunk;
+    const int groups_row = (W + 7) / 8;
+    const Plane* rrow = k.RPp + (size_t)y * k.Wp;
+    const uint32_t* srow = k.S + (size_t)y * W * k.Dp2;
+
+    if (lane == 0) {
+        for (int b = 0; b < kHSlots + kChunkSlots; b++) mbar_init(smem_u32(&sbar[b]), 1);
+        fence_mbar_init();
+    }
+    if (lr)
+        for (int i = lane; i < kRing; i += 32) lrring[i] = 0xFFFFFFFFu;
+    __syncwarp();
+
+    auto cl_of = [&](int x) { return max(0, x - DSPAN + 2) / kChunk; };
+    auto ch_of = [&](int x) { return x / kChunk; };
+    auto chunk_use = [&](int c) { return dx > 0 ? c / kChunkSlots : (nch - 1 - c) / kChunkSlots; };
+    auto issue_chunk = [&](int c) {
+        const int ng = min(kChunk / 8, groups_row - c * (kChunk / 8));
+        const uint32_t bar = smem_u32(&cbar[c % kChunkSlots]);
+        mbar_expect_tx(bar, (uint32_t)ng * kGroupBytes);
+        tma_load(smem_u32(cring + (c % kChunkSlots) * kChunkBytes), rrow + 9 * (c * (kChunk / 8)),
+                 (uint32_t)ng * kGroupBytes, bar);
     };
-    auto finish = [&](int x, int y, const uint32_t* sv) {
-        // WTA: lowest (S, d) -- ties to the lowest d (tdvision/wtacpu.cpp:26-30)
-        uint32_t key = 0xFFFFFFFFu;
+    auto issue_s = [&](int t) {
+        const int x = x0 + dx * t;
+        const uint32_t bar = smem_u32(&sbar[t % kHSlots]);
+        mbar_expect_tx(bar, SB);
+        tma_load(smem_u32(sring + (t % kHSlots) * SB), srow + (size_t)x * k.Dp2, SB, bar);
+    };
+    auto drain_chunks = [&](int waited_c, int next) {
+        if (dx > 0)
+            for (int c = waited_c + 1; c < next; c++)
+                mbar_wait(smem_u32(&cbar[c % kChunkSlots]), (uint32_t)chunk_use(c) & 1u);
+        else
+            for (int c = waited_c - 1; c > next; c--)
+                mbar_wait(smem_u32(&cbar[c % kChunkSlots]), (uint32_t)chunk_use(c) & 1u);
+    };
+
+    // chunks: next to issue and the last one waited for
+    int next_c = dx > 0 ? 0 : nch - 1;
+    int waited = dx > 0 ? -1 : nch;
+    int s_issued = 0;
+    if (lane == 0) {
+        for (; s_issued < kHSlots && s_issued < W; s_issued++) issue_s(s_issued);
+    }
+    bool ok = true;
+    const int base_d = lane * 2 * PPL;
+    uint32_t L[PPL], m = 0, s[PPL];
+    uint4 lp_next = __ldg((const uint4*)&k.LP[(size_t)y * W + x0]);
+
+    auto finish = [&](int x, const uint32_t* sv) {
+        uint32_t key = FULL;
 #pragma unroll
         for (int q = 0; q < PPL; q++) {
-            const uint32_t d = base + 2 * q;
+            const uint32_t d = base_d + 2 * q;
             key = min(key, ((sv[q] & 0xFFFFu) << 8) | d);
             key = min(key, ((sv[q] >> 16) << 8) | (d + 1));
             if (lr) {
-                // right view: candidate for xr = x - d
                 const int xr0 = x - (int)d, xr1 = xr0 - 1;
                 if (xr0 >= 0) {
-                    uint32_t& r0 = ring[xr0 & (kRing - 1)];
+                    uint32_t& r0 = lrring[xr0 & (kRing - 1)];
                     r0 = min(r0, ((sv[q] & 0xFFFFu) << 8) | d);
                 }
                 if (xr1 >= 0) {
-                    uint32_t& r1 = ring[xr1 & (kRing - 1)];
+                    uint32_t& r1 = lrring[xr1 & (kRing - 1)];
                     r1 = min(r1, ((sv[q] >> 16) << 8) | (d + 1));
                 }
             }
         }
-        key = __reduce_min_sync(0xFFFFFFFFu, key);
+        key = __reduce_min_sync(FULL, key);
         const uint16_t dl = (uint16_t)(key & 0xFFu);
         if (lr) {
             __syncwarp();
             if (lane == 0) {
-                uint32_t& r = ring[x & (kRing - 1)];
+                uint32_t& r = lrring[x & (kRing - 1)];
                 rowR[x] = (uint16_t)(r & 0xFFu);
                 r = 0xFFFFFFFFu;
                 rowL[x] = dl;
             }
             __syncwarp();
         } else if (lane == 0) {
-            const size_t o = (size_t)y * k.W + x;
+            const size_t o = (size_t)y * W + x;
             if (k.disp) k.disp[o] = dl;
             if (k.disp_norm) k.disp_norm[o] = __fdiv_rn((float)dl, (float)k.D);
         }
     };
 
-    // step 0: L = C at the path start
-    int x = sx, y = sy;
-    bt_pairs<PPL>(k, x, y, base, c);
-#pragma unroll
-    for (int q = 0; q < PPL; q++) L[q] = c[q];
-    if (MODE == 0) {
-        Vec<PPL>::st(sptr(0), L);
-    } else {
-        Vec<PPL>::ld(sptr(0), s);
-#pragma unroll
-        for (int q = 0; q < PPL; q++) s[q] += L[q];
-        if (MODE == 1) Vec<PPL>::st(sptr(0), s);
-        else finish(x, y, s);
-    }
-    uint32_t m = warp_min_pairs<PPL>(L);
-    if (MODE != 0) {
-#pragma unroll
-        for (int u = 0; u < kLook; u++)
-            if (1 + u < len) Vec<PPL>::ld(sptr(1 + u), sb[u]);
-    }
-
-    for (int t0 = 1; t0 < len; t0 += kLook) {
-#pragma unroll
-        for (int u = 0; u < kLook; u++) {
-            const int t = t0 + u;
-            if (t < len) {
-                x += dx;
-                y += dy;
-                bt_pairs<PPL>(k, x, y, base, c);
-                const uint32_t MM = m * 0x10001u;
-                const uint32_t MP2 = MM + k.P2P2;
-                uint32_t up = __shfl_up_sync(0xFFFFFFFFu, L[PPL - 1], 1);
-                uint32_t dn = __shfl_down_sync(0xFFFFFFFFu, L[0], 1);
-                if (lane == 0) up = k.BIGBIG;
-                if (lane == 31) dn = k.BIGBIG;
-                uint32_t Ln[PPL];
-#pragma unroll
-                for (int q = 0; q < PPL; q++) {
-                    const uint32_t lm = hi_lo(q > 0 ? L[q - 1] : up, L[q]);
-                    const uint32_t lp = hi_lo(L[q], q < PPL - 1 ? L[q + 1] : dn);
-                    uint32_t tv = vmin2(lm, lp) + k.P1P1;
-                    tv = vmin2(vmin2(tv, L[q]), MP2);
-                    Ln[q] = tv + c[q] - MM;
+    int t = 0;
+    for (; t < W; t++) {
+        const int x = x0 + dx * t;
+        // keep the right-plane window [x-DSPAN+2, x] resident, kLookC chunks ahead
+        if (lane == 0) {
+            if (dx > 0) {
+                while (next_c < nch && next_c <= ch_of(x) + kLookC && cl_of(x) > next_c - kChunkSlots) {
+                    fence_proxy_async();
+                    issue_chunk(next_c++);
                 }
-#pragma unroll
-                for (int q = 0; q < PPL; q++) L[q] = Ln[q];
-                if (MODE == 0) {
-                    Vec<PPL>::st(sptr(t), L);
-                } else {
-#pragma unroll
-                    for (int q = 0; q < PPL; q++) s[q] = sb[u][q] + L[q];
-                    if (t + kLook < len) Vec<PPL>::ld(sptr(t + kLook), sb[u]);
-                    if (MODE == 1) Vec<PPL>::st(sptr(t), s);
-                    else finish(x, y, s);
+            } else {
+                while (next_c >= 0 && next_c >= cl_of(x) - kLookC && ch_of(x) < next_c + kChunkSlots) {
+                    fence_proxy_async();
+                    issue_chunk(next_c--);
                 }
-                m = warp_min_pairs<PPL>(L);
             }
+        }
+        next_c = __shfl_sync(FULL, next_c, 0);
+        bool good = true;
+        if (dx > 0) {
+            while (good && waited < ch_of(x)) {
+                waited++;
+                good = mbar_wait(smem_u32(&cbar[waited % kChunkSlots]), (uint32_t)chunk_use(waited) & 1u);
+            }
+        } else {
+            while (good && waited > cl_of(x)) {
+                waited--;
+                good = mbar_wait(smem_u32(&cbar[waited % kChunkSlots]), (uint32_t)chunk_use(waited) & 1u);
+            }
+        }
+        good = good && mbar_wait(smem_u32(&sbar[t % kHSlots]), (uint32_t)(t / kHSlots) & 1u);
+        ok = __all_sync(FULL, good);
+        if (!ok) break;
+
+        const uint4 lp = lp_next;
+        if (t + 1 < W) lp_next = __ldg((const uint4*)&k.LP[(size_t)y * W + x + dx]);
+        const int lim = min(x + 1, k.D);
+        uint32_t c[PPL], Ln[PPL];
+#pragma unroll
+        for (int q = 0; q < PPL; q++) {
+            const int d = base_d + 2 * q;
+            const int e = max(x - d, 0);
+            const int c_e = e / kChunk, w_e = e % kChunk;
+            const uint4 rp = *(const uint4*)(cring + (c_e % kChunkSlots) * kChunkBytes + ppos(w_e) * 16);
+            c[q] = mask_pair(bt_pair(lp, rp), d, lim, k.BIGBIG);
+        }
+        if (t == 0) {
+#pragma unroll
+            for (int q = 0; q < PPL; q++) Ln[q] = c[q];
+        } else {
+            recur<PPL>(L, m, c, Ln, lane, k);
+        }
+        Vec<PPL>::lds((const uint32_t*)(sring + (t % kHSlots) * SB) + lane * PPL, s);
+#pragma unroll
+        for (int q = 0; q < PPL; q++) s[q] += Ln[q];
+        if (MODE == 1) Vec<PPL>::st(k.S + ((size_t)y * W + x) * k.Dp2 + lane * PPL, s);
+        else finish(x, s);
+#pragma unroll
+        for (int q = 0; q < PPL; q++) L[q] = Ln[q];
+        m = warp_min_pairs<PPL>(L);
+        __syncwarp();
+        if (lane == 0 && s_issued < W) {
+            fence_proxy_async();
+            issue_s(s_issued++);
         }
     }
 
+    if (!ok) {
+        if (lane == 0) {
+            atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
+            for (int r = t; r < s_issued; r++)
+                mbar_wait(smem_u32(&sbar[r % kHSlots]), (uint32_t)(r / kHSlots) & 1u);
+            drain_chunks(waited, next_c);
+        }
+        return;
+    }
+    // chunks fetched ahead but never needed still have copies in flight
+    if (lane == 0) drain_chunks(waited, next_c);
+
     if (lr) {
         __syncwarp();
-        const int yy = sy;
-        for (int xx = lane; xx < k.W; xx += 32) {
+        for (int xx = lane; xx < W; xx += 32) {
             const int dl = rowL[xx];
             const int xr = xx - dl;
             const bool bad = xr < 0 || abs(dl - (int)rowR[xr]) > k.lr_thr;
-            const size_t o = (size_t)yy * k.W + xx;
+            const size_t o = (size_t)y * W + xx;
             if (k.disp) k.disp[o] = bad ? (uint16_t)0xFFFF : (uint16_t)dl;
             if (k.disp_norm) k.disp_norm[o] = bad ? -1.0f : __fdiv_rn((float)dl, (float)k.D);
             if (k.disp_right) k.disp_right[o] = rowR[xx];
@@ -340,51 +582,83 @@ __global__ void __launch_bounds__(kWarps * 32) fused_pass(FK k, int dx, int dy, 
     }
 }
 
-int nwalks_for(int dx, int dy, int W, int H) {
-    if (dy == 0) return H;
-    if (dx == 0) return W;
-    return W + H - 1;
+// ------------------------------------------------------------- host side
+int ppl_for(int D) { return D <= 64 ? 1 : (D <= 128 ? 2 : 4); }
+
+constexpr int kSmemBudget = 220 * 1024;
+
+template <int PPL, int MODE>
+cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
+    const int s = dx * dy;
+    const int nlines = s == 0 ? k.W : k.W + k.H - 1;
+    const int kmin = s > 0 ? -(k.H - 1) : 0;
+    int G = (nlines + 147) / 148;
+    G = G < 1 ? 1 : (G > kMaxG ? kMaxG : G);
+    const int SB = 128 * PPL, DSPAN = 64 * PPL;
+    const int NRG = (G + DSPAN) / 8 + 2;
+    const int slotBytes = align128(G * SB + G * 16 + NRG * kGroupBytes);
+    int nslots = (kSmemBudget - 128) / slotBytes;
+    nslots = nslots > kRowSlots ? kRowSlots : nslots;
+    if (nslots < 2) return cudaErrorInvalidConfiguration;
+    const int smem = 128 + nslots * slotBytes;
+    cudaError_t e =
+        cudaFuncSetAttribute(vd_pass<PPL, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const int blocks = (nlines + G - 1) / G;
+    vd_pass<PPL, MODE><<<blocks, G * 32, smem, st>>>(k, s, dy, kmin, nlines, G, nslots);
+    return cudaGetLastError();
+}
+
+template <int PPL, int MODE>
+cudaError_t launch_h(const FK& k, int dx, cudaStream_t st) {
+    const int SB = 128 * PPL;
+    const bool lr = MODE == 2 && k.lr_thr >= 0;
+    const int warp_bytes = align128(128 + kHSlots * SB + kChunkSlots * kChunkBytes +
+                                    (lr ? kRing * 4 + 2 * k.W * 2 : 0));
+    int GH = kSmemBudget / warp_bytes;
+    GH = GH > kMaxGH ? kMaxGH : GH;
+    if (GH < 1) return cudaErrorInvalidConfiguration;
+    const int smem = GH * warp_bytes;
+    cudaError_t e =
+        cudaFuncSetAttribute(h_pass<PPL, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const int blocks = (k.H + GH - 1) / GH;
+    h_pass<PPL, MODE><<<blocks, GH * 32, smem, st>>>(k, dx, GH, warp_bytes);
+    return cudaGetLastError();
 }
 
 template <int PPL>
 cudaError_t run_fused(const FK& k, int paths, cudaStream_t st, Timer* tm) {
-    static const char* names8[8] = {"fused_pass_V+", "fused_pass_V-", "fused_pass_D1+", "fused_pass_D1-",
-                                    "fused_pass_D2+", "fused_pass_D2-", "fused_pass_H+", "fused_pass_H-_wta"};
-    static const char* names4[4] = {"fused_pass_V+", "fused_pass_V-", "fused_pass_H+", "fused_pass_H-_wta"};
-    static const int dirs8[8][2] = {{0, 1}, {0, -1}, {1, 1}, {-1, -1}, {-1, 1}, {1, -1}, {1, 0}, {-1, 0}};
-    static const int dirs4[4][2] = {{0, 1}, {0, -1}, {1, 0}, {-1, 0}};
-    const int n = paths == 4 ? 4 : 8;
-    const size_t lr_smem = (size_t)kWarps * kRing * 4 + (size_t)kWarps * 2 * k.W * 2;
-    for (int p = 0; p < n; p++) {
-        const int dx = paths == 4 ? dirs4[p][0] : dirs8[p][0];
-        const int dy = paths == 4 ? dirs4[p][1] : dirs8[p][1];
-        const int nw = nwalks_for(dx, dy, k.W, k.H);
-        const int blocks = (nw + kWarps - 1) / kWarps;
-        if (p == 0) {
-            fused_pass<PPL, 0><<<blocks, kWarps * 32, 0, st>>>(k, dx, dy, nw);
-        } else if (p < n - 1) {
-            fused_pass<PPL, 1><<<blocks, kWarps * 32, 0, st>>>(k, dx, dy, nw);
-        } else {
-            const size_t sm = k.lr_thr >= 0 ? lr_smem : 0;
-            if (sm > 48 * 1024) {
-                cudaError_t e = cudaFuncSetAttribute(fused_pass<PPL, 2>,
-                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-                if (e != cudaSuccess) return e;
-            }
-            fused_pass<PPL, 2><<<blocks, kWarps * 32, sm, st>>>(k, dx, dy, nw);
-        }
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        if (tm) tm->mark(paths == 4 ? names4[p] : names8[p]);
+    cudaError_t e;
+    auto mark = [&](const char* n) {
+        if (tm) tm->mark(n);
+    };
+    if ((e = launch_vd<PPL, 0>(k, 0, 1, st)) != cudaSuccess) return e;
+    mark("fused_pass_V+");
+    if ((e = launch_vd<PPL, 1>(k, 0, -1, st)) != cudaSuccess) return e;
+    mark("fused_pass_V-");
+    if (paths == 8) {
+        if ((e = launch_vd<PPL, 1>(k, 1, 1, st)) != cudaSuccess) return e;
+        mark("fused_pass_D1+");
+        if ((e = launch_vd<PPL, 1>(k, -1, -1, st)) != cudaSuccess) return e;
+        mark("fused_pass_D1-");
+        if ((e = launch_vd<PPL, 1>(k, -1, 1, st)) != cudaSuccess) return e;
+        mark("fused_pass_D2+");
+        if ((e = launch_vd<PPL, 1>(k, 1, -1, st)) != cudaSuccess) return e;
+        mark("fused_pass_D2-");
     }
+    if ((e = launch_h<PPL, 1>(k, 1, st)) != cudaSuccess) return e;
+    mark("fused_pass_H+");
+    if ((e = launch_h<PPL, 2>(k, -1, st)) != cudaSuccess) return e;
+    mark("fused_pass_H-_wta");
     return cudaSuccess;
 }
 
-int ppl_for(int D) { return D <= 64 ? 1 : (D <= 128 ? 2 : 4); }
-
 }  // namespace
 
-size_t fused_plane_bytes(int W, int H) { return (size_t)2 * W * H * sizeof(Plane); }
+size_t fused_plane_bytes(int W, int H) {
+    return ((size_t)W * H + (size_t)padded_len(W) * H) * sizeof(Plane);
+}
 
 size_t fused_agg_bytes(int W, int H, int D) {
     return (size_t)W * H * 64 * ppl_for(D) * sizeof(uint16_t);
@@ -392,19 +666,21 @@ size_t fused_agg_bytes(int W, int H, int D) {
 
 cudaError_t launch_fused(const FusedArgs& a, cudaStream_t st, Timer* tm) {
     Plane* LP = (Plane*)a.planes;
-    Plane* RP = LP + (size_t)a.W * a.H;
+    Plane* RPp = LP + (size_t)a.W * a.H;
+    const int Wp = padded_len(a.W);
     dim3 pb(128), pg((a.W + 127) / 128, a.H);
-    prep_kernel<<<pg, pb, 0, st>>>(a.L, a.R, LP, RP, a.W, a.H);
+    prep_kernel<<<pg, pb, 0, st>>>(a.L, a.R, LP, RPp, a.W, a.H, Wp);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (tm) tm->mark("fused_prep");
     FK k;
     k.LP = LP;
-    k.RP = RP;
+    k.RPp = RPp;
     k.S = (uint32_t*)a.agg;
     k.W = a.W;
     k.H = a.H;
     k.D = a.D;
+    k.Wp = Wp;
     const int ppl = ppl_for(a.D);
     k.Dp2 = 32 * ppl;
     const uint32_t big = 511u + 2u * (uint32_t)a.p2h;
@@ -415,6 +691,7 @@ cudaError_t launch_fused(const FusedArgs& a, cudaStream_t st, Timer* tm) {
     k.disp_norm = a.disp_norm;
     k.disp_right = a.disp_right;
     k.lr_thr = a.lr_thr;
+    k.err = a.err;
     if (ppl == 1) return run_fused<1>(k, a.paths, st, tm);
     if (ppl == 2) return run_fused<2>(k, a.paths, st, tm);
     return run_fused<4>(k, a.paths, st, tm);

@@ -94,6 +94,7 @@ struct tdv_ctx {
     Buf planes;   // fused path: left/right BT planes
     Buf codes;    // DP choice codes
     Buf misc;     // small per-call scratch
+    Buf err;      // one device int: error status written by kernels
 
     tdv::PassSchedule sched;
     Buf sched_buf;
@@ -149,8 +150,9 @@ struct FusedArgs {
     float* disp_norm;
     uint16_t* disp_right;
     int lr_thr;
-    void* planes;  // 2 * W*H*16 bytes
-    void* agg;     // W*H*Dp*2 bytes
+    void* planes;  // fused_plane_bytes(W, H)
+    void* agg;     // fused_agg_bytes(W, H, D)
+    int* err;      // device word: kernels record TDV_ERR_TIMEOUT here
 };
 size_t fused_agg_bytes(int W, int H, int D);
 size_t fused_plane_bytes(int W, int H);
