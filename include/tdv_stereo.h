@@ -66,7 +66,7 @@ typedef struct {
     void* ptr;        /* device, dense, no padding between pixels */
     int32_t width, height, depth;
     int32_t layout;   /* tdv_layout */
-    int32_t dtype;    /* TDV_F32 (TDV_F64 accepted by the soft-SGM calls) */
+    int32_t dtype;    /* TDV_F32; the soft-SGM calls also take TDV_F64 */
 } tdv_volume;
 
 typedef struct {
@@ -145,6 +145,36 @@ tdv_status tdv_fast_wta(tdv_ctx* ctx, const tdv_image* left, const tdv_image* ri
 tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right,
                           int32_t max_disp, const tdv_sgm_params* params, tdv_disparity* out,
                           tdv_stream stream);
+
+/* ---- differentiable soft-argmin SGM (no reference counterpart) --------- */
+typedef struct {
+    float p1, p2;       /* penalties, constant P2 */
+    int32_t paths;      /* 8 or 4 */
+    float tau;          /* softmin temperature, > 0 */
+    int32_t checkpoint; /* 0: the tape keeps 2-bit choice codes of every cell;
+                           k in [1,32]: it keeps L every k steps of each path
+                           and the adjoint recomputes one k-step segment at a
+                           time */
+} tdv_soft_params;
+
+/* Bytes of the tape tdv_soft_sgm_forward records for the adjoint. */
+size_t tdv_soft_sgm_tape_bytes(int32_t width, int32_t height, int32_t depth, int32_t dtype,
+                               const tdv_soft_params* params);
+
+/* Expected disparity dhat = sum_d d*softmax(-S/tau) of the STANDARD 4/8-path
+ * aggregation S of `cost` (HWD layout, TDV_F32 or TDV_F64); dhat is W*H of
+ * the cost's dtype.  With `tape` (tdv_soft_sgm_tape_bytes bytes, device) the
+ * call records what tdv_soft_sgm_backward needs; with tape = NULL it only
+ * evaluates. */
+tdv_status tdv_soft_sgm_forward(tdv_ctx* ctx, const tdv_volume* cost, const tdv_soft_params* params,
+                                void* dhat, void* tape, size_t tape_bytes, tdv_stream stream);
+
+/* Adjoint of tdv_soft_sgm_forward: given g = dLoss/d(dhat) (W*H), writes
+ * dLoss/dcost into `dcost` (same shape/dtype as the cost) and
+ * (dLoss/dP1, dLoss/dP2) into dpen[0..1] (device, cost dtype). */
+tdv_status tdv_soft_sgm_backward(tdv_ctx* ctx, const tdv_volume* cost, const tdv_soft_params* params,
+                                 const void* tape, size_t tape_bytes, const void* g_dhat,
+                                 tdv_volume* dcost, void* dpen, tdv_stream stream);
 
 /* ---- context ---------------------------------------------------------- */
 typedef void* (*tdv_alloc_fn)(size_t bytes, void* user);

@@ -7,7 +7,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <new>
+#include <vector>
 
 #include "tdv_internal.hpp"
 
@@ -211,6 +213,102 @@ tdv_status run_sgm(tdv_ctx* ctx, const tdv_volume* cost, const tdv_image* guide,
     return TDV_OK;
 }
 
+// ---- soft SGM tape layout -------------------------------------------------
+struct SoftLayout {
+    size_t S, stats, codes, kstar, off, ckpt, total;
+    long long nck;
+};
+
+size_t al256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+int soft_ndir(int paths) { return paths == 4 ? 4 : 8; }
+
+// walk lengths per direction, in the order the kernels number the walks
+void soft_walk_lengths(int W, int H, int dx, int dy, std::vector<int>& out) {
+    out.clear();
+    if (dy == 0) {
+        out.assign(H, W);
+        return;
+    }
+    if (dx == 0) {
+        out.assign(W, H);
+        return;
+    }
+    for (int i = 0; i < W + H - 1; i++) {
+        int sx, sy;
+        const int ye = dy > 0 ? 0 : H - 1, xe = dx > 0 ? 0 : W - 1;
+        if (i < W) {
+            sx = i;
+            sy = ye;
+        } else {
+            sx = xe;
+            sy = ye + dy * (i - W + 1);
+        }
+        const int nx = dx > 0 ? W - sx : sx + 1;
+        const int ny = dy > 0 ? H - sy : sy + 1;
+        out.push_back(std::min(nx, ny));
+    }
+}
+
+const int kSoftDirs[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1}, {-1, 1}, {1, -1}};
+
+SoftLayout soft_layout(int W, int H, int D, int esize, const tdv_soft_params* p,
+                       std::vector<long long>* offs) {
+    SoftLayout L{};
+    const size_t npix = (size_t)W * H;
+    const int nd = soft_ndir(p->paths);
+    const int npl = D <= 32 ? 1 : (D <= 64 ? 2 : (D <= 128 ? 4 : 8));
+    const int cb = (npl + 3) / 4;
+    size_t o = 0;
+    L.S = o;
+    o = al256(o + npix * D * esize);
+    L.stats = o;
+    o = al256(o + npix * 3 * esize);
+    if (p->checkpoint == 0) {
+        L.codes = o;
+        o = al256(o + (size_t)nd * npix * 32 * cb);
+        L.kstar = o;
+        o = al256(o + (size_t)nd * npix * 2);
+    } else {
+        long long n = 0;
+        std::vector<int> lens;
+        if (offs) offs->assign((size_t)nd * (W + H), 0);
+        for (int d = 0; d < nd; d++) {
+            soft_walk_lengths(W, H, kSoftDirs[d][0], kSoftDirs[d][1], lens);
+            for (size_t w = 0; w < lens.size(); w++) {
+                if (offs) (*offs)[(size_t)d * (W + H) + w] = n;
+                n += (lens[w] + p->checkpoint - 1) / p->checkpoint;
+            }
+        }
+        L.nck = n;
+        L.off = o;
+        o = al256(o + (size_t)nd * (W + H) * sizeof(long long));
+        L.ckpt = o;
+        o = al256(o + (size_t)n * D * esize);
+    }
+    L.total = o;
+    return L;
+}
+
+tdv_status check_soft(tdv_ctx* ctx, const tdv_volume* cost, const tdv_soft_params* p) {
+    if (!cost || !cost->ptr) return fail(ctx, TDV_ERR_INVALID_ARG, "cost: null volume");
+    if (cost->width <= 0 || cost->height <= 0 || cost->depth <= 0 || cost->width > kMaxSide ||
+        cost->height > kMaxSide)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "cost: bad size");
+    if (cost->layout != TDV_LAYOUT_HWD) return fail(ctx, TDV_ERR_INVALID_ARG, "soft SGM takes the HWD layout");
+    if (cost->dtype != TDV_F32 && cost->dtype != TDV_F64)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "soft SGM takes TDV_F32 or TDV_F64");
+    if (cost->depth > tdv::kMaxDispSgm) return fail(ctx, TDV_ERR_UNSUPPORTED, "soft SGM supports D <= 256");
+    if (!p) return fail(ctx, TDV_ERR_INVALID_ARG, "null soft params");
+    if (p->paths != 4 && p->paths != 8) return fail(ctx, TDV_ERR_INVALID_ARG, "paths must be 4 or 8");
+    if (!(p->tau > 0.0f) || !std::isfinite(p->tau)) return fail(ctx, TDV_ERR_INVALID_ARG, "tau must be > 0");
+    if (!std::isfinite(p->p1) || !std::isfinite(p->p2))
+        return fail(ctx, TDV_ERR_INVALID_ARG, "penalties must be finite");
+    if (p->checkpoint < 0 || p->checkpoint > 32)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "checkpoint must be in [0, 32]");
+    return TDV_OK;
+}
+
 bool is_half_multiple(float v) { return v >= 0.0f && v <= 4096.0f && std::floor(2.0f * v) == 2.0f * v; }
 
 }  // namespace
@@ -283,7 +381,7 @@ tdv_status tdv_ctx_create(int32_t device, tdv_ctx** out) {
 void tdv_ctx_destroy(tdv_ctx* ctx) {
     if (!ctx) return;
     const bool any = ctx->agg.ptr || ctx->cost.ptr || ctx->planes.ptr || ctx->codes.ptr ||
-                     ctx->misc.ptr || ctx->sched_buf.ptr || ctx->err.ptr;
+                     ctx->misc.ptr || ctx->sched_buf.ptr || ctx->err.ptr || ctx->soft.ptr;
     if (any) {
         DeviceScope ds(ctx->device);
         cudaDeviceSynchronize();
@@ -294,6 +392,7 @@ void tdv_ctx_destroy(tdv_ctx* ctx) {
         release_buf(ctx, ctx->misc);
         release_buf(ctx, ctx->sched_buf);
         release_buf(ctx, ctx->err);
+        release_buf(ctx, ctx->soft);
     }
     if (!ctx->timer.ev.empty()) {
         DeviceScope ds(ctx->device);
@@ -367,6 +466,108 @@ tdv_status tdv_ctx_device_status(tdv_ctx* ctx, tdv_stream stream) {
         TDV_CUDA(cudaMemsetAsync(ctx->err.ptr, 0, sizeof(int), S(stream)));
         return fail(ctx, (tdv_status)v, "a kernel reported %s", tdv_status_string((tdv_status)v));
     }
+    return TDV_OK;
+}
+
+size_t tdv_soft_sgm_tape_bytes(int32_t W, int32_t H, int32_t D, int32_t dtype, const tdv_soft_params* p) {
+    if (W <= 0 || H <= 0 || D <= 0 || !p || (dtype != TDV_F32 && dtype != TDV_F64)) return 0;
+    if (p->checkpoint < 0 || p->checkpoint > 32 || (p->paths != 4 && p->paths != 8)) return 0;
+    return soft_layout(W, H, D, dtype == TDV_F64 ? 8 : 4, p, nullptr).total;
+}
+
+tdv_status tdv_soft_sgm_forward(tdv_ctx* ctx, const tdv_volume* cost, const tdv_soft_params* p, void* dhat,
+                                void* tape, size_t tape_bytes, tdv_stream stream) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    TDV_TRY(check_soft(ctx, cost, p));
+    if (!dhat) return fail(ctx, TDV_ERR_INVALID_ARG, "null dhat");
+    const int W = cost->width, H = cost->height, D = cost->depth;
+    const int es = cost->dtype == TDV_F64 ? 8 : 4;
+    SoftLayout lay = soft_layout(W, H, D, es, p, &ctx->ckpt_off_host);
+    if (tape && tape_bytes < lay.total)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "tape of %zu bytes < %zu needed", tape_bytes, lay.total);
+    TDV_DEVICE_SCOPE(ctx);
+    ctx->timer.begin(S(stream));
+    unsigned char* base;
+    if (tape) {
+        base = (unsigned char*)tape;
+    } else {
+        TDV_TRY(ensure(ctx, ctx->soft, lay.stats + al256((size_t)W * H * 3 * es)));
+        base = (unsigned char*)ctx->soft.ptr;
+    }
+    if (tape && p->checkpoint > 0)
+        TDV_CUDA(cudaMemcpyAsync(base + lay.off, ctx->ckpt_off_host.data(),
+                                 ctx->ckpt_off_host.size() * sizeof(long long), cudaMemcpyHostToDevice,
+                                 S(stream)));
+    tdv::SoftLaunch a{};
+    a.f64 = es == 8;
+    a.cost = cost->ptr;
+    a.S = base + lay.S;
+    a.stats = base + lay.stats;
+    a.dhat = dhat;
+    a.W = W;
+    a.H = H;
+    a.D = D;
+    a.paths = p->paths;
+    a.ck = tape ? p->checkpoint : 0;
+    a.record = tape ? 1 : 0;
+    if (tape && p->checkpoint == 0) {
+        a.codes = base + lay.codes;
+        a.kstar = base + lay.kstar;
+    }
+    if (tape && p->checkpoint > 0) {
+        a.ckpt = base + lay.ckpt;
+        a.ckpt_off = (const long long*)(base + lay.off);
+    }
+    a.p1 = p->p1;
+    a.p2 = p->p2;
+    a.tau = p->tau;
+    TDV_CUDA(tdv::launch_soft_forward(a, S(stream), &ctx->timer));
+    return TDV_OK;
+}
+
+tdv_status tdv_soft_sgm_backward(tdv_ctx* ctx, const tdv_volume* cost, const tdv_soft_params* p,
+                                 const void* tape, size_t tape_bytes, const void* g_dhat, tdv_volume* dcost,
+                                 void* dpen, tdv_stream stream) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    TDV_TRY(check_soft(ctx, cost, p));
+    if (!tape || !g_dhat || !dpen) return fail(ctx, TDV_ERR_INVALID_ARG, "null tape, gradient or dpen");
+    if (!dcost || !dcost->ptr || dcost->width != cost->width || dcost->height != cost->height ||
+        dcost->depth != cost->depth || dcost->layout != cost->layout || dcost->dtype != cost->dtype)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "dcost must match the cost volume");
+    const int W = cost->width, H = cost->height, D = cost->depth;
+    const int es = cost->dtype == TDV_F64 ? 8 : 4;
+    SoftLayout lay = soft_layout(W, H, D, es, p, nullptr);
+    if (tape_bytes < lay.total)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "tape of %zu bytes < %zu needed", tape_bytes, lay.total);
+    TDV_DEVICE_SCOPE(ctx);
+    ctx->timer.begin(S(stream));
+    TDV_TRY(ensure(ctx, ctx->soft, (size_t)W * H * D * es));
+    unsigned char* base = (unsigned char*)tape;
+    tdv::SoftLaunch a{};
+    a.f64 = es == 8;
+    a.cost = cost->ptr;
+    a.S = base + lay.S;
+    a.stats = base + lay.stats;
+    a.dS = ctx->soft.ptr;
+    a.dcost = dcost->ptr;
+    a.g = g_dhat;
+    a.dpen = dpen;
+    a.W = W;
+    a.H = H;
+    a.D = D;
+    a.paths = p->paths;
+    a.ck = p->checkpoint;
+    if (p->checkpoint == 0) {
+        a.codes = base + lay.codes;
+        a.kstar = base + lay.kstar;
+    } else {
+        a.ckpt = base + lay.ckpt;
+        a.ckpt_off = (const long long*)(base + lay.off);
+    }
+    a.p1 = p->p1;
+    a.p2 = p->p2;
+    a.tau = p->tau;
+    TDV_CUDA(tdv::launch_soft_backward(a, S(stream), &ctx->timer));
     return TDV_OK;
 }
 

@@ -45,15 +45,15 @@ namespace tdv {
 
 namespace {
 
-constexpr int kMaxG = 16;       // warps per block, vertical/diagonal passes
-constexpr int kRowSlots = 6;    // ring depth (rows), vertical/diagonal passes
+constexpr int kMaxG = 24;       // consumer warps per block, vertical/diagonal passes
+constexpr int kRowSlots = 8;    // ring depth (rows), vertical/diagonal passes (power of 2)
 constexpr int kMaxGH = 8;       // warps per block, horizontal passes
 constexpr int kHSlots = 8;      // S ring depth (steps), horizontal passes
 constexpr int kChunk = 64;      // right-plane entries per horizontal refill
 constexpr int kChunkSlots = 8;  // resident chunks per horizontal warp
 constexpr int kLookC = 2;       // chunks fetched ahead of need
-constexpr int kRing = 256;      // right-disparity ring per warp (>= max D)
-constexpr uint32_t kSpin = 1u << 22;
+constexpr uint64_t kWaitNs = 1000000000ull;   // 1 s: a wait this long means a lost copy
+constexpr uint64_t kDrainNs = 10000000ull;    // 10 ms per wait while retiring after an error
 constexpr int kGroupBytes = 9 * 16;
 constexpr int kChunkBytes = (kChunk / 8) * kGroupBytes;
 constexpr uint32_t FULL = 0xFFFFFFFFu;
@@ -92,6 +92,9 @@ __device__ __forceinline__ void fence_mbar_init() {
 __device__ __forceinline__ void fence_proxy_async() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                  : "memory");
@@ -114,11 +117,19 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait for phase `parity` of `bar`; false when the bound runs out.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (uint32_t it = 0; it < kSpin; it++)
-        if (mbar_try(bar, parity)) return true;
-    return false;
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait for phase `parity` of `bar`: false once `limit_ns` of wall
+// time have passed without the phase completing.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_t limit_ns = kWaitNs) {
+    if (mbar_try(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_try(bar, parity))
+        if (global_ns() - t0 > limit_ns) return false;
+    return true;
 }
 
 // ---------------------------------------------------------------- planes
@@ -255,17 +266,22 @@ __device__ __forceinline__ void recur(const uint32_t* L, uint32_t m, const uint3
 // ---------------------------------------------- vertical / diagonal passes
 // A path line is x = kp + s*y (s = dx*dy); the block owns lines
 // j0 .. j0+G-1 (kp = kmin + j) and walks rows in the pass direction dy.
+// Warps 0..G-1 consume one row per step; warp G is the producer: its lane 0
+// issues the TMA copies of row i into ring slot i % kRowSlots once every
+// consumer warp has released the slot's previous row (full/empty mbarrier
+// pairs), so no block-wide barrier is taken per row.
 template <int PPL, int MODE>
-__global__ void __launch_bounds__(kMaxG * 32, 1)
-    vd_pass(FK k, int s, int dy, int kmin, int nlines, int G, int nslots) {
+__global__ void __launch_bounds__((kMaxG + 1) * 32, 1)
+    vd_pass(FK k, int s, int dy, int kmin, int nlines, int G) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int SB = 128 * PPL;
     constexpr int DSPAN = 64 * PPL;
     const int NRG = (G + DSPAN) / 8 + 2;
     const int offL = G * SB, offR = offL + G * 16;
     const int slotBytes = align128(offR + NRG * kGroupBytes);
-    uint64_t* bars = (uint64_t*)smem;
-    unsigned char* slots = smem + 128;
+    uint64_t* full = (uint64_t*)smem;
+    uint64_t* empty = full + kRowSlots;
+    unsigned char* slots = smem + 2 * kRowSlots * 8;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int j0 = blockIdx.x * G;
@@ -284,75 +300,106 @@ __global__ void __launch_bounds__(kMaxG * 32, 1)
     }
     const int nrows = yhi - ylo + 1;
     if (nrows <= 0) return;  // uniform for the block
-
-    auto row_of = [&](int i) { return dy > 0 ? ylo + i : yhi - i; };
-    auto issue = [&](int i) {
-        const int y = row_of(i);
-        const int xf = kf + s * y;
-        const int xlo = max(xf, 0), xhi = min(xf + Gb, k.W);
-        const int npx = xhi - xlo;
-        const int g0 = max(0, xlo - DSPAN + 2) >> 3, g1 = (xhi - 1) >> 3;
-        unsigned char* base = slots + (i % nslots) * slotBytes;
-        const uint32_t bar = smem_u32(&bars[i % nslots]);
-        const uint32_t sb = MODE != 0 ? (uint32_t)npx * SB : 0u;
-        const uint32_t lb = (uint32_t)npx * 16;
-        const uint32_t rb = (uint32_t)(g1 - g0 + 1) * kGroupBytes;
-        mbar_expect_tx(bar, sb + lb + rb);
-        if (MODE != 0)
-            tma_load(smem_u32(base + (xlo - xf) * SB), k.S + ((size_t)y * k.W + xlo) * k.Dp2, sb, bar);
-        tma_load(smem_u32(base + offL + (xlo - xf) * 16), k.LP + (size_t)y * k.W + xlo, lb, bar);
-        tma_load(smem_u32(base + offR), k.RPp + (size_t)y * k.Wp + 9 * g0, rb, bar);
-    };
+    const int y0 = dy > 0 ? ylo : yhi;
 
     if (threadIdx.x == 0) {
-        for (int b = 0; b < nslots; b++) mbar_init(smem_u32(&bars[b]), 1);
+        for (int b = 0; b < kRowSlots; b++) {
+            mbar_init(smem_u32(&full[b]), 1);
+            mbar_init(smem_u32(&empty[b]), G);
+        }
         fence_mbar_init();
     }
     __syncthreads();
-    int issued = 0;
-    if (threadIdx.x == 0) {
-        for (; issued < nslots && issued < nrows; issued++) issue(issued);
+
+    if (warp == G) {
+        // ---- producer ----
+        if (lane == 0) {
+            int i = 0;
+            bool ok = true;
+            for (; i < nrows; i++) {
+                const int b = i & (kRowSlots - 1);
+                if (i >= kRowSlots && !mbar_wait(smem_u32(&empty[b]), (uint32_t)((i / kRowSlots) - 1) & 1u)) {
+                    ok = false;
+                    break;
+                }
+                const int y = y0 + dy * i;
+                const int xf = kf + s * y;
+                const int xlo = max(xf, 0), xhi = min(xf + Gb, k.W);
+                const int npx = xhi - xlo;
+                const int g0 = max(0, xlo - DSPAN + 2) >> 3, g1 = (xhi - 1) >> 3;
+                unsigned char* base = slots + b * slotBytes;
+                const uint32_t bar = smem_u32(&full[b]);
+                const uint32_t sb = MODE != 0 ? (uint32_t)npx * SB : 0u;
+                const uint32_t lb = (uint32_t)npx * 16;
+                const uint32_t rb = (uint32_t)(g1 - g0 + 1) * kGroupBytes;
+                fence_proxy_async();
+                mbar_expect_tx(bar, sb + lb + rb);
+                if (MODE != 0)
+                    tma_load(smem_u32(base + (xlo - xf) * SB), k.S + ((size_t)y * k.W + xlo) * k.Dp2, sb, bar);
+                tma_load(smem_u32(base + offL + (xlo - xf) * 16), k.LP + (size_t)y * k.W + xlo, lb, bar);
+                tma_load(smem_u32(base + offR), k.RPp + (size_t)y * k.Wp + 9 * g0, rb, bar);
+            }
+            if (!ok) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
+            // the block must not retire with copies in flight
+            for (int r = max(0, i - kRowSlots); r < i; r++)
+                mbar_wait(smem_u32(&full[r & (kRowSlots - 1)]), (uint32_t)(r / kRowSlots) & 1u,
+                          ok ? kWaitNs : kDrainNs);
+        }
+        return;
     }
 
+    // ---- consumers ----
     const int kp = kf + warp;
     const bool has_line = warp < Gb;
     const int base_d = lane * 2 * PPL;
-    bool started = false, ok = true;
+    const bool edge_lane = base_d + 2 * PPL > k.D;  // holds disparities >= D
+    const uint32_t* lp_slot = (const uint32_t*)(slots + offL + warp * 16);
+    const uint32_t* sv_slot = (const uint32_t*)(slots + warp * SB) + lane * PPL;
+    const long long step_px = (long long)dy * (k.W + s);  // pixel-index step per row
+    bool started = false;
     uint32_t L[PPL], m = 0;
+    uint32_t* sg = nullptr;
 
     for (int i = 0; i < nrows; i++) {
-        const int slot = i % nslots;
-        ok = ok && mbar_wait(smem_u32(&bars[slot]), (uint32_t)(i / nslots) & 1u);
-        const int y = row_of(i);
-        const int xf = kf + s * y;
+        const int b = i & (kRowSlots - 1);
+        if (!__all_sync(FULL, mbar_wait(smem_u32(&full[b]), (uint32_t)(i / kRowSlots) & 1u))) {
+            if (lane == 0) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
+            return;
+        }
+        const int y = y0 + dy * i;
         const int x = kp + s * y;
-        if (ok && has_line && x >= 0 && x < k.W) {
-            const unsigned char* base = slots + slot * slotBytes;
-            const uint4 lp = *(const uint4*)(base + offL + (x - xf) * 16);
-            const int g0 = max(0, max(xf, 0) - DSPAN + 2) >> 3;
-            const Plane* rseg = (const Plane*)(base + offR);
-            const int lim = min(x + 1, k.D);
+        if (has_line && x >= 0 && x < k.W) {
+            const int boff = b * slotBytes;
+            const uint4 lp = *(const uint4*)((const unsigned char*)lp_slot + boff);
+            const int xlo = max(kf + s * y, 0);
+            const int roff = -9 * (max(0, xlo - DSPAN + 2) >> 3);
+            const Plane* rseg = (const Plane*)(slots + boff + offR);
             uint32_t c[PPL], Ln[PPL];
+            const int eb = x - base_d;
 #pragma unroll
             for (int q = 0; q < PPL; q++) {
-                const int d = base_d + 2 * q;
-                const int e = max(x - d, 0);
-                const uint4 rp = *(const uint4*)&rseg[ppos(e) - 9 * g0];
-                c[q] = mask_pair(bt_pair(lp, rp), d, lim, k.BIGBIG);
+                const int e = max(eb - 2 * q, 0);
+                c[q] = bt_pair(lp, *(const uint4*)&rseg[ppos(e) + roff]);
+            }
+            const int lim = min(x + 1, k.D);
+            if (edge_lane || eb < 2 * PPL) {
+#pragma unroll
+                for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
             }
             if (!started) {
 #pragma unroll
                 for (int q = 0; q < PPL; q++) Ln[q] = c[q];
                 started = true;
+                sg = k.S + ((size_t)y * k.W + x) * k.Dp2 + lane * PPL;
             } else {
                 recur<PPL>(L, m, c, Ln, lane, k);
+                sg += step_px * k.Dp2;
             }
-            uint32_t* sg = k.S + ((size_t)y * k.W + x) * k.Dp2 + lane * PPL;
             if (MODE == 0) {
                 Vec<PPL>::st(sg, Ln);
             } else {
                 uint32_t sv[PPL];
-                Vec<PPL>::lds((const uint32_t*)(base + (x - xf) * SB) + lane * PPL, sv);
+                Vec<PPL>::lds((const uint32_t*)((const unsigned char*)sv_slot + boff), sv);
 #pragma unroll
                 for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
                 Vec<PPL>::st(sg, sv);
@@ -361,32 +408,25 @@ __global__ void __launch_bounds__(kMaxG * 32, 1)
             for (int q = 0; q < PPL; q++) L[q] = Ln[q];
             m = warp_min_pairs<PPL>(L);
         }
-        // every thread is done with this slot: refill it with row i + nslots
-        if (__syncthreads_or(ok ? 0 : 1)) {
-            if (threadIdx.x == 0) {
-                atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
-                for (int r = i + 1; r < issued; r++)
-                    mbar_wait(smem_u32(&bars[r % nslots]), (uint32_t)(r / nslots) & 1u);
-                mbar_wait(smem_u32(&bars[slot]), (uint32_t)(i / nslots) & 1u);
-            }
-            return;
-        }
-        if (threadIdx.x == 0 && issued < nrows) {
-            fence_proxy_async();
-            issue(issued);
-            issued++;
-        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&empty[b]));
     }
 }
 
 // ------------------------------------------------------ horizontal passes
 // One warp per image row, walking x in direction dx.  MODE 1: S += L;
 // MODE 2: final S -> WTA (+ right-view disparity and left-right check).
+// The right-view disparity dR(xr) = argmin_d S(xr+d, d) is carried in
+// registers: lane l keeps the running minimum for the 2*PPL right pixels
+// xr = x - base_d - j its disparities reach at column x; stepping to x-1
+// shifts them by one and takes the lane-above's finished entry by shuffle, and
+// lane 0's entry for xr = x is complete.  (Only launched with dx = -1.)
 template <int PPL, int MODE>
 __global__ void __launch_bounds__(kMaxGH * 32, 1) h_pass(FK k, int dx, int GH, int warp_bytes) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int SB = 128 * PPL;
     constexpr int DSPAN = 64 * PPL;
+    constexpr int NJ = 2 * PPL;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y = blockIdx.x * GH + warp;
     if (y >= k.H) return;  // warps are independent: no block-wide barrier below
@@ -395,8 +435,7 @@ __global__ void __launch_bounds__(kMaxGH * 32, 1) h_pass(FK k, int dx, int GH, i
     uint64_t* cbar = sbar + kHSlots;    // kChunkSlots barriers
     unsigned char* sring = wbase + 128;
     unsigned char* cring = sring + kHSlots * SB;
-    uint32_t* lrring = (uint32_t*)(cring + kChunkSlots * kChunkBytes);
-    uint16_t* rowL = (uint16_t*)(lrring + kRing);
+    uint16_t* rowL = (uint16_t*)(cring + kChunkSlots * kChunkBytes);
     uint16_t* rowR = rowL + k.W;
     const bool lr = MODE == 2 && k.lr_thr >= 0;
 
@@ -411,129 +450,99 @@ __global__ void __launch_bounds__(kMaxGH * 32, 1) h_pass(FK k, int dx, int GH, i
         for (int b = 0; b < kHSlots + kChunkSlots; b++) mbar_init(smem_u32(&sbar[b]), 1);
         fence_mbar_init();
     }
-    if (lr)
-        for (int i = lane; i < kRing; i += 32) lrring[i] = 0xFFFFFFFFu;
     __syncwarp();
 
-    auto cl_of = [&](int x) { return max(0, x - DSPAN + 2) / kChunk; };
-    auto ch_of = [&](int x) { return x / kChunk; };
+    auto cl_of = [&](int x) { return max(0, x - DSPAN + 2) >> 6; };
     auto chunk_use = [&](int c) { return dx > 0 ? c / kChunkSlots : (nch - 1 - c) / kChunkSlots; };
+    auto chunk_bar = [&](int c) { return smem_u32(&cbar[c & (kChunkSlots - 1)]); };
     auto issue_chunk = [&](int c) {
         const int ng = min(kChunk / 8, groups_row - c * (kChunk / 8));
-        const uint32_t bar = smem_u32(&cbar[c % kChunkSlots]);
+        const uint32_t bar = chunk_bar(c);
+        fence_proxy_async();
         mbar_expect_tx(bar, (uint32_t)ng * kGroupBytes);
-        tma_load(smem_u32(cring + (c % kChunkSlots) * kChunkBytes), rrow + 9 * (c * (kChunk / 8)),
+        tma_load(smem_u32(cring + (c & (kChunkSlots - 1)) * kChunkBytes), rrow + 9 * (c * (kChunk / 8)),
                  (uint32_t)ng * kGroupBytes, bar);
     };
     auto issue_s = [&](int t) {
         const int x = x0 + dx * t;
-        const uint32_t bar = smem_u32(&sbar[t % kHSlots]);
+        const uint32_t bar = smem_u32(&sbar[t & (kHSlots - 1)]);
+        fence_proxy_async();
         mbar_expect_tx(bar, SB);
-        tma_load(smem_u32(sring + (t % kHSlots) * SB), srow + (size_t)x * k.Dp2, SB, bar);
-    };
-    auto drain_chunks = [&](int waited_c, int next) {
-        if (dx > 0)
-            for (int c = waited_c + 1; c < next; c++)
-                mbar_wait(smem_u32(&cbar[c % kChunkSlots]), (uint32_t)chunk_use(c) & 1u);
-        else
-            for (int c = waited_c - 1; c > next; c--)
-                mbar_wait(smem_u32(&cbar[c % kChunkSlots]), (uint32_t)chunk_use(c) & 1u);
+        tma_load(smem_u32(sring + (t & (kHSlots - 1)) * SB), srow + (size_t)x * k.Dp2, SB, bar);
     };
 
-    // chunks: next to issue and the last one waited for
-    int next_c = dx > 0 ? 0 : nch - 1;
-    int waited = dx > 0 ? -1 : nch;
-    int s_issued = 0;
-    if (lane == 0) {
-        for (; s_issued < kHSlots && s_issued < W; s_issued++) issue_s(s_issued);
+    // Right-plane chunks: the window [x-DSPAN+2, x] is resident and kLookC
+    // chunks beyond it are in flight.  `need` is the next chunk to wait for,
+    // `next` the next to issue, both moving in the walk direction.
+    int need, next;
+    if (dx > 0) {
+        need = 0;
+        next = 0;
+        if (lane == 0)
+            for (; next < nch && next <= kLookC; next++) issue_chunk(next);
+    } else {
+        need = nch - 1;
+        next = nch - 1;
+        if (lane == 0)
+            for (; next >= 0 && next >= cl_of(W - 1) - kLookC; next--) issue_chunk(next);
     }
+    int s_issued = 0;
+    if (lane == 0)
+        for (; s_issued < kHSlots && s_issued < W; s_issued++) issue_s(s_issued);
+    next = __shfl_sync(FULL, next, 0);
+    s_issued = __shfl_sync(FULL, s_issued, 0);
+
     bool ok = true;
     const int base_d = lane * 2 * PPL;
-    uint32_t L[PPL], m = 0, s[PPL];
-    uint4 lp_next = __ldg((const uint4*)&k.LP[(size_t)y * W + x0]);
-
-    auto finish = [&](int x, const uint32_t* sv) {
-        uint32_t key = FULL;
+    const bool edge_lane = base_d + 2 * PPL > k.D;
+    uint32_t L[PPL], m = 0, sv[PPL];
+    uint32_t P[NJ];  // right-view running minima (MODE 2, dx = -1)
 #pragma unroll
-        for (int q = 0; q < PPL; q++) {
-            const uint32_t d = base_d + 2 * q;
-            key = min(key, ((sv[q] & 0xFFFFu) << 8) | d);
-            key = min(key, ((sv[q] >> 16) << 8) | (d + 1));
-            if (lr) {
-                const int xr0 = x - (int)d, xr1 = xr0 - 1;
-                if (xr0 >= 0) {
-                    uint32_t& r0 = lrring[xr0 & (kRing - 1)];
-                    r0 = min(r0, ((sv[q] & 0xFFFFu) << 8) | d);
-                }
-                if (xr1 >= 0) {
-                    uint32_t& r1 = lrring[xr1 & (kRing - 1)];
-                    r1 = min(r1, ((sv[q] >> 16) << 8) | (d + 1));
-                }
-            }
-        }
-        key = __reduce_min_sync(FULL, key);
-        const uint16_t dl = (uint16_t)(key & 0xFFu);
-        if (lr) {
-            __syncwarp();
-            if (lane == 0) {
-                uint32_t& r = lrring[x & (kRing - 1)];
-                rowR[x] = (uint16_t)(r & 0xFFu);
-                r = 0xFFFFFFFFu;
-                rowL[x] = dl;
-            }
-            __syncwarp();
-        } else if (lane == 0) {
-            const size_t o = (size_t)y * W + x;
-            if (k.disp) k.disp[o] = dl;
-            if (k.disp_norm) k.disp_norm[o] = __fdiv_rn((float)dl, (float)k.D);
-        }
-    };
+    for (int j = 0; j < NJ; j++) P[j] = FULL;
+    uint4 lp_next = __ldg((const uint4*)&k.LP[(size_t)y * W + x0]);
+    uint32_t* sg = k.S + ((size_t)y * W + x0) * k.Dp2 + lane * PPL;
+    const long long sstep = (long long)dx * k.Dp2;
 
     int t = 0;
     for (; t < W; t++) {
         const int x = x0 + dx * t;
-        // keep the right-plane window [x-DSPAN+2, x] resident, kLookC chunks ahead
-        if (lane == 0) {
-            if (dx > 0) {
-                while (next_c < nch && next_c <= ch_of(x) + kLookC && cl_of(x) > next_c - kChunkSlots) {
-                    fence_proxy_async();
-                    issue_chunk(next_c++);
-                }
-            } else {
-                while (next_c >= 0 && next_c >= cl_of(x) - kLookC && ch_of(x) < next_c + kChunkSlots) {
-                    fence_proxy_async();
-                    issue_chunk(next_c--);
-                }
-            }
-        }
-        next_c = __shfl_sync(FULL, next_c, 0);
         bool good = true;
         if (dx > 0) {
-            while (good && waited < ch_of(x)) {
-                waited++;
-                good = mbar_wait(smem_u32(&cbar[waited % kChunkSlots]), (uint32_t)chunk_use(waited) & 1u);
+            if ((x & (kChunk - 1)) == 0) {
+                const int c = x >> 6;
+                if (lane == 0 && next < nch) issue_chunk(next);
+                if (next < nch) next++;
+                good = mbar_wait(chunk_bar(c), (uint32_t)chunk_use(c) & 1u);
+                need = c + 1;
             }
         } else {
-            while (good && waited > cl_of(x)) {
-                waited--;
-                good = mbar_wait(smem_u32(&cbar[waited % kChunkSlots]), (uint32_t)chunk_use(waited) & 1u);
+            const int cl = cl_of(x);
+            while (good && need >= cl) {
+                good = mbar_wait(chunk_bar(need), (uint32_t)chunk_use(need) & 1u);
+                need--;
+            }
+            if (next >= 0 && next >= cl - kLookC) {
+                if (lane == 0) issue_chunk(next);
+                next--;
             }
         }
-        good = good && mbar_wait(smem_u32(&sbar[t % kHSlots]), (uint32_t)(t / kHSlots) & 1u);
+        good = good && mbar_wait(smem_u32(&sbar[t & (kHSlots - 1)]), (uint32_t)(t / kHSlots) & 1u);
         ok = __all_sync(FULL, good);
         if (!ok) break;
 
         const uint4 lp = lp_next;
         if (t + 1 < W) lp_next = __ldg((const uint4*)&k.LP[(size_t)y * W + x + dx]);
-        const int lim = min(x + 1, k.D);
         uint32_t c[PPL], Ln[PPL];
+        const int eb = x - base_d;
 #pragma unroll
         for (int q = 0; q < PPL; q++) {
-            const int d = base_d + 2 * q;
-            const int e = max(x - d, 0);
-            const int c_e = e / kChunk, w_e = e % kChunk;
-            const uint4 rp = *(const uint4*)(cring + (c_e % kChunkSlots) * kChunkBytes + ppos(w_e) * 16);
-            c[q] = mask_pair(bt_pair(lp, rp), d, lim, k.BIGBIG);
+            const int e = max(eb - 2 * q, 0);
+            c[q] = bt_pair(lp, *(const uint4*)(cring + ppos(e & (kChunkSlots * kChunk - 1)) * 16));
+        }
+        if (edge_lane || eb < 2 * PPL) {
+            const int lim = min(x + 1, k.D);
+#pragma unroll
+            for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
         }
         if (t == 0) {
 #pragma unroll
@@ -541,32 +550,68 @@ __global__ void __launch_bounds__(kMaxGH * 32, 1) h_pass(FK k, int dx, int GH, i
         } else {
             recur<PPL>(L, m, c, Ln, lane, k);
         }
-        Vec<PPL>::lds((const uint32_t*)(sring + (t % kHSlots) * SB) + lane * PPL, s);
+        Vec<PPL>::lds((const uint32_t*)(sring + (t & (kHSlots - 1)) * SB) + lane * PPL, sv);
 #pragma unroll
-        for (int q = 0; q < PPL; q++) s[q] += Ln[q];
-        if (MODE == 1) Vec<PPL>::st(k.S + ((size_t)y * W + x) * k.Dp2 + lane * PPL, s);
-        else finish(x, s);
+        for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
+        if (MODE == 1) {
+            Vec<PPL>::st(sg, sv);
+        } else {
+            // WTA key (S << 8 | d): lowest S, then lowest d (tdvision/wtacpu.cpp:26-30)
+            uint32_t key[NJ];
+#pragma unroll
+            for (int q = 0; q < PPL; q++) {
+                key[2 * q] = ((sv[q] & 0xFFFFu) << 8) | (uint32_t)(base_d + 2 * q);
+                key[2 * q + 1] = ((sv[q] >> 16) << 8) | (uint32_t)(base_d + 2 * q + 1);
+            }
+            uint32_t kmin = key[0];
+#pragma unroll
+            for (int j = 1; j < NJ; j++) kmin = min(kmin, key[j]);
+            kmin = __reduce_min_sync(FULL, kmin);
+            if (lr) {
+#pragma unroll
+                for (int j = 0; j < NJ; j++) P[j] = min(P[j], key[j]);
+                uint32_t in = __shfl_down_sync(FULL, P[0], 1);
+                if (lane == 31) in = FULL;
+                if (lane == 0) {
+                    rowR[x] = (uint16_t)(P[0] & 0xFFu);
+                    rowL[x] = (uint16_t)(kmin & 0xFFu);
+                }
+#pragma unroll
+                for (int j = 0; j < NJ - 1; j++) P[j] = P[j + 1];
+                P[NJ - 1] = in;
+            } else if (lane == 0) {
+                const size_t o = (size_t)y * W + x;
+                const uint16_t dl = (uint16_t)(kmin & 0xFFu);
+                if (k.disp) k.disp[o] = dl;
+                if (k.disp_norm) k.disp_norm[o] = __fdiv_rn((float)dl, (float)k.D);
+            }
+        }
+        sg += sstep;
 #pragma unroll
         for (int q = 0; q < PPL; q++) L[q] = Ln[q];
         m = warp_min_pairs<PPL>(L);
         __syncwarp();
-        if (lane == 0 && s_issued < W) {
-            fence_proxy_async();
-            issue_s(s_issued++);
+        if (s_issued < W) {
+            if (lane == 0) issue_s(s_issued);
+            s_issued++;
         }
     }
 
-    if (!ok) {
-        if (lane == 0) {
-            atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
-            for (int r = t; r < s_issued; r++)
-                mbar_wait(smem_u32(&sbar[r % kHSlots]), (uint32_t)(r / kHSlots) & 1u);
-            drain_chunks(waited, next_c);
+    // copies still in flight (chunks fetched ahead, or the tail after a
+    // failed wait) must land before the warp's shared memory can be reused
+    if (lane == 0) {
+        const uint64_t lim = ok ? kWaitNs : kDrainNs;
+        for (int r = t + 1; r < s_issued; r++)
+            mbar_wait(smem_u32(&sbar[r & (kHSlots - 1)]), (uint32_t)(r / kHSlots) & 1u, lim);
+        if (!ok) mbar_wait(smem_u32(&sbar[t & (kHSlots - 1)]), (uint32_t)(t / kHSlots) & 1u, lim);
+        if (dx > 0) {
+            for (int c = need; c < next; c++) mbar_wait(chunk_bar(c), (uint32_t)chunk_use(c) & 1u, lim);
+        } else {
+            for (int c = need; c > next; c--) mbar_wait(chunk_bar(c), (uint32_t)chunk_use(c) & 1u, lim);
         }
-        return;
+        if (!ok) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
     }
-    // chunks fetched ahead but never needed still have copies in flight
-    if (lane == 0) drain_chunks(waited, next_c);
+    if (!ok) return;
 
     if (lr) {
         __syncwarp();
@@ -597,15 +642,13 @@ cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
     const int SB = 128 * PPL, DSPAN = 64 * PPL;
     const int NRG = (G + DSPAN) / 8 + 2;
     const int slotBytes = align128(G * SB + G * 16 + NRG * kGroupBytes);
-    int nslots = (kSmemBudget - 128) / slotBytes;
-    nslots = nslots > kRowSlots ? kRowSlots : nslots;
-    if (nslots < 2) return cudaErrorInvalidConfiguration;
-    const int smem = 128 + nslots * slotBytes;
+    const int smem = 2 * kRowSlots * 8 + kRowSlots * slotBytes;
+    if (smem > kSmemBudget) return cudaErrorInvalidConfiguration;
     cudaError_t e =
         cudaFuncSetAttribute(vd_pass<PPL, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     const int blocks = (nlines + G - 1) / G;
-    vd_pass<PPL, MODE><<<blocks, G * 32, smem, st>>>(k, s, dy, kmin, nlines, G, nslots);
+    vd_pass<PPL, MODE><<<blocks, (G + 1) * 32, smem, st>>>(k, s, dy, kmin, nlines, G);
     return cudaGetLastError();
 }
 
@@ -613,8 +656,7 @@ template <int PPL, int MODE>
 cudaError_t launch_h(const FK& k, int dx, cudaStream_t st) {
     const int SB = 128 * PPL;
     const bool lr = MODE == 2 && k.lr_thr >= 0;
-    const int warp_bytes = align128(128 + kHSlots * SB + kChunkSlots * kChunkBytes +
-                                    (lr ? kRing * 4 + 2 * k.W * 2 : 0));
+    const int warp_bytes = align128(128 + kHSlots * SB + kChunkSlots * kChunkBytes + (lr ? 2 * k.W * 2 : 0));
     int GH = kSmemBudget / warp_bytes;
     GH = GH > kMaxGH ? kMaxGH : GH;
     if (GH < 1) return cudaErrorInvalidConfiguration;

@@ -95,6 +95,8 @@ struct tdv_ctx {
     Buf codes;    // DP choice codes
     Buf misc;     // small per-call scratch
     Buf err;      // one device int: error status written by kernels
+    Buf soft;     // soft-SGM: dS volume / inference-mode S and statistics
+    std::vector<long long> ckpt_off_host;
 
     tdv::PassSchedule sched;
     Buf sched_buf;
@@ -157,5 +159,26 @@ struct FusedArgs {
 size_t fused_agg_bytes(int W, int H, int D);
 size_t fused_plane_bytes(int W, int H);
 cudaError_t launch_fused(const FusedArgs& a, cudaStream_t st, Timer* tm);
+
+// Differentiable soft-argmin SGM (kernels_soft.cu).
+struct SoftLaunch {
+    int f64;
+    const void* cost;
+    void* S;
+    void* dS;
+    void* dcost;
+    void* codes;
+    void* kstar;
+    void* ckpt;
+    const long long* ckpt_off;
+    void* dhat;
+    void* stats;
+    const void* g;
+    void* dpen;
+    int W, H, D, paths, ck, record;
+    double p1, p2, tau;
+};
+cudaError_t launch_soft_forward(const SoftLaunch& a, cudaStream_t st, Timer* tm);
+cudaError_t launch_soft_backward(const SoftLaunch& a, cudaStream_t st, Timer* tm);
 
 }  // namespace tdv
