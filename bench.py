@@ -244,18 +244,25 @@ def run_ours(args):
     dl = torch.empty((H, W), dtype=torch.uint8, device=dev)
     dr = torch.empty((H, W), dtype=torch.uint8, device=dev)
     e2e_ms = 0.0
+    parts = [0.0, 0.0, 0.0]
+    clk2 = Clocks(local)
     for i in range(args.steps):
         flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         pl, pr = pinned[i % len(pinned)]
-        e0.record(st)
+        ev[0].record(st)
         dl.copy_(pl, non_blocking=True)
         dr.copy_(pr, non_blocking=True)
+        ev[1].record(st)
         out = ctx.stereo_sgm(dl, dr, D, P1, P2, paths=PATHS, lr=LR)
+        ev[2].record(st)
         host_out.copy_(out["disp"], non_blocking=True)
-        e1.record(st)
-        e1.synchronize()
-        e2e_ms += e0.elapsed_time(e1)
+        ev[3].record(st)
+        ev[3].synchronize()
+        e2e_ms += ev[0].elapsed_time(ev[3])
+        for j in range(3):
+            parts[j] += ev[j].elapsed_time(ev[j + 1])
+    clocks_e2e = clk2.stop()
 
     t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
     if world > 1:
@@ -298,7 +305,9 @@ def run_ours(args):
         "config": config({"parallelism": f"replicas x{world}, frames sharded by rank"}),
         "gcells_per_s": cells * fps / 1e9,
         "e2e": {"value": e2e_fps, "unit": UNIT, "h2d_bytes_per_step": 2 * W * H,
-                "d2h_bytes_per_step": 2 * W * H},
+                "d2h_bytes_per_step": 2 * W * H,
+                "ms_per_step": {"h2d": parts[0] / args.steps, "stereo_sgm": parts[1] / args.steps,
+                                "d2h": parts[2] / args.steps}, "clocks": clocks_e2e},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks

@@ -28,6 +28,7 @@ EXPORTS = [
     "tdv_ctx_create", "tdv_ctx_destroy", "tdv_ctx_set_allocator", "tdv_ctx_reserve",
     "tdv_last_error_string", "tdv_status_string", "tdv_version", "tdv_volume_bytes",
     "tdv_ctx_enable_timing", "tdv_ctx_timings", "tdv_ctx_timing_name", "tdv_ctx_device_status",
+    "tdv_soft_sgm_tape_bytes", "tdv_soft_sgm_forward", "tdv_soft_sgm_backward",
 ]
 
 
@@ -53,6 +54,11 @@ class tdv_cost_params(ctypes.Structure):
 class tdv_sgm_params(ctypes.Structure):
     _fields_ = [("p1", ctypes.c_float), ("p2", ctypes.c_float), ("p2_mode", ctypes.c_int32),
                 ("paths", ctypes.c_int32), ("table", ctypes.c_int32), ("semantics", ctypes.c_int32)]
+
+
+class tdv_soft_params(ctypes.Structure):
+    _fields_ = [("p1", ctypes.c_float), ("p2", ctypes.c_float), ("paths", ctypes.c_int32),
+                ("tau", ctypes.c_float), ("checkpoint", ctypes.c_int32)]
 
 
 ALLOC_FN = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
@@ -94,6 +100,10 @@ def _declare(lib):
         "tdv_ctx_timing_name": (ctypes.c_char_p, [vp, ctypes.c_int32]),
         "tdv_ctx_device_status": (st, [vp, vp]),
         "tdv_volume_bytes": (ctypes.c_size_t, [ctypes.c_int32] * 4),
+        "tdv_soft_sgm_tape_bytes": (ctypes.c_size_t, [ctypes.c_int32] * 4 + [P(tdv_soft_params)]),
+        "tdv_soft_sgm_forward": (st, [vp, P(tdv_volume), P(tdv_soft_params), vp, vp, ctypes.c_size_t, vp]),
+        "tdv_soft_sgm_backward": (st, [vp, P(tdv_volume), P(tdv_soft_params), vp, ctypes.c_size_t, vp,
+                                       P(tdv_volume), vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
