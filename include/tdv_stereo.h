@@ -146,6 +146,20 @@ tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* 
                           int32_t max_disp, const tdv_sgm_params* params, tdv_disparity* out,
                           tdv_stream stream);
 
+/* Allocation-free variant of tdv_stereo_sgm's fused integer-domain path, for
+ * callers that cannot call cudaMalloc while they run (a capture or control
+ * loop with a device-memory budget fixed at start-up, a plugin whose host owns
+ * every allocation, a real-time frame loop that must not stall on an
+ * allocation).  It has no counterpart in the reference.  All scratch comes
+ * from one 64 MiB static __device__ array held by every GPU that loads this
+ * library until the process exits; pairs whose scratch exceeds it (about
+ * W*H*(34 + 128*ceil(D/64)) bytes) are rejected with TDV_ERR_UNSUPPORTED, as
+ * are inputs outside the fused path.  The first call on a device resolves the
+ * array's address there; make it before any stream capture.  Calls share the
+ * array: calls whose GPU work overlaps race. */
+tdv_status tdv_stereo_sgm_static(const tdv_image* left, const tdv_image* right, int32_t max_disp,
+                                 const tdv_sgm_params* params, tdv_disparity* out, tdv_stream stream);
+
 /* ---- differentiable soft-argmin SGM (no reference counterpart) --------- */
 typedef struct {
     float p1, p2;       /* penalties, constant P2 */
