@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--frames", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batch and soft-SGM measurements")
     return ap.parse_args()
 
 
@@ -154,6 +156,130 @@ def run_reference(args):
                              "sample": desc},
             "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------- extra metrics
+def _event_ms(fn, reps, warm, st):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        fn()
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def measure_batch(ctx, dev, reps=3):
+    """Uneven batch: 64 seeded pairs, W ~ U[320,1920], H ~ U[240,1080] (multiples
+    of 16), D in {32,64,128,256}; BT + SGM-8 + WTA.  One graph-captured
+    persistent launch with autotuned tiles vs (a) 64 per-pair launches of the
+    plain method -- BT cost DSI (tdv_cost, FP32) then SGM + WTA (tdv_sgm) --
+    and (b) 64 per-pair launches of the fused path (tdv_stereo_sgm); outputs
+    and the DSI preallocated, all on one stream, device time."""
+    import ctypes
+
+    import torch
+
+    from thundervision_b200 import _lib, api, synthetic
+    shapes = synthetic.batch_shapes(seed=0, n=64)
+    pairs = []
+    for i, (w, h, d) in enumerate(shapes):
+        l, r, _, _ = synthetic.pair_sized(w, h, d, synthetic.pair_seed(0, i) % (2 ** 31))
+        pairs.append((torch.from_numpy(l).to(dev), torch.from_numpy(r).to(dev), d))
+    cells = sum(w * h * d * 8 for (w, h, d) in shapes)
+    st = torch.cuda.current_stream()
+    lib = _lib.lib()
+    prm = _lib.tdv_sgm_params(P1, P2, _lib.P2_CONST, 8, _lib.TABLE_FULL, _lib.SEM_STANDARD)
+    outs = [torch.empty(l.shape, dtype=torch.uint16, device=dev) for (l, r, d) in pairs]
+    calls = [(api._image(l), api._image(r), d, _lib.tdv_disparity(o.data_ptr(), None, None, -1))
+             for (l, r, d), o in zip(pairs, outs)]
+    ctx.reserve(max(s[0] for s in shapes), max(s[1] for s in shapes), 256)
+
+    def per_pair():
+        sp = api._stream()
+        for li, ri, d, o in calls:
+            ctx.check(lib.tdv_stereo_sgm(ctx.handle, ctypes.byref(li), ctypes.byref(ri), d,
+                                         ctypes.byref(prm), ctypes.byref(o), sp))
+
+    t_pair = _event_ms(per_pair, reps, 1, st)
+    fused_ref = [o.clone() for o in outs]
+
+    maxc = max(w * h * d for (w, h, d) in shapes)
+    dsi = torch.empty(maxc, dtype=torch.float32, device=dev)
+    cprm = _lib.tdv_cost_params(_lib.COST_BT, 0)
+    plain_calls = []
+    for (l, r, d), o in zip(pairs, outs):
+        h, w = l.shape
+        plain_calls.append((api._image(l), api._image(r), _lib.tdv_volume(dsi.data_ptr(), w, h, d, _lib.LAYOUT_HWD,
+                                                                           _lib.F32),
+                            _lib.tdv_disparity(o.data_ptr(), None, None, -1)))
+
+    def per_pair_plain():
+        sp = api._stream()
+        for li, ri, v, o in plain_calls:
+            ctx.check(lib.tdv_cost(ctx.handle, ctypes.byref(li), ctypes.byref(ri), ctypes.byref(cprm),
+                                   ctypes.byref(v), sp))
+            ctx.check(lib.tdv_sgm(ctx.handle, ctypes.byref(v), None, ctypes.byref(prm), None, ctypes.byref(o),
+                                  sp))
+
+    t_plain = _event_ms(per_pair_plain, 1, 1, st)
+    plain_equal = all(torch.equal(o, ref) for o, ref in zip(outs, fused_ref))
+    del dsi
+    b = api.Batch(ctx, pairs, P1, P2, paths=8)
+    t_default = _event_ms(b.run, reps, 1, st)
+    tiles, t_tune = b.autotune(reps=2)
+    t_run = _event_ms(b.run, reps, 1, st)
+    t_graph = _event_ms(b.graph_launch, reps, 1, st)
+    b.status()
+    equal = all(torch.equal(o["disp"], ref) for o, ref in zip(b.outputs, fused_ref))
+    n_items = b.work_queue()[1]
+    b.close()
+    return {"workload": "64 pairs, W~U[320,1920], H~U[240,1080] (x16), D in {32,64,128,256}, "
+                        "BT + SGM-8 + WTA, seed 0",
+            "pairs": len(shapes), "cells": cells, "work_items": n_items,
+            "per_pair_plain_ms": t_plain, "per_pair_fused_ms": t_pair, "batch_default_tiles_ms": t_default,
+            "batch_tuned_ms": t_run, "batch_graph_ms": t_graph, "tiles": tiles,
+            "pairs_per_s": len(shapes) / (t_graph / 1000.0),
+            "gcells_per_s": cells / (t_graph / 1000.0) / 1e9,
+            "per_pair_fused_gcells_per_s": cells / (t_pair / 1000.0) / 1e9,
+            "speedup_vs_per_pair_plain": t_plain / t_graph, "speedup_vs_per_pair_fused": t_pair / t_graph,
+            "bit_identical_to_per_pair": equal and plain_equal}
+
+
+def measure_soft(ctx, dev, reps=5):
+    """Soft-argmin SGM at 960x540, D=128, FP32 BT volume, 8 paths, tau=1,
+    checkpoint every 32 steps: forward (recording the tape) + adjoint vs the
+    plain forward (no tape) and vs the hard SGM + WTA on the same volume."""
+    import torch
+
+    from thundervision_b200 import soft, synthetic
+    l, r, gt, _ = synthetic.make_pair(960, 540, 128, 17, n_rects=8, slanted=True, salt_pepper=0.02)
+    cost = ctx.cost(torch.from_numpy(l).to(dev), torch.from_numpy(r).to(dev), 128)
+    gt_t = torch.from_numpy(gt.astype("float32")).to(dev)
+    st = torch.cuda.current_stream()
+    p = torch.tensor([P1, P2], dtype=torch.float32, device=dev, requires_grad=True)
+    c = cost.clone().requires_grad_(True)
+
+    def fwd_bwd():
+        dh = soft.soft_sgm(c, p[0], p[1], tau=1.0, paths=8, checkpoint=32, ctx=ctx)
+        (dh - gt_t).abs().mean().backward()
+
+    def fwd_plain():
+        soft.soft_sgm_infer(cost, P1, P2, tau=1.0, paths=8, ctx=ctx)
+
+    def hard():
+        ctx.sgm(cost, P1, P2)
+
+    t_fb = _event_ms(fwd_bwd, reps, 2, st)
+    t_f = _event_ms(fwd_plain, reps, 2, st)
+    t_h = _event_ms(hard, reps, 2, st)
+    return {"workload": "960x540, D=128, FP32 BT cost, 8 paths, tau=1, L1 loss, checkpoint 32",
+            "fwd_adjoint_ms": t_fb, "plain_soft_forward_ms": t_f, "hard_sgm_wta_ms": t_h,
+            "ratio_vs_plain_forward": t_fb / t_f, "ratio_vs_hard_sgm": t_fb / t_h}
 
 
 # ------------------------------------------------------------------ ours
@@ -319,6 +445,9 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if not args.no_extras:
+        line["batch"] = measure_batch(ctx, dev)
+        line["soft"] = measure_soft(ctx, dev)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample()
     print(json.dumps(line), flush=True)

@@ -160,11 +160,69 @@ tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* 
 tdv_status tdv_stereo_sgm_static(const tdv_image* left, const tdv_image* right, int32_t max_disp,
                                  const tdv_sgm_params* params, tdv_disparity* out, tdv_stream stream);
 
+/* ---- batched pairs: one persistent launch (no reference counterpart) ----
+ * The reference matches one pair per pipeline update
+ * (tdvision/devstereomatcher.cpp:36-48 chains the cost and optimizer stages
+ * of one frame); these calls run the fused integer-domain path of
+ * tdv_stereo_sgm over many pairs of uneven size and disparity range in one
+ * persistent kernel fed by a device work queue, with results bit-identical
+ * to per-pair tdv_stereo_sgm calls. */
+typedef struct {
+    tdv_image left, right; /* TDV_U8, scale 1, device memory, equal sizes */
+    int32_t max_disp;      /* 1..256 */
+    tdv_disparity out;     /* as for tdv_stereo_sgm */
+} tdv_batch_pair;
+
+typedef enum { TDV_BATCH_ORDER_LONGEST_FIRST = 0, TDV_BATCH_ORDER_INPUT = 1 } tdv_batch_order;
+
+/* Tile shapes of the persistent kernel. */
+typedef struct {
+    int32_t lines_per_cta;   /* vertical/diagonal passes: path lines per block, 1..24 */
+    int32_t rows_per_cta;    /* horizontal passes: image rows per block, 1..25 (12 when split) */
+    int32_t split_disparity; /* horizontal passes, D > 64: 1 = two warps share a row's
+                                disparity range, 0 = one warp per row */
+    int32_t order;           /* tdv_batch_order: pairs inside each pass of the queue */
+} tdv_batch_tiles;
+
+typedef struct tdv_batch tdv_batch;
+
+/* Plans a batch: validates every pair (integer-domain fused path only:
+ * P1/P2 multiples of 1/2, P2 <= 1280, STANDARD, FULL, P2_CONST), allocates
+ * the planes and aggregation volumes of all pairs and the device work queue
+ * from the context's allocator, and uploads the queue built with the default
+ * tiles.  The pair pointers are fixed at creation (a video loop rewrites the
+ * same input buffers and relaunches). */
+tdv_status tdv_batch_create(tdv_ctx* ctx, const tdv_batch_pair* pairs, int32_t n_pairs,
+                            const tdv_sgm_params* params, tdv_batch** out);
+void tdv_batch_destroy(tdv_batch* batch);
+tdv_status tdv_batch_set_tiles(tdv_batch* batch, const tdv_batch_tiles* tiles);
+tdv_status tdv_batch_get_tiles(const tdv_batch* batch, tdv_batch_tiles* tiles);
+/* Times candidate tile shapes on this batch (each run `reps` times on
+ * `stream`, device time by CUDA events), keeps the fastest and returns it
+ * with its milliseconds per run. */
+tdv_status tdv_batch_autotune(tdv_batch* batch, int32_t reps, tdv_stream stream,
+                              tdv_batch_tiles* chosen, double* best_ms);
+/* One run: zero the queue's control words, one persistent launch. */
+tdv_status tdv_batch_run(tdv_batch* batch, tdv_stream stream);
+/* The same run through a CUDA graph, captured on first use (and again after
+ * the tiles change) and replayed on `stream`. */
+tdv_status tdv_batch_graph_launch(tdv_batch* batch, tdv_stream stream);
+/* Synchronises `stream` and returns the device status of the last run:
+ * TDV_ERR_TIMEOUT (a bounded wait ran out), TDV_ERR_BAD_WORK (a work item out
+ * of range), else TDV_OK. */
+tdv_status tdv_batch_status(tdv_batch* batch, tdv_stream stream);
+/* Bounded-wait limit for the kernel's dependency waits (default 2 s). */
+tdv_status tdv_batch_set_wait_limit(tdv_batch* batch, double seconds);
+/* The device work queue (n_items entries of item_bytes: int32 pair*16+pass,
+ * int32 block), pass-major, and the per-pass item counts; for inspection and
+ * for tests that plant faults in the queue. */
+tdv_status tdv_batch_work_queue(tdv_batch* batch, void** items, int32_t* n_items, int32_t* item_bytes);
+
 /* ---- differentiable soft-argmin SGM (no reference counterpart) --------- */
 typedef struct {
-    float p1, p2;       /* penalties, constant P2 */
+    double p1, p2;      /* penalties, constant P2 (double so FP64 runs keep them exact) */
     int32_t paths;      /* 8 or 4 */
-    float tau;          /* softmin temperature, > 0 */
+    double tau;         /* softmin temperature, > 0 */
     int32_t checkpoint; /* 0: the tape keeps 2-bit choice codes of every cell;
                            k in [1,32]: it keeps L every k steps of each path
                            and the adjoint recomputes one k-step segment at a

@@ -192,3 +192,44 @@ def test_injected_allocator_success_is_used(lib):
     assert n >= 2
     lib.tdv_ctx_destroy(h)
     assert sorted(freed) == sorted(blocks)
+
+
+def test_batch_argument_validation(lib, hctx):
+    def pairs(*specs):
+        arr = (L.tdv_batch_pair * len(specs))()
+        for i, (li, ri, D) in enumerate(specs):
+            arr[i] = L.tdv_batch_pair(li, ri, D, _out())
+        return arr
+
+    h = ctypes.c_void_p()
+    ok = pairs((_img(), _img(), 16), (_img(w=32, h=9), _img(w=32, h=9), 64))
+    assert lib.tdv_batch_create(None, ok, 2, B(_params()), B(h)) == L.TDV_ERR_INVALID_ARG
+    assert lib.tdv_batch_create(hctx, ok, 0, B(_params()), B(h)) == L.TDV_ERR_INVALID_ARG
+    assert lib.tdv_batch_create(hctx, None, 2, B(_params()), B(h)) == L.TDV_ERR_INVALID_ARG
+    assert lib.tdv_batch_create(hctx, ok, 2, B(_params()), None) == L.TDV_ERR_INVALID_ARG
+    # only the integer-domain fused path batches
+    for prm in (_params(semantics=L.SEM_REF_CPU), _params(table=L.TABLE_REF), _params(p2_mode=L.P2_ADJUST),
+                _params(p1=10.25), _params(p2=1300.0)):
+        st = lib.tdv_batch_create(hctx, ok, 2, B(prm), B(h))
+        assert st in (L.TDV_ERR_UNSUPPORTED, L.TDV_ERR_INVALID_ARG)
+    cases = [
+        (pairs((_img(dt=L.F32), _img(dt=L.F32), 16)), L.TDV_ERR_UNSUPPORTED, "u8"),
+        (pairs((_img(scale=0.5), _img(scale=0.5), 16)), L.TDV_ERR_UNSUPPORTED, "scale"),
+        (pairs((_img(), _img(), 300)), L.TDV_ERR_UNSUPPORTED, "max_disp"),
+        (pairs((_img(), _img(), 0)), L.TDV_ERR_UNSUPPORTED, "max_disp"),
+        (pairs((_img(), _img(w=9), 16)), L.TDV_ERR_INVALID_ARG, "differ"),
+        (pairs((_img(), _img(ptr=0), 16)), L.TDV_ERR_INVALID_ARG, "pair 0 right"),
+        (pairs((_img(), _img(), 16), (_img(pitch=2), _img(), 16)), L.TDV_ERR_INVALID_ARG, "pair 1 left"),
+    ]
+    for arr, want, msg in cases:
+        assert lib.tdv_batch_create(hctx, arr, len(arr), B(_params()), B(h)) == want, msg
+        assert msg in lib.tdv_last_error_string(hctx).decode()
+    none_out = (L.tdv_batch_pair * 1)()
+    none_out[0] = L.tdv_batch_pair(_img(), _img(), 16, L.tdv_disparity(None, None, None, -1))
+    assert lib.tdv_batch_create(hctx, none_out, 1, B(_params()), B(h)) == L.TDV_ERR_INVALID_ARG
+    t = L.tdv_batch_tiles(8, 8, 0, 0)
+    for fn, args in (("tdv_batch_set_tiles", (B(t),)), ("tdv_batch_get_tiles", (B(t),)),
+                     ("tdv_batch_run", (None,)), ("tdv_batch_graph_launch", (None,)),
+                     ("tdv_batch_status", (None,)), ("tdv_batch_set_wait_limit", (1.0,))):
+        assert getattr(lib, fn)(None, *args) == L.TDV_ERR_INVALID_ARG, fn
+    lib.tdv_batch_destroy(None)

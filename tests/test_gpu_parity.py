@@ -144,6 +144,17 @@ def test_fused_medium(ctx, orc, medium_pair, paths):
     _check_fused(ctx, orc, L, R, 64, 10, 120, paths, 1)
 
 
+@pytest.mark.parametrize("W,H,D", [(640, 96, 128), (640, 96, 256), (1001, 37, 200),
+                                   (257, 64, 129), (1920, 24, 256), (777, 19, 65)])
+@pytest.mark.parametrize("lr", [None, 1])
+def test_fused_wide_large_d(ctx, orc, W, H, D, lr):
+    """Disparity ranges above 64 (two or four disparity pairs per lane, the
+    range split over two warps in the horizontal passes) on rows many
+    right-plane chunks long, including widths that are not chunk multiples."""
+    L, R, _, _ = syn.make_pair(W, H, D, W + 7 * H + D, n_rects=4, slanted=True)
+    _check_fused(ctx, orc, L, R, D, 10, 120, 8, lr)
+
+
 def _check_fused(ctx, orc, L, R, D, p1, p2, paths, lr):
     Lf, Rf = orc.u8_to_f32(L), orc.u8_to_f32(R)
     C = orc.bt_cost(Lf, Rf, D)

@@ -7,12 +7,12 @@ reference's MatchingCost / Optimizer plugin classes.
 """
 from ._lib import TdvError, build, lib  # noqa: F401
 
-__all__ = ["TdvError", "build", "lib", "Context", "default_context"]
+__all__ = ["TdvError", "build", "lib", "Context", "Batch", "default_context"]
 
 
 def __getattr__(name):
     # torch is imported lazily so that the ABI layer loads without it
-    if name in ("Context", "default_context"):
+    if name in ("Context", "Batch", "default_context"):
         from . import api
         return getattr(api, name)
     raise AttributeError(name)

@@ -30,7 +30,11 @@ EXPORTS = [
     "tdv_ctx_enable_timing", "tdv_ctx_timings", "tdv_ctx_timing_name", "tdv_ctx_device_status",
     "tdv_soft_sgm_tape_bytes", "tdv_soft_sgm_forward", "tdv_soft_sgm_backward",
     "tdv_stereo_sgm_static",
+    "tdv_batch_create", "tdv_batch_destroy", "tdv_batch_set_tiles", "tdv_batch_get_tiles",
+    "tdv_batch_autotune", "tdv_batch_run", "tdv_batch_graph_launch", "tdv_batch_status",
+    "tdv_batch_set_wait_limit", "tdv_batch_work_queue",
 ]
+BATCH_ORDER_LONGEST_FIRST, BATCH_ORDER_INPUT = 0, 1
 
 
 class tdv_image(ctypes.Structure):
@@ -58,8 +62,18 @@ class tdv_sgm_params(ctypes.Structure):
 
 
 class tdv_soft_params(ctypes.Structure):
-    _fields_ = [("p1", ctypes.c_float), ("p2", ctypes.c_float), ("paths", ctypes.c_int32),
-                ("tau", ctypes.c_float), ("checkpoint", ctypes.c_int32)]
+    _fields_ = [("p1", ctypes.c_double), ("p2", ctypes.c_double), ("paths", ctypes.c_int32),
+                ("tau", ctypes.c_double), ("checkpoint", ctypes.c_int32)]
+
+
+class tdv_batch_pair(ctypes.Structure):
+    _fields_ = [("left", tdv_image), ("right", tdv_image), ("max_disp", ctypes.c_int32),
+                ("out", tdv_disparity)]
+
+
+class tdv_batch_tiles(ctypes.Structure):
+    _fields_ = [("lines_per_cta", ctypes.c_int32), ("rows_per_cta", ctypes.c_int32),
+                ("split_disparity", ctypes.c_int32), ("order", ctypes.c_int32)]
 
 
 ALLOC_FN = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
@@ -107,6 +121,16 @@ def _declare(lib):
         "tdv_soft_sgm_forward": (st, [vp, P(tdv_volume), P(tdv_soft_params), vp, vp, ctypes.c_size_t, vp]),
         "tdv_soft_sgm_backward": (st, [vp, P(tdv_volume), P(tdv_soft_params), vp, ctypes.c_size_t, vp,
                                        P(tdv_volume), vp, vp]),
+        "tdv_batch_create": (st, [vp, P(tdv_batch_pair), ctypes.c_int32, P(tdv_sgm_params), P(vp)]),
+        "tdv_batch_destroy": (None, [vp]),
+        "tdv_batch_set_tiles": (st, [vp, P(tdv_batch_tiles)]),
+        "tdv_batch_get_tiles": (st, [vp, P(tdv_batch_tiles)]),
+        "tdv_batch_autotune": (st, [vp, ctypes.c_int32, vp, P(tdv_batch_tiles), P(ctypes.c_double)]),
+        "tdv_batch_run": (st, [vp, vp]),
+        "tdv_batch_graph_launch": (st, [vp, vp]),
+        "tdv_batch_status": (st, [vp, vp]),
+        "tdv_batch_set_wait_limit": (st, [vp, ctypes.c_double]),
+        "tdv_batch_work_queue": (st, [vp, P(vp), P(ctypes.c_int32), P(ctypes.c_int32)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

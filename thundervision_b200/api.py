@@ -192,6 +192,98 @@ class Context:
         return self._result(disp, dn, dr)
 
 
+class Batch:
+    """Many uint8 pairs of uneven size and disparity range aggregated by one
+    persistent launch (tdv_batch_*): BT + SGM + WTA (+ left-right check) with
+    results bit-identical to per-pair ``Context.stereo_sgm`` calls.
+
+    ``pairs`` is a list of ``(left, right, max_disp)`` or
+    ``(left, right, max_disp, lr)`` with (H, W) uint8 CUDA tensors; the
+    tensors are kept alive and read again by every run, so a video loop
+    copies new frames into them and relaunches.  ``outputs[i]`` holds pair
+    i's result tensors (rewritten by every run).  ``right_disp``: False, True,
+    or "lr" (right-view maps for the pairs that run the left-right check).
+    """
+
+    def __init__(self, ctx, pairs, p1, p2, paths=8, lr=None, norm=False, right_disp=False):
+        self.ctx = ctx
+        self.handle = None
+        n = len(pairs)
+        arr = (L.tdv_batch_pair * n)()
+        self.outputs = []
+        self._inputs = []
+        for i, pr in enumerate(pairs):
+            left, right, D = pr[0], pr[1], int(pr[2])
+            lr_i = pr[3] if len(pr) > 3 else lr
+            H, W = left.shape
+            want_right = (lr_i is not None) if right_disp == "lr" else bool(right_disp)
+            o, disp, dn, dr = ctx._outputs(W, H, left.device, norm, want_right, lr_i)
+            arr[i] = L.tdv_batch_pair(_image(left), _image(right), D, o)
+            self.outputs.append(Context._result(disp, dn, dr))
+            self._inputs.append((left, right))
+        prm = L.tdv_sgm_params(p1, p2, L.P2_CONST, paths, L.TABLE_FULL, L.SEM_STANDARD)
+        h = ctypes.c_void_p()
+        ctx.check(L.lib().tdv_batch_create(ctx.handle, arr, n, ctypes.byref(prm), ctypes.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            L.lib().tdv_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self):
+        """One persistent launch on torch's current stream."""
+        self.ctx.check(L.lib().tdv_batch_run(self.handle, _stream()))
+        return self.outputs
+
+    def graph_launch(self):
+        """The same run replayed from a CUDA graph (captured on first use)."""
+        self.ctx.check(L.lib().tdv_batch_graph_launch(self.handle, _stream()))
+        return self.outputs
+
+    def status(self):
+        """Synchronise; raise TdvError if the last run recorded a device error."""
+        self.ctx.check(L.lib().tdv_batch_status(self.handle, _stream()))
+
+    @property
+    def tiles(self):
+        t = L.tdv_batch_tiles()
+        self.ctx.check(L.lib().tdv_batch_get_tiles(self.handle, ctypes.byref(t)))
+        return {f: getattr(t, f) for f, _ in L.tdv_batch_tiles._fields_}
+
+    def set_tiles(self, **kw):
+        cur = self.tiles
+        cur.update(kw)
+        t = L.tdv_batch_tiles(**cur)
+        self.ctx.check(L.lib().tdv_batch_set_tiles(self.handle, ctypes.byref(t)))
+
+    def autotune(self, reps=3):
+        """Time candidate tile shapes, keep the fastest; returns (tiles, ms)."""
+        t = L.tdv_batch_tiles()
+        ms = ctypes.c_double()
+        self.ctx.check(L.lib().tdv_batch_autotune(self.handle, reps, _stream(), ctypes.byref(t),
+                                                  ctypes.byref(ms)))
+        return {f: getattr(t, f) for f, _ in L.tdv_batch_tiles._fields_}, ms.value
+
+    def set_wait_limit(self, seconds):
+        self.ctx.check(L.lib().tdv_batch_set_wait_limit(self.handle, float(seconds)))
+
+    def work_queue(self):
+        """(device pointer, item count, bytes per item) of the work queue."""
+        p = ctypes.c_void_p()
+        n = ctypes.c_int32()
+        b = ctypes.c_int32()
+        self.ctx.check(L.lib().tdv_batch_work_queue(self.handle, ctypes.byref(p), ctypes.byref(n),
+                                                    ctypes.byref(b)))
+        return p.value, n.value, b.value
+
+
 _default = {}
 
 

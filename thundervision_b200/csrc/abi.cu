@@ -301,7 +301,7 @@ tdv_status check_soft(tdv_ctx* ctx, const tdv_volume* cost, const tdv_soft_param
     if (cost->depth > tdv::kMaxDispSgm) return fail(ctx, TDV_ERR_UNSUPPORTED, "soft SGM supports D <= 256");
     if (!p) return fail(ctx, TDV_ERR_INVALID_ARG, "null soft params");
     if (p->paths != 4 && p->paths != 8) return fail(ctx, TDV_ERR_INVALID_ARG, "paths must be 4 or 8");
-    if (!(p->tau > 0.0f) || !std::isfinite(p->tau)) return fail(ctx, TDV_ERR_INVALID_ARG, "tau must be > 0");
+    if (!(p->tau > 0.0) || !std::isfinite(p->tau)) return fail(ctx, TDV_ERR_INVALID_ARG, "tau must be > 0");
     if (!std::isfinite(p->p1) || !std::isfinite(p->p2))
         return fail(ctx, TDV_ERR_INVALID_ARG, "penalties must be finite");
     if (p->checkpoint < 0 || p->checkpoint > 32)
@@ -541,7 +541,8 @@ tdv_status tdv_soft_sgm_backward(tdv_ctx* ctx, const tdv_volume* cost, const tdv
         return fail(ctx, TDV_ERR_INVALID_ARG, "tape of %zu bytes < %zu needed", tape_bytes, lay.total);
     TDV_DEVICE_SCOPE(ctx);
     ctx->timer.begin(S(stream));
-    TDV_TRY(ensure(ctx, ctx->soft, (size_t)W * H * D * es));
+    const size_t ds_bytes = al256((size_t)W * H * D * es);
+    TDV_TRY(ensure(ctx, ctx->soft, ds_bytes + (size_t)8 * (W + H) * 2 * es));
     unsigned char* base = (unsigned char*)tape;
     tdv::SoftLaunch a{};
     a.f64 = es == 8;
@@ -549,6 +550,7 @@ tdv_status tdv_soft_sgm_backward(tdv_ctx* ctx, const tdv_volume* cost, const tdv
     a.S = base + lay.S;
     a.stats = base + lay.stats;
     a.dS = ctx->soft.ptr;
+    a.dpen_part = (unsigned char*)ctx->soft.ptr + ds_bytes;
     a.dcost = dcost->ptr;
     a.g = g_dhat;
     a.dpen = dpen;
@@ -739,6 +741,315 @@ tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* 
     TDV_CUDA(tdv::launch_cost(tdv::make_img(*left), tdv::make_img(*right), TDV_COST_BT, 0,
                               tdv::make_vol(cv), S(stream), &ctx->timer));
     return run_sgm(ctx, &cv, left, params, nullptr, out, S(stream));
+}
+
+// ------------------------------------------------------------ batched pairs
+}  // extern "C"
+
+struct tdv_batch {
+    tdv_ctx* ctx = nullptr;
+    std::vector<tdv::BatchPairArgs> pairs;
+    int p1h = 0, p2h = 0, paths = 8;
+    tdv_batch_tiles tiles{};
+    tdv::BatchPlan plan;
+    void* scratch = nullptr;
+    void* desc = nullptr;
+    size_t desc_bytes = 0;
+    cudaGraphExec_t gexec = nullptr;
+    unsigned long long wait_ns = 2000000000ull;
+    int grid = 0;
+};
+
+namespace {
+
+void* dev_alloc(tdv_ctx* ctx, size_t bytes) {
+    void* p = nullptr;
+    if (ctx->alloc) return ctx->alloc(bytes, ctx->alloc_user);
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void dev_free(tdv_ctx* ctx, void* p) {
+    if (!p) return;
+    if (ctx->release) ctx->release(p, ctx->alloc_user);
+    else cudaFree(p);
+}
+
+void drop_graph(tdv_batch* b) {
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+}
+
+// Plans with `t` and uploads the queue; the device must be idle for this
+// batch (callers synchronise first).
+tdv_status batch_replan(tdv_batch* b, const tdv_batch_tiles& t) {
+    tdv_ctx* ctx = b->ctx;
+    for (int pass = 0; pass < 2; pass++) {
+        tdv::BatchPlan plan;
+        const char* msg = tdv::batch_plan(b->pairs, b->p1h, b->p2h, b->paths, t, (unsigned char*)b->scratch,
+                                          (unsigned char*)b->desc, plan);
+        if (msg) return fail(ctx, TDV_ERR_UNSUPPORTED, "batch tiles: %s", msg);
+        if (plan.bytes > b->desc_bytes) {
+            // the descriptors hold the queue's own address: grow, then plan again
+            dev_free(ctx, b->desc);
+            b->desc = dev_alloc(ctx, plan.bytes);
+            b->desc_bytes = b->desc ? plan.bytes : 0;
+            if (!b->desc) return fail(ctx, TDV_ERR_OOM, "allocating %zu bytes of work queue failed", plan.bytes);
+            continue;
+        }
+        TDV_CUDA(cudaMemcpy(b->desc, plan.desc.data(), plan.bytes, cudaMemcpyHostToDevice));
+        b->plan = std::move(plan);
+        b->tiles = t;
+        drop_graph(b);
+        return TDV_OK;
+    }
+    return fail(ctx, TDV_ERR_OOM, "work queue did not settle");
+}
+
+tdv_status batch_launch_on(tdv_batch* b, cudaStream_t st) {
+    tdv_ctx* ctx = b->ctx;
+    TDV_CUDA(tdv::batch_configure(b->plan));
+    TDV_CUDA(tdv::batch_launch(b->plan, (unsigned char*)b->desc, b->wait_ns, b->grid, st));
+    return TDV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+tdv_status tdv_batch_create(tdv_ctx* ctx, const tdv_batch_pair* pairs, int32_t n_pairs,
+                            const tdv_sgm_params* params, tdv_batch** out) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    if (!out) return fail(ctx, TDV_ERR_INVALID_ARG, "null output handle");
+    *out = nullptr;
+    if (!pairs || n_pairs < 1 || n_pairs > 65536)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "n_pairs must be in [1, 65536] with a pair array");
+    TDV_TRY(check_params(ctx, params));
+    if (params->semantics != TDV_SEM_STANDARD || params->table != TDV_TABLE_FULL ||
+        params->p2_mode != TDV_P2_CONST || !is_half_multiple(params->p1) || !is_half_multiple(params->p2) ||
+        2.0f * params->p2 > 2560.0f)
+        return fail(ctx, TDV_ERR_UNSUPPORTED,
+                    "batches run the integer-domain fused path: STANDARD, FULL, P2_CONST, "
+                    "P1/P2 multiples of 1/2, P2 <= 1280");
+    std::vector<tdv::BatchPairArgs> args((size_t)n_pairs);
+    for (int i = 0; i < n_pairs; i++) {
+        const tdv_batch_pair& p = pairs[i];
+        char nm[32];
+        snprintf(nm, sizeof(nm), "pair %d left", i);
+        TDV_TRY(check_image(ctx, &p.left, nm));
+        snprintf(nm, sizeof(nm), "pair %d right", i);
+        TDV_TRY(check_image(ctx, &p.right, nm));
+        TDV_TRY(check_out(ctx, &p.out));
+        if (p.left.dtype != TDV_U8 || p.right.dtype != TDV_U8 || p.left.scale != 1.0f || p.right.scale != 1.0f)
+            return fail(ctx, TDV_ERR_UNSUPPORTED, "pair %d: batches take u8 images with scale 1", i);
+        if (p.left.width != p.right.width || p.left.height != p.right.height)
+            return fail(ctx, TDV_ERR_INVALID_ARG, "pair %d: left and right images differ in size", i);
+        if (p.max_disp < 1 || p.max_disp > tdv::kMaxDispSgm)
+            return fail(ctx, TDV_ERR_UNSUPPORTED, "pair %d: max_disp must be in [1, %d]", i, tdv::kMaxDispSgm);
+        tdv::BatchPairArgs& a = args[i];
+        a.L = tdv::make_img(p.left);
+        a.R = tdv::make_img(p.right);
+        a.W = p.left.width;
+        a.H = p.left.height;
+        a.D = p.max_disp;
+        a.disp = p.out.disp;
+        a.disp_norm = p.out.disp_norm;
+        a.disp_right = p.out.disp_right;
+        a.lr_thr = p.out.lr_threshold >= 0 ? p.out.lr_threshold : (p.out.disp_right ? 0x7FFFFFFF : -1);
+    }
+    TDV_DEVICE_SCOPE(ctx);
+    tdv_batch* b = new (std::nothrow) tdv_batch;
+    if (!b) return fail(ctx, TDV_ERR_OOM, "host allocation failed");
+    b->ctx = ctx;
+    b->pairs = std::move(args);
+    b->p1h = (int)(2.0f * params->p1);
+    b->p2h = (int)(2.0f * params->p2);
+    b->paths = params->paths;
+    if (cudaDeviceGetAttribute(&b->grid, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess ||
+        b->grid < 1) {
+        delete b;
+        return fail(ctx, TDV_ERR_CUDA, "querying the SM count failed");
+    }
+    const size_t sb = tdv::batch_scratch_bytes(b->pairs);
+    b->scratch = dev_alloc(ctx, sb);
+    if (!b->scratch) {
+        delete b;
+        return fail(ctx, TDV_ERR_OOM, "allocating %zu bytes of batch scratch failed", sb);
+    }
+    tdv_batch_tiles t;
+    t.lines_per_cta = 24;
+    t.rows_per_cta = 8;
+    t.split_disparity = 0;
+    t.order = TDV_BATCH_ORDER_LONGEST_FIRST;
+    const tdv_status st = batch_replan(b, t);
+    if (st != TDV_OK) {
+        tdv_batch_destroy(b);
+        return st;
+    }
+    *out = b;
+    return TDV_OK;
+}
+
+void tdv_batch_destroy(tdv_batch* b) {
+    if (!b) return;
+    DeviceScope ds(b->ctx->device);
+    cudaDeviceSynchronize();
+    drop_graph(b);
+    dev_free(b->ctx, b->scratch);
+    dev_free(b->ctx, b->desc);
+    delete b;
+}
+
+tdv_status tdv_batch_set_tiles(tdv_batch* b, const tdv_batch_tiles* tiles) {
+    if (!b) return TDV_ERR_INVALID_ARG;
+    tdv_ctx* ctx = b->ctx;
+    if (!tiles) return fail(ctx, TDV_ERR_INVALID_ARG, "null tiles");
+    if (tiles->order != TDV_BATCH_ORDER_LONGEST_FIRST && tiles->order != TDV_BATCH_ORDER_INPUT)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "bad queue order %d", tiles->order);
+    if (tiles->split_disparity != 0 && tiles->split_disparity != 1)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "split_disparity must be 0 or 1");
+    TDV_DEVICE_SCOPE(ctx);
+    TDV_CUDA(cudaDeviceSynchronize());
+    return batch_replan(b, *tiles);
+}
+
+tdv_status tdv_batch_get_tiles(const tdv_batch* b, tdv_batch_tiles* tiles) {
+    if (!b || !tiles) return TDV_ERR_INVALID_ARG;
+    *tiles = b->tiles;
+    return TDV_OK;
+}
+
+tdv_status tdv_batch_run(tdv_batch* b, tdv_stream stream) {
+    if (!b) return TDV_ERR_INVALID_ARG;
+    tdv_ctx* ctx = b->ctx;
+    TDV_DEVICE_SCOPE(ctx);
+    return batch_launch_on(b, S(stream));
+}
+
+tdv_status tdv_batch_graph_launch(tdv_batch* b, tdv_stream stream) {
+    if (!b) return TDV_ERR_INVALID_ARG;
+    tdv_ctx* ctx = b->ctx;
+    TDV_DEVICE_SCOPE(ctx);
+    if (!b->gexec) {
+        // the shared-memory opt-in is not a stream operation: set it outside the capture
+        TDV_CUDA(tdv::batch_configure(b->plan));
+        cudaStream_t cs;
+        TDV_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            const cudaError_t el = tdv::batch_launch(b->plan, (unsigned char*)b->desc, b->wait_ns, b->grid, cs);
+            e = cudaStreamEndCapture(cs, &g);
+            if (el != cudaSuccess) e = el;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->gexec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        cudaStreamDestroy(cs);
+        if (e != cudaSuccess) {
+            b->gexec = nullptr;
+            return fail(ctx, TDV_ERR_CUDA, "capturing the batch graph failed: %s", cudaGetErrorString(e));
+        }
+    }
+    TDV_CUDA(cudaGraphLaunch(b->gexec, S(stream)));
+    return TDV_OK;
+}
+
+tdv_status tdv_batch_status(tdv_batch* b, tdv_stream stream) {
+    if (!b) return TDV_ERR_INVALID_ARG;
+    tdv_ctx* ctx = b->ctx;
+    TDV_DEVICE_SCOPE(ctx);
+    TDV_CUDA(cudaStreamSynchronize(S(stream)));
+    int w[2] = {0, 0};
+    TDV_CUDA(cudaMemcpy(w, (unsigned char*)b->desc + b->plan.ctl_off, sizeof(w), cudaMemcpyDeviceToHost));
+    if (w[1] == TDV_ERR_TIMEOUT)
+        return fail(ctx, TDV_ERR_TIMEOUT, "a bounded wait in the batch kernel ran out");
+    if (w[1] == TDV_ERR_BAD_WORK)
+        return fail(ctx, TDV_ERR_BAD_WORK, "the batch work queue held an item out of range");
+    if (w[1] != 0) return fail(ctx, TDV_ERR_CUDA, "batch kernel recorded status %d", w[1]);
+    return TDV_OK;
+}
+
+tdv_status tdv_batch_set_wait_limit(tdv_batch* b, double seconds) {
+    if (!b) return TDV_ERR_INVALID_ARG;
+    if (!(seconds >= 1e-3 && seconds <= 60.0))
+        return fail(b->ctx, TDV_ERR_INVALID_ARG, "wait limit must be in [0.001, 60] s");
+    b->wait_ns = (unsigned long long)(seconds * 1e9);
+    drop_graph(b);
+    return TDV_OK;
+}
+
+tdv_status tdv_batch_work_queue(tdv_batch* b, void** items, int32_t* n_items, int32_t* item_bytes) {
+    if (!b) return TDV_ERR_INVALID_ARG;
+    if (!items || !n_items || !item_bytes) return fail(b->ctx, TDV_ERR_INVALID_ARG, "null output");
+    *items = (unsigned char*)b->desc + b->plan.items_off;
+    *n_items = b->plan.n_items;
+    *item_bytes = b->plan.item_bytes;
+    return TDV_OK;
+}
+
+tdv_status tdv_batch_autotune(tdv_batch* b, int32_t reps, tdv_stream stream, tdv_batch_tiles* chosen,
+                              double* best_ms) {
+    if (!b) return TDV_ERR_INVALID_ARG;
+    tdv_ctx* ctx = b->ctx;
+    if (reps < 1 || reps > 100) return fail(ctx, TDV_ERR_INVALID_ARG, "reps must be in [1, 100]");
+    TDV_DEVICE_SCOPE(ctx);
+    cudaStream_t st = S(stream);
+    cudaEvent_t e0, e1;
+    TDV_CUDA(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(ctx, TDV_ERR_CUDA, "cudaEventCreate failed");
+    }
+    // times one candidate; +inf if it does not fit
+    auto time_tiles = [&](const tdv_batch_tiles& t, double& ms) -> tdv_status {
+        ms = HUGE_VAL;
+        TDV_CUDA(cudaStreamSynchronize(st));
+        if (batch_replan(b, t) != TDV_OK) return TDV_OK;
+        TDV_TRY(batch_launch_on(b, st));  // warm-up
+        TDV_TRY(tdv_batch_status(b, stream));
+        TDV_CUDA(cudaEventRecord(e0, st));
+        for (int r = 0; r < reps; r++) TDV_TRY(batch_launch_on(b, st));
+        TDV_CUDA(cudaEventRecord(e1, st));
+        TDV_TRY(tdv_batch_status(b, stream));
+        float f = 0.0f;
+        TDV_CUDA(cudaEventElapsedTime(&f, e0, e1));
+        ms = (double)f / reps;
+        return TDV_OK;
+    };
+    tdv_batch_tiles best = b->tiles;
+    double best_t = HUGE_VAL;
+    tdv_status st_all = time_tiles(best, best_t);
+    // coordinate descent over the tile shapes, one axis at a time
+    const int Gs[] = {8, 12, 16, 20, 24};
+    const int Rs[] = {4, 6, 8, 12, 16, 24};
+    for (int axis = 0; axis < 4 && st_all == TDV_OK; axis++) {
+        const int n = axis == 0 ? 5 : (axis == 1 ? 6 : 2);
+        for (int j = 0; j < n && st_all == TDV_OK; j++) {
+            tdv_batch_tiles t = best;
+            if (axis == 0) t.lines_per_cta = Gs[j];
+            else if (axis == 1) t.rows_per_cta = Rs[j];
+            else if (axis == 2) t.split_disparity = j;
+            else t.order = j;
+            if (memcmp(&t, &best, sizeof(t)) == 0) continue;
+            double ms;
+            st_all = time_tiles(t, ms);
+            if (st_all == TDV_OK && ms < best_t) {
+                best_t = ms;
+                best = t;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st_all != TDV_OK) return st_all;
+    TDV_CUDA(cudaStreamSynchronize(st));
+    TDV_TRY(batch_replan(b, best));
+    if (chosen) *chosen = best;
+    if (best_ms) *best_ms = best_t;
+    return TDV_OK;
 }
 
 }  // extern "C"

@@ -1,0 +1,928 @@
+// Fused Birchfield-Tomasi + SGM + WTA (+ left-right check) for integer-domain
+// inputs: u8 intensities used unscaled, P1/P2 multiples of 1/2, constant P2,
+// STANDARD recurrence over the FULL path table, D <= 256.
+//
+// Exactness.  In this domain every BT cost is a multiple of 1/2 in [0, 255]
+// and every path cost L = C + min(...) - m' lies in [0, 255 + P2], so all
+// quantities are small multiples of 1/2.  The kernels carry them as unsigned
+// 16-bit "half-units" (2x the value), two disparities per 32-bit register.
+// Integer arithmetic on these is exact, so the result is bit-identical to the
+// float32 recurrence of the reference (tdvision/semiglobalcpu.cpp:104-122)
+// evaluated on the same values, in any summation order.  Cells with x-d < 0
+// (+INF in the reference) carry a sentinel BIG = 511 + 2*P2h that can never
+// win a minimum and stays bounded: every invalid L is in [BIG, BIG + P2h] and
+// every invalid S in [8*BIG, 8*(BIG + P2h)] <= 65535, above any valid S.
+//
+// Data flow per frame (8 paths):
+//   prep : BT planes of both images (I, half-sample min, half-sample max in
+//          half-units).  The right plane stores, at pixel x, the values of x
+//          and x-1 so the disparity pair (d, d+1) of left column x reads one
+//          16-byte entry; rows are padded with one 16-byte slot after every 8
+//          entries so that lanes reading entries 8 apart hit distinct banks.
+//   pass : V+ V- D1+ D1- D2+ D2- H+ H-.  Lanes own consecutive disparity
+//          pairs; d-1/d+1 neighbours by byte permutes plus one shuffle each
+//          way; u16x2 min/max; min over d by redux.sync.  The aggregation
+//          volume S ([y][x][64*PPL] u16 in HBM) is stored by the first pass,
+//          read-modify-written by the middle ones and read by the last (H-),
+//          which finishes S in registers and reduces it to disparities (WTA,
+//          right-view disparity, left-right check) without storing it.
+//   Vertical and diagonal passes run row-synchronous blocks: G warps own G
+//   adjacent path lines and advance one image row per step; per row one
+//   thread issues TMA bulk copies (cp.async.bulk) of the S chunk, the left
+//   plane entries and the shared right-plane segment into a ring of shared
+//   memory slots completed by mbarriers.  Horizontal passes give each warp a
+//   row, an S ring and a sliding window of right-plane chunks, also filled by
+//   TMA bulk copies.  Every mbarrier wait is bounded; a wait that runs out
+//   records TDV_ERR_TIMEOUT, waits (bounded) for its copies in flight and
+//   returns.
+//
+// This header holds the device code of those passes as __device__ bodies that
+// take their block index and shared-memory base explicitly, so that the
+// per-frame kernels (kernels_fused.cu, one launch per pass) and the
+// persistent batch kernel (kernels_batch.cu, one launch per batch of pairs)
+// run the same code.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "tdv_internal.hpp"
+
+namespace tdv {
+
+namespace {
+
+constexpr int kMaxG = 24;       // consumer warps per block, vertical/diagonal passes
+constexpr int kRowSlots = 8;    // ring depth (rows), vertical/diagonal passes (power of 2)
+constexpr int kMaxGH = 8;       // warps per block, horizontal passes
+constexpr int kHSlots = 8;      // S ring depth (steps), horizontal passes
+constexpr int kChunk = 64;      // right-plane entries per horizontal refill
+constexpr int kChunkSlots = 8;  // resident chunks per horizontal warp
+constexpr int kChunk2 = 32;     // right-plane entries per refill, split-D horizontal passes
+constexpr int kMaxRowsH2 = 8;   // rows (2 warps each) per block, split-D horizontal passes
+constexpr int kLookC = 2;       // chunks fetched ahead of need
+constexpr uint64_t kWaitNs = 1000000000ull;   // 1 s: a wait this long means a lost copy
+constexpr uint64_t kDrainNs = 10000000ull;    // 10 ms per wait while retiring after an error
+constexpr int kGroupBytes = 9 * 16;
+constexpr int kChunkBytes = (kChunk / 8) * kGroupBytes;
+constexpr uint32_t FULL = 0xFFFFFFFFu;
+
+struct __align__(16) Plane {
+    uint32_t i, mn, mx, pad;
+};
+
+__host__ __device__ inline int padded_len(int W) { return 9 * ((W + 7) / 8); }
+__host__ __device__ inline int align128(int v) { return (v + 127) & ~127; }
+__device__ __forceinline__ int ppos(int e) { return e + (e >> 3); }
+// Left-plane entry load: through the read-only path when the planes were
+// written by an earlier launch, through L2 when a producer in the same
+// (persistent) launch may have written them.
+__device__ __forceinline__ uint4 ld_plane(const void* p, bool nc) {
+    return nc ? __ldg((const uint4*)p) : __ldcg((const uint4*)p);
+}
+
+// ------------------------------------------------- tile sizes (host + device)
+// Disparity pairs per lane: 64 disparities per warp-row of 32 lanes per pair.
+__host__ __device__ inline int ppl_for(int D) { return D <= 64 ? 1 : (D <= 128 ? 2 : 4); }
+constexpr int kSmemBudget = 220 * 1024;  // dynamic shared memory per block
+
+// vertical/diagonal pass, G lines: barriers + kRowSlots ring slots of
+// (S chunk, left entries, shared right segment)
+__host__ __device__ inline int vd_smem_bytes(int G, int ppl) {
+    const int NRG = (G + 64 * ppl) / 8 + 2;
+    return 2 * kRowSlots * 8 + kRowSlots * align128(G * 128 * ppl + G * 16 + NRG * kGroupBytes);
+}
+// horizontal pass, one warp per row: barriers, S ring, chunk ring, L-R rows
+__host__ __device__ inline int h_warp_bytes(int ppl, bool lr, int W) {
+    return align128(128 + kHSlots * 128 * ppl + kChunkSlots * kChunkBytes + (lr ? 2 * W * 2 : 0));
+}
+// horizontal pass, two warps per row: per warp, then per row (exchange + L-R rows)
+__host__ __device__ inline int h2_warp_bytes(int ph) {
+    return align128(128 + kHSlots * 128 * ph + kChunkSlots * (kChunk2 / 8) * kGroupBytes);
+}
+__host__ __device__ inline int h2_row_bytes(bool lr, int W) { return align128(128 + (lr ? 2 * W * 2 : 0)); }
+
+// ---------------------------------------------------------------- PTX
+__device__ __forceinline__ uint32_t vmin2(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("min.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+__device__ __forceinline__ uint32_t vmax2(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("max.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+// (hi16(a), lo16(b)) as (lo, hi) of the result
+__device__ __forceinline__ uint32_t hi_lo(uint32_t a, uint32_t b) { return __byte_perm(a, b, 0x5432); }
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_inval(uint32_t bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+// Slot reuse needs no proxy fence: every generic read of a ring slot feeds
+// arithmetic that precedes the release of the slot (mbarrier arrive or warp
+// sync), so those reads have completed before the refill is issued.
+// 1-D TMA bulk copy global -> shared, completion counted on `bar`.
+__device__ __forceinline__ void tma_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait for phase `parity` of `bar`: false once `limit_ns` of wall
+// time have passed without the phase completing.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_t limit_ns = kWaitNs) {
+    if (mbar_try(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_try(bar, parity))
+        if (global_ns() - t0 > limit_ns) return false;
+    return true;
+}
+
+// ---------------------------------------------------------------- planes
+__device__ __forceinline__ int u8_at(const ImgArg& im, int x, int y) {
+    x = min(max(x, 0), im.W - 1);
+    y = min(max(y, 0), im.H - 1);
+    return ((const uint8_t*)im.ptr)[(size_t)y * im.pitch + x];
+}
+
+// Per pixel, in half-units: 2I, min(2I, I+I(x-1), I+I(x+1)), max(...) with
+// clamp-to-edge taps (tdvision/birchfieldcost.cu:22-32).
+__device__ __forceinline__ void bt_triple(const ImgArg& im, int x, int y, uint32_t& i2,
+                                          uint32_t& mn, uint32_t& mx) {
+    const int v = u8_at(im, x, y);
+    const int a = v + u8_at(im, x - 1, y);
+    const int b = v + u8_at(im, x + 1, y);
+    i2 = 2 * v;
+    mn = min(2 * v, min(a, b));
+    mx = max(2 * v, max(a, b));
+}
+
+__device__ __forceinline__ void prep_pixel(const ImgArg& L, const ImgArg& R, Plane* LP, Plane* RPp, int W,
+                                           int Wp, int x, int y) {
+    uint32_t i2, mn, mx;
+    bt_triple(L, x, y, i2, mn, mx);
+    Plane lp;
+    lp.i = i2 * 0x10001u;
+    lp.mn = mn * 0x10001u;
+    lp.mx = mx * 0x10001u;
+    lp.pad = 0;
+    LP[(size_t)y * W + x] = lp;
+    uint32_t j2, jn, jx, k2, kn, kx;
+    bt_triple(R, x, y, j2, jn, jx);
+    bt_triple(R, max(x - 1, 0), y, k2, kn, kx);
+    Plane rp;
+    rp.i = j2 | (k2 << 16);
+    rp.mn = jn | (kn << 16);
+    rp.mx = jx | (kx << 16);
+    rp.pad = 0;
+    RPp[(size_t)y * Wp + x + (x >> 3)] = rp;
+}
+
+struct FK {
+    const Plane* LP;
+    const Plane* RPp;  // padded rows of Wp entries
+    uint32_t* S;       // aggregation volume, u16 pairs
+    int W, H, D, Dp2, Wp;
+    uint32_t P1P1, P2P2, BIGBIG;
+    uint16_t* disp;
+    float* disp_norm;
+    uint16_t* disp_right;
+    int lr_thr;
+    int* err;
+};
+
+// ---------------------------------------------------------------- compute
+template <int PPL>
+struct Vec;
+template <>
+struct Vec<1> {
+    static __device__ __forceinline__ void st(uint32_t* p, const uint32_t* v) { __stcs(p, v[0]); }
+    static __device__ __forceinline__ void lds(const uint32_t* p, uint32_t* v) { v[0] = p[0]; }
+};
+template <>
+struct Vec<2> {
+    static __device__ __forceinline__ void st(uint32_t* p, const uint32_t* v) {
+        __stcs((uint2*)p, make_uint2(v[0], v[1]));
+    }
+    static __device__ __forceinline__ void lds(const uint32_t* p, uint32_t* v) {
+        const uint2 t = *(const uint2*)p;
+        v[0] = t.x;
+        v[1] = t.y;
+    }
+};
+template <>
+struct Vec<4> {
+    static __device__ __forceinline__ void st(uint32_t* p, const uint32_t* v) {
+        __stcs((uint4*)p, make_uint4(v[0], v[1], v[2], v[3]));
+    }
+    static __device__ __forceinline__ void lds(const uint32_t* p, uint32_t* v) {
+        const uint4 t = *(const uint4*)p;
+        v[0] = t.x;
+        v[1] = t.y;
+        v[2] = t.z;
+        v[3] = t.w;
+    }
+};
+
+// BT of one disparity pair from a left entry and a right entry.
+__device__ __forceinline__ uint32_t bt_pair(const uint4& lp, const uint4& rp) {
+    // .x = I, .y = half-sample min, .z = half-sample max
+    const uint32_t A = vmax2(lp.x, rp.y) - vmin2(lp.x, rp.z);
+    const uint32_t B = vmax2(rp.x, lp.y) - vmin2(rp.x, lp.z);
+    return vmin2(A, B);
+}
+
+// Invalid halves (d > x or d >= D) carry BIG.
+__device__ __forceinline__ uint32_t mask_pair(uint32_t v, int d, int lim, uint32_t BIGBIG) {
+    if (d + 1 >= lim) v = (d < lim) ? ((v & 0xFFFFu) | (BIGBIG & 0xFFFF0000u)) : BIGBIG;
+    return v;
+}
+
+template <int PPL>
+__device__ __forceinline__ uint32_t warp_min_pairs(const uint32_t* L) {
+    uint32_t t = L[0];
+    #pragma unroll
+    for (int q = 1; q < PPL; q++) t = vmin2(t, L[q]);
+    t = min(t & 0xFFFFu, t >> 16);
+    return __reduce_min_sync(FULL, t);
+}
+
+// One step of the min-plus recurrence for this lane's pairs.
+template <int PPL>
+__device__ __forceinline__ void recur(const uint32_t* L, uint32_t m, const uint32_t* c, uint32_t* Ln,
+                                      int lane, const FK& k) {
+    const uint32_t MM = m * 0x10001u;
+    const uint32_t MP2 = MM + k.P2P2;
+    uint32_t up = __shfl_up_sync(FULL, L[PPL - 1], 1);
+    uint32_t dn = __shfl_down_sync(FULL, L[0], 1);
+    if (lane == 0) up = k.BIGBIG;
+    if (lane == 31) dn = k.BIGBIG;
+    #pragma unroll
+    for (int q = 0; q < PPL; q++) {
+        const uint32_t lm = hi_lo(q > 0 ? L[q - 1] : up, L[q]);
+        const uint32_t lp = hi_lo(L[q], q < PPL - 1 ? L[q + 1] : dn);
+        uint32_t tv = vmin2(lm, lp) + k.P1P1;
+        tv = vmin2(vmin2(tv, L[q]), MP2);
+        Ln[q] = tv + c[q] - MM;
+    }
+}
+
+// ---------------------------------------------- vertical / diagonal passes
+// A path line is x = kp + s*y (s = dx*dy); the block owns lines
+// j0 .. j0+G-1 (kp = kmin + j) and walks rows in the pass direction dy.
+// Warps 0..G-1 consume one row per step; warp G is the producer: its lane 0
+// issues the TMA copies of row i into ring slot i % kRowSlots once every
+// consumer warp has released the slot's previous row (full/empty mbarrier
+// pairs), so no block-wide barrier is taken per row.
+template <int PPL, int MODE>
+__device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, int nlines, int G, int blk,
+                                        unsigned char* smem) {
+    constexpr int SB = 128 * PPL;
+    constexpr int DSPAN = 64 * PPL;
+    const int NRG = (G + DSPAN) / 8 + 2;
+    const int offL = G * SB, offR = offL + G * 16;
+    const int slotBytes = align128(offR + NRG * kGroupBytes);
+    uint64_t* full = (uint64_t*)smem;
+    uint64_t* empty = full + kRowSlots;
+    unsigned char* slots = smem + 2 * kRowSlots * 8;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int j0 = blk * G;
+    const int Gb = min(G, nlines - j0);
+    const int kf = kmin + j0;
+    int ylo, yhi;
+    if (s == 0) {
+        ylo = 0;
+        yhi = k.H - 1;
+    } else if (s > 0) {
+        ylo = max(0, -(kf + Gb - 1));
+        yhi = min(k.H - 1, k.W - 1 - kf);
+    } else {
+        ylo = max(0, kf - k.W + 1);
+        yhi = min(k.H - 1, kf + Gb - 1);
+    }
+    const int nrows = yhi - ylo + 1;
+    if (nrows <= 0) return;  // uniform for the block
+    const int y0 = dy > 0 ? ylo : yhi;
+
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < kRowSlots; b++) {
+            mbar_init(smem_u32(&full[b]), 1);
+            mbar_init(smem_u32(&empty[b]), G);
+        }
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    if (warp == G) {
+        // ---- producer ----
+        if (lane == 0) {
+            int i = 0;
+            bool ok = true;
+            for (; i < nrows; i++) {
+                const int b = i & (kRowSlots - 1);
+                if (i >= kRowSlots && !mbar_wait(smem_u32(&empty[b]), (uint32_t)((i / kRowSlots) - 1) & 1u)) {
+                    ok = false;
+                    break;
+                }
+                const int y = y0 + dy * i;
+                const int xf = kf + s * y;
+                const int xlo = max(xf, 0), xhi = min(xf + Gb, k.W);
+                const int npx = xhi - xlo;
+                const int g0 = max(0, xlo - DSPAN + 2) >> 3, g1 = (xhi - 1) >> 3;
+                unsigned char* base = slots + b * slotBytes;
+                const uint32_t bar = smem_u32(&full[b]);
+                const uint32_t sb = MODE != 0 ? (uint32_t)npx * SB : 0u;
+                const uint32_t lb = (uint32_t)npx * 16;
+                const uint32_t rb = (uint32_t)(g1 - g0 + 1) * kGroupBytes;
+                mbar_expect_tx(bar, sb + lb + rb);
+                if (MODE != 0)
+                    tma_load(smem_u32(base + (xlo - xf) * SB), k.S + ((size_t)y * k.W + xlo) * k.Dp2, sb, bar);
+                tma_load(smem_u32(base + offL + (xlo - xf) * 16), k.LP + (size_t)y * k.W + xlo, lb, bar);
+                tma_load(smem_u32(base + offR), k.RPp + (size_t)y * k.Wp + 9 * g0, rb, bar);
+            }
+            if (!ok) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
+            // the block must not retire with copies in flight
+            for (int r = max(0, i - kRowSlots); r < i; r++)
+                mbar_wait(smem_u32(&full[r & (kRowSlots - 1)]), (uint32_t)(r / kRowSlots) & 1u,
+                          ok ? kWaitNs : kDrainNs);
+        }
+    } else if (warp < G) {
+        // ---- consumers ----
+        const int kp = kf + warp;
+        const bool has_line = warp < Gb;
+        const int base_d = lane * 2 * PPL;
+        const bool edge_lane = base_d + 2 * PPL > k.D;  // holds disparities >= D
+        const uint32_t* lp_slot = (const uint32_t*)(slots + offL + warp * 16);
+        const uint32_t* sv_slot = (const uint32_t*)(slots + warp * SB) + lane * PPL;
+        const long long step_px = (long long)dy * (k.W + s);  // pixel-index step per row
+        bool started = false;
+        uint32_t L[PPL], m = 0;
+        uint32_t* sg = nullptr;
+
+        for (int i = 0; i < nrows; i++) {
+            const int b = i & (kRowSlots - 1);
+            if (!__all_sync(FULL, mbar_wait(smem_u32(&full[b]), (uint32_t)(i / kRowSlots) & 1u))) {
+                if (lane == 0) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
+                break;
+            }
+            const int y = y0 + dy * i;
+            const int x = kp + s * y;
+            if (has_line && x >= 0 && x < k.W) {
+                const int boff = b * slotBytes;
+                const uint4 lp = *(const uint4*)((const unsigned char*)lp_slot + boff);
+                const int xlo = max(kf + s * y, 0);
+                const int roff = -9 * (max(0, xlo - DSPAN + 2) >> 3);
+                const Plane* rseg = (const Plane*)(slots + boff + offR);
+                uint32_t c[PPL], Ln[PPL];
+                const int eb = x - base_d;
+                #pragma unroll
+                for (int q = 0; q < PPL; q++) {
+                    const int e = max(eb - 2 * q, 0);
+                    c[q] = bt_pair(lp, *(const uint4*)&rseg[ppos(e) + roff]);
+                }
+                const int lim = min(x + 1, k.D);
+                if (edge_lane || eb < 2 * PPL) {
+                    #pragma unroll
+                    for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
+                }
+                if (!started) {
+                    #pragma unroll
+                    for (int q = 0; q < PPL; q++) Ln[q] = c[q];
+                    started = true;
+                    sg = k.S + ((size_t)y * k.W + x) * k.Dp2 + lane * PPL;
+                } else {
+                    recur<PPL>(L, m, c, Ln, lane, k);
+                    sg += step_px * k.Dp2;
+                }
+                if (MODE == 0) {
+                    Vec<PPL>::st(sg, Ln);
+                } else {
+                    uint32_t sv[PPL];
+                    Vec<PPL>::lds((const uint32_t*)((const unsigned char*)sv_slot + boff), sv);
+                    #pragma unroll
+                    for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
+                    Vec<PPL>::st(sg, sv);
+                }
+                #pragma unroll
+                for (int q = 0; q < PPL; q++) L[q] = Ln[q];
+                m = warp_min_pairs<PPL>(L);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&empty[b]));
+        }
+    }
+    // every role is done with the ring: retire its barriers so that the
+    // shared memory can be reused by the next work item
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int b = 0; b < 2 * kRowSlots; b++) mbar_inval(smem_u32(&full[b]));
+}
+
+// ------------------------------------------------------ horizontal passes
+// One warp per image row, walking x in direction dx.  MODE 1: S += L;
+// MODE 2: final S -> WTA (+ right-view disparity and left-right check).
+// The right-view disparity dR(xr) = argmin_d S(xr+d, d) is carried in
+// registers: lane l keeps the running minimum for the 2*PPL right pixels
+// xr = x - base_d - j its disparities reach at column x; stepping to x-1
+// shifts them by one and takes the lane-above's finished entry by shuffle, and
+// lane 0's entry for xr = x is complete.  (Only launched with dx = -1.)
+template <int PPL, int MODE>
+__device__ __forceinline__ void h_body(const FK& k, int dx, int GH, int warp_bytes, int blk,
+                                       unsigned char* smem, bool nc) {
+    constexpr int SB = 128 * PPL;
+    constexpr int DSPAN = 64 * PPL;
+    constexpr int NJ = 2 * PPL;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y = blk * GH + warp;
+    if (warp >= GH || y >= k.H) return;  // warps are independent: no block-wide barrier below
+    unsigned char* wbase = smem + (size_t)warp * warp_bytes;
+    uint64_t* sbar = (uint64_t*)wbase;  // kHSlots barriers
+    uint64_t* cbar = sbar + kHSlots;    // kChunkSlots barriers
+    unsigned char* sring = wbase + 128;
+    unsigned char* cring = sring + kHSlots * SB;
+    uint16_t* rowL = (uint16_t*)(cring + kChunkSlots * kChunkBytes);
+    uint16_t* rowR = rowL + k.W;
+    const bool lr = MODE == 2 && k.lr_thr >= 0;
+
+    const int W = k.W;
+    const int x0 = dx > 0 ? 0 : W - 1;
+    const int nch = (W + kChunk - 1) / kChunk;
+    const int groups_row = (W + 7) / 8;
+    const Plane* rrow = k.RPp + (size_t)y * k.Wp;
+    const uint32_t* srow = k.S + (size_t)y * W * k.Dp2;
+
+    if (lane == 0) {
+        for (int b = 0; b < kHSlots + kChunkSlots; b++) mbar_init(smem_u32(&sbar[b]), 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+
+    auto cl_of = [&](int x) { return max(0, x - DSPAN + 2) >> 6; };
+    auto chunk_use = [&](int c) { return dx > 0 ? c / kChunkSlots : (nch - 1 - c) / kChunkSlots; };
+    auto chunk_bar = [&](int c) { return smem_u32(&cbar[c & (kChunkSlots - 1)]); };
+    auto issue_chunk = [&](int c) {
+        const int ng = min(kChunk / 8, groups_row - c * (kChunk / 8));
+        const uint32_t bar = chunk_bar(c);
+        mbar_expect_tx(bar, (uint32_t)ng * kGroupBytes);
+        tma_load(smem_u32(cring + (c & (kChunkSlots - 1)) * kChunkBytes), rrow + 9 * (c * (kChunk / 8)),
+                 (uint32_t)ng * kGroupBytes, bar);
+    };
+    auto issue_s = [&](int t) {
+        const int x = x0 + dx * t;
+        const uint32_t bar = smem_u32(&sbar[t & (kHSlots - 1)]);
+        mbar_expect_tx(bar, SB);
+        tma_load(smem_u32(sring + (t & (kHSlots - 1)) * SB), srow + (size_t)x * k.Dp2, SB, bar);
+    };
+
+    // Right-plane chunks: the window [x-DSPAN+2, x] is resident and kLookC
+    // chunks beyond it are in flight.  `need` is the next chunk to wait for,
+    // `next` the next to issue, both moving in the walk direction.
+    int need, next;
+    if (dx > 0) {
+        need = 0;
+        next = 0;
+        if (lane == 0)
+            for (; next < nch && next <= kLookC; next++) issue_chunk(next);
+    } else {
+        need = nch - 1;
+        next = nch - 1;
+        if (lane == 0)
+            for (; next >= 0 && next >= cl_of(W - 1) - kLookC; next--) issue_chunk(next);
+    }
+    int s_issued = 0;
+    if (lane == 0)
+        for (; s_issued < kHSlots && s_issued < W; s_issued++) issue_s(s_issued);
+    next = __shfl_sync(FULL, next, 0);
+    s_issued = __shfl_sync(FULL, s_issued, 0);
+
+    bool ok = true;
+    const int base_d = lane * 2 * PPL;
+    const bool edge_lane = base_d + 2 * PPL > k.D;
+    uint32_t L[PPL], m = 0, sv[PPL];
+    uint32_t P[NJ];  // right-view running minima (MODE 2, dx = -1)
+    #pragma unroll
+    for (int j = 0; j < NJ; j++) P[j] = FULL;
+    uint4 lp_next = ld_plane(&k.LP[(size_t)y * W + x0], nc);
+    uint32_t* sg = k.S + ((size_t)y * W + x0) * k.Dp2 + lane * PPL;
+    const long long sstep = (long long)dx * k.Dp2;
+
+    int t = 0;
+    for (; t < W; t++) {
+        const int x = x0 + dx * t;
+        bool good = true;
+        if (dx > 0) {
+            if ((x & (kChunk - 1)) == 0) {
+                const int c = x >> 6;
+                if (lane == 0 && next < nch) issue_chunk(next);
+                if (next < nch) next++;
+                good = mbar_wait(chunk_bar(c), (uint32_t)chunk_use(c) & 1u);
+                need = c + 1;
+            }
+        } else {
+            const int cl = cl_of(x);
+            while (good && need >= cl) {
+                good = mbar_wait(chunk_bar(need), (uint32_t)chunk_use(need) & 1u);
+                need--;
+            }
+            if (next >= 0 && next >= cl - kLookC) {
+                if (lane == 0) issue_chunk(next);
+                next--;
+            }
+        }
+        good = good && mbar_wait(smem_u32(&sbar[t & (kHSlots - 1)]), (uint32_t)(t / kHSlots) & 1u);
+        ok = __all_sync(FULL, good);
+        if (!ok) break;
+
+        const uint4 lp = lp_next;
+        if (t + 1 < W) lp_next = ld_plane(&k.LP[(size_t)y * W + x + dx], nc);
+        uint32_t c[PPL], Ln[PPL];
+        const int eb = x - base_d;
+        #pragma unroll
+        for (int q = 0; q < PPL; q++) {
+            const int e = max(eb - 2 * q, 0);
+            c[q] = bt_pair(lp, *(const uint4*)(cring + ppos(e & (kChunkSlots * kChunk - 1)) * 16));
+        }
+        if (edge_lane || eb < 2 * PPL) {
+            const int lim = min(x + 1, k.D);
+            #pragma unroll
+            for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
+        }
+        if (t == 0) {
+            #pragma unroll
+            for (int q = 0; q < PPL; q++) Ln[q] = c[q];
+        } else {
+            recur<PPL>(L, m, c, Ln, lane, k);
+        }
+        Vec<PPL>::lds((const uint32_t*)(sring + (t & (kHSlots - 1)) * SB) + lane * PPL, sv);
+        #pragma unroll
+        for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
+        if (MODE == 1) {
+            Vec<PPL>::st(sg, sv);
+        } else {
+            // WTA key (S << 8 | d): lowest S, then lowest d (tdvision/wtacpu.cpp:26-30)
+            uint32_t key[NJ];
+            #pragma unroll
+            for (int q = 0; q < PPL; q++) {
+                key[2 * q] = ((sv[q] & 0xFFFFu) << 8) | (uint32_t)(base_d + 2 * q);
+                key[2 * q + 1] = ((sv[q] >> 16) << 8) | (uint32_t)(base_d + 2 * q + 1);
+            }
+            uint32_t kmin = key[0];
+            #pragma unroll
+            for (int j = 1; j < NJ; j++) kmin = min(kmin, key[j]);
+            kmin = __reduce_min_sync(FULL, kmin);
+            if (lr) {
+                #pragma unroll
+                for (int j = 0; j < NJ; j++) P[j] = min(P[j], key[j]);
+                uint32_t in = __shfl_down_sync(FULL, P[0], 1);
+                if (lane == 31) in = FULL;
+                if (lane == 0) {
+                    rowR[x] = (uint16_t)(P[0] & 0xFFu);
+                    rowL[x] = (uint16_t)(kmin & 0xFFu);
+                }
+                #pragma unroll
+                for (int j = 0; j < NJ - 1; j++) P[j] = P[j + 1];
+                P[NJ - 1] = in;
+            } else if (lane == 0) {
+                const size_t o = (size_t)y * W + x;
+                const uint16_t dl = (uint16_t)(kmin & 0xFFu);
+                if (k.disp) k.disp[o] = dl;
+                if (k.disp_norm) k.disp_norm[o] = __fdiv_rn((float)dl, (float)k.D);
+            }
+        }
+        sg += sstep;
+        #pragma unroll
+        for (int q = 0; q < PPL; q++) L[q] = Ln[q];
+        m = warp_min_pairs<PPL>(L);
+        __syncwarp();
+        if (s_issued < W) {
+            if (lane == 0) issue_s(s_issued);
+            s_issued++;
+        }
+    }
+
+    // copies still in flight (chunks fetched ahead, or the tail after a
+    // failed wait) must land before the warp's shared memory can be reused
+    if (lane == 0) {
+        const uint64_t lim = ok ? kWaitNs : kDrainNs;
+        for (int r = t + 1; r < s_issued; r++)
+            mbar_wait(smem_u32(&sbar[r & (kHSlots - 1)]), (uint32_t)(r / kHSlots) & 1u, lim);
+        if (!ok) mbar_wait(smem_u32(&sbar[t & (kHSlots - 1)]), (uint32_t)(t / kHSlots) & 1u, lim);
+        if (dx > 0) {
+            for (int c = need; c < next; c++) mbar_wait(chunk_bar(c), (uint32_t)chunk_use(c) & 1u, lim);
+        } else {
+            for (int c = need; c > next; c--) mbar_wait(chunk_bar(c), (uint32_t)chunk_use(c) & 1u, lim);
+        }
+        if (!ok) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
+        for (int b = 0; b < kHSlots + kChunkSlots; b++) mbar_inval(smem_u32(&sbar[b]));
+    }
+    if (!ok) return;
+
+    if (lr) {
+        __syncwarp();
+        for (int xx = lane; xx < W; xx += 32) {
+            const int dl = rowL[xx];
+            const int xr = xx - dl;
+            const bool bad = xr < 0 || abs(dl - (int)rowR[xr]) > k.lr_thr;
+            const size_t o = (size_t)y * W + xx;
+            if (k.disp) k.disp[o] = bad ? (uint16_t)0xFFFF : (uint16_t)dl;
+            if (k.disp_norm) k.disp_norm[o] = bad ? -1.0f : __fdiv_rn((float)dl, (float)k.D);
+            if (k.disp_right) k.disp_right[o] = rowR[xx];
+        }
+    }
+}
+
+// ------------------------------------------- horizontal passes, split D
+// Two warps per image row: warp h owns disparity pairs [h*32*PH, (h+1)*32*PH)
+// (PH pairs per lane).  Each step they exchange, through shared memory and one
+// 64-thread named barrier, what couples the halves: the minimum of the new L
+// (the m of the next step), the boundary neighbour across the split, and in
+// the last pass the WTA key and the right-view chain value.  This doubles the
+// independent work per SM over one warp per row (1080 rows fill only ~7 warps
+// of each of the 148 SMs).
+template <int PH, int MODE>
+__device__ __forceinline__ void h2_body(const FK& k, int dx, int R, int warp_bytes, int row_bytes, int blk,
+                                        unsigned char* smem, bool nc) {
+    constexpr int SBH = 128 * PH;  // this warp's share of a pixel's S vector
+    constexpr int DH = 64 * PH;    // disparities per warp
+    constexpr int NJ = 2 * PH;
+    constexpr int CH = kChunk2;  // entries per chunk
+    constexpr int CHB = (CH / 8) * kGroupBytes;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ri = warp >> 1, h = warp & 1;
+    const int y = blk * R + ri;
+    if (ri >= R || y >= k.H) return;  // both warps of the row leave together
+    unsigned char* wbase = smem + (size_t)warp * warp_bytes;
+    unsigned char* rbase = smem + (size_t)2 * R * warp_bytes + (size_t)ri * row_bytes;
+    uint64_t* sbar = (uint64_t*)wbase;
+    uint64_t* cbar = sbar + kHSlots;
+    unsigned char* sring = wbase + 128;
+    unsigned char* cring = sring + kHSlots * SBH;
+    uint32_t* xch = (uint32_t*)rbase;  // [2 parity][2 warps][8]
+    uint16_t* rowL = (uint16_t*)(rbase + 128);
+    uint16_t* rowR = rowL + k.W;
+    const bool lr = MODE == 2 && k.lr_thr >= 0;
+    const int bar_id = 1 + ri;
+
+    const int W = k.W;
+    const int x0 = dx > 0 ? 0 : W - 1;
+    const int dlo = h * DH, dhi = dlo + DH;
+    const int nch = (W + CH - 1) / CH;
+    const int groups_row = (W + 7) / 8;
+    const Plane* rrow = k.RPp + (size_t)y * k.Wp;
+    const uint32_t* srow = k.S + (size_t)y * W * k.Dp2 + h * (SBH / 4);
+
+    if (lane == 0) {
+        for (int b = 0; b < kHSlots + kChunkSlots; b++) mbar_init(smem_u32(&sbar[b]), 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+
+    auto e_lo = [&](int x) { return max(0, x - dhi + 2); };
+    auto e_hi = [&](int x) { return max(0, x - dlo); };
+    // a warp walking right to left starts at its own first chunk c0, which is
+    // below nch-1 for the upper half; phases count from there
+    const int c0 = dx > 0 ? 0 : e_hi(W - 1) / CH;
+    auto chunk_use = [&](int c) { return dx > 0 ? c / kChunkSlots : (c0 - c) / kChunkSlots; };
+    auto chunk_bar = [&](int c) { return smem_u32(&cbar[c & (kChunkSlots - 1)]); };
+    auto issue_chunk = [&](int c) {
+        const int ng = min(CH / 8, groups_row - c * (CH / 8));
+        const uint32_t bar = chunk_bar(c);
+        mbar_expect_tx(bar, (uint32_t)ng * kGroupBytes);
+        tma_load(smem_u32(cring + (c & (kChunkSlots - 1)) * CHB), rrow + 9 * (c * (CH / 8)),
+                 (uint32_t)ng * kGroupBytes, bar);
+    };
+    auto issue_s = [&](int t) {
+        const int x = x0 + dx * t;
+        const uint32_t bar = smem_u32(&sbar[t & (kHSlots - 1)]);
+        mbar_expect_tx(bar, SBH);
+        tma_load(smem_u32(sring + (t & (kHSlots - 1)) * SBH), srow + (size_t)x * k.Dp2, SBH, bar);
+    };
+
+    // chunk window [e_lo(x), e_hi(x)]: `waited` is the last chunk waited for,
+    // `next` the next to issue, both moving in the walk direction
+    int waited, next;
+    if (dx > 0) {
+        waited = -1;
+        next = 0;
+    } else {
+        waited = c0 + 1;
+        next = c0;
+    }
+    int s_issued = 0;
+    if (lane == 0)
+        for (; s_issued < kHSlots && s_issued < W; s_issued++) issue_s(s_issued);
+    s_issued = __shfl_sync(FULL, s_issued, 0);
+
+    bool ok = true;
+    const int base_d = dlo + lane * 2 * PH;
+    const bool edge_lane = base_d + 2 * PH > k.D;
+    uint32_t L[PH], m = 0, sv[PH], bnd = k.BIGBIG;
+    uint32_t P[NJ];
+    #pragma unroll
+    for (int j = 0; j < NJ; j++) P[j] = FULL;
+    uint4 lp_next = ld_plane(&k.LP[(size_t)y * W + x0], nc);
+    uint32_t* sg = k.S + ((size_t)y * W + x0) * k.Dp2 + h * (SBH / 4) + lane * PH;
+    const long long sstep = (long long)dx * k.Dp2;
+
+    int t = 0;
+    for (; t < W; t++) {
+        const int x = x0 + dx * t;
+        bool good = true;
+        if (dx > 0) {
+            const int tc = e_hi(x) / CH;
+            if (lane == 0)
+                while (next < nch && next <= tc + kLookC) issue_chunk(next++);
+            while (good && waited < tc) {
+                waited++;
+                good = mbar_wait(chunk_bar(waited), (uint32_t)chunk_use(waited) & 1u);
+            }
+        } else {
+            const int tc = e_lo(x) / CH;
+            if (lane == 0)
+                while (next >= 0 && next >= tc - kLookC) issue_chunk(next--);
+            while (good && waited > tc) {
+                waited--;
+                good = mbar_wait(chunk_bar(waited), (uint32_t)chunk_use(waited) & 1u);
+            }
+        }
+        next = __shfl_sync(FULL, next, 0);
+        good = good && mbar_wait(smem_u32(&sbar[t & (kHSlots - 1)]), (uint32_t)(t / kHSlots) & 1u);
+        const bool mine_ok = __all_sync(FULL, good);
+        uint32_t kmin = FULL;
+        if (mine_ok) {
+        const uint4 lp = lp_next;
+        if (t + 1 < W) lp_next = ld_plane(&k.LP[(size_t)y * W + x + dx], nc);
+        uint32_t c[PH], Ln[PH];
+        const int eb = x - base_d;
+        #pragma unroll
+        for (int q = 0; q < PH; q++) {
+            const int e = max(eb - 2 * q, 0);
+            c[q] = bt_pair(lp, *(const uint4*)(cring + ppos(e & (kChunkSlots * CH - 1)) * 16));
+        }
+        if (edge_lane || eb < 2 * PH) {
+            const int lim = min(x + 1, k.D);
+            #pragma unroll
+            for (int q = 0; q < PH; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
+        }
+        if (t == 0) {
+            #pragma unroll
+            for (int q = 0; q < PH; q++) Ln[q] = c[q];
+        } else {
+            // neighbours across lanes, and across the two warps at the split
+            const uint32_t MM = m * 0x10001u;
+            const uint32_t MP2 = MM + k.P2P2;
+            uint32_t up = __shfl_up_sync(FULL, L[PH - 1], 1);
+            uint32_t dn = __shfl_down_sync(FULL, L[0], 1);
+            if (lane == 0) up = h == 0 ? k.BIGBIG : bnd;
+            if (lane == 31) dn = h == 1 ? k.BIGBIG : bnd;
+            #pragma unroll
+            for (int q = 0; q < PH; q++) {
+                const uint32_t lm = hi_lo(q > 0 ? L[q - 1] : up, L[q]);
+                const uint32_t lpn = hi_lo(L[q], q < PH - 1 ? L[q + 1] : dn);
+                uint32_t tv = vmin2(lm, lpn) + k.P1P1;
+                tv = vmin2(vmin2(tv, L[q]), MP2);
+                Ln[q] = tv + c[q] - MM;
+            }
+        }
+        Vec<PH>::lds((const uint32_t*)(sring + (t & (kHSlots - 1)) * SBH) + lane * PH, sv);
+        #pragma unroll
+        for (int q = 0; q < PH; q++) sv[q] += Ln[q];
+        if (MODE == 1) {
+            Vec<PH>::st(sg, sv);
+        } else {
+            uint32_t key[NJ];
+            #pragma unroll
+            for (int q = 0; q < PH; q++) {
+                key[2 * q] = ((sv[q] & 0xFFFFu) << 8) | (uint32_t)(base_d + 2 * q);
+                key[2 * q + 1] = ((sv[q] >> 16) << 8) | (uint32_t)(base_d + 2 * q + 1);
+            }
+            kmin = key[0];
+            #pragma unroll
+            for (int j = 1; j < NJ; j++) kmin = min(kmin, key[j]);
+            kmin = __reduce_min_sync(FULL, kmin);
+            if (lr) {
+                #pragma unroll
+                for (int j = 0; j < NJ; j++) P[j] = min(P[j], key[j]);
+            }
+        }
+        sg += sstep;
+        #pragma unroll
+        for (int q = 0; q < PH; q++) L[q] = Ln[q];
+        }  // mine_ok
+        // ---- exchange with the other half (double-buffered by step parity);
+        //      a failed wait on either side ends both warps at this step ----
+        uint32_t lmin = L[0];
+        #pragma unroll
+        for (int q = 1; q < PH; q++) lmin = vmin2(lmin, L[q]);
+        lmin = __reduce_min_sync(FULL, min(lmin & 0xFFFFu, lmin >> 16));
+        uint32_t* mine = xch + ((t & 1) * 2 + h) * 8;
+        const uint32_t* other = xch + ((t & 1) * 2 + (1 - h)) * 8;
+        const uint32_t chain_out = __shfl_sync(FULL, P[0], 0);  // warp 1 lane 0 feeds warp 0 lane 31
+        const uint32_t edge = __shfl_sync(FULL, h == 0 ? L[PH - 1] : L[0], h == 0 ? 31 : 0);
+        if (lane == 0) {
+            mine[0] = lmin;
+            mine[1] = edge;
+            mine[2] = kmin;
+            mine[3] = chain_out;
+            mine[4] = mine_ok ? 0u : 1u;
+        }
+        asm volatile("bar.sync %0, 64;" ::"r"(bar_id) : "memory");
+        ok = mine_ok && other[4] == 0u;
+        if (!ok) break;
+        m = min(lmin, other[0]);
+        bnd = other[1];
+        if (MODE == 2) {
+            const uint32_t kk = min(kmin, other[2]);
+            if (lr) {
+                uint32_t in = __shfl_down_sync(FULL, P[0], 1);
+                if (lane == 31) in = h == 0 ? other[3] : FULL;
+                if (h == 0 && lane == 0) {
+                    rowR[x] = (uint16_t)(P[0] & 0xFFu);
+                    rowL[x] = (uint16_t)(kk & 0xFFu);
+                }
+                #pragma unroll
+                for (int j = 0; j < NJ - 1; j++) P[j] = P[j + 1];
+                P[NJ - 1] = in;
+            } else if (h == 0 && lane == 0) {
+                const size_t o = (size_t)y * W + x;
+                const uint16_t dl = (uint16_t)(kk & 0xFFu);
+                if (k.disp) k.disp[o] = dl;
+                if (k.disp_norm) k.disp_norm[o] = __fdiv_rn((float)dl, (float)k.D);
+            }
+        }
+        __syncwarp();
+        if (s_issued < W) {
+            if (lane == 0) issue_s(s_issued);
+            s_issued++;
+        }
+    }
+
+    if (lane == 0) {
+        const uint64_t lim = ok ? kWaitNs : kDrainNs;
+        for (int r = t + 1; r < s_issued; r++)
+            mbar_wait(smem_u32(&sbar[r & (kHSlots - 1)]), (uint32_t)(r / kHSlots) & 1u, lim);
+        if (!ok) mbar_wait(smem_u32(&sbar[t & (kHSlots - 1)]), (uint32_t)(t / kHSlots) & 1u, lim);
+        if (dx > 0) {
+            for (int c = waited + 1; c < next; c++) mbar_wait(chunk_bar(c), (uint32_t)chunk_use(c) & 1u, lim);
+        } else {
+            for (int c = waited - 1; c > next; c--) mbar_wait(chunk_bar(c), (uint32_t)chunk_use(c) & 1u, lim);
+        }
+        if (!ok) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
+        for (int b = 0; b < kHSlots + kChunkSlots; b++) mbar_inval(smem_u32(&sbar[b]));
+    }
+    if (!ok) return;
+
+    if (lr) {
+        asm volatile("bar.sync %0, 64;" ::"r"(bar_id) : "memory");
+        for (int xx = h * 32 + lane; xx < W; xx += 64) {
+            const int dl = rowL[xx];
+            const int xr = xx - dl;
+            const bool bad = xr < 0 || abs(dl - (int)rowR[xr]) > k.lr_thr;
+            const size_t o = (size_t)y * W + xx;
+            if (k.disp) k.disp[o] = bad ? (uint16_t)0xFFFF : (uint16_t)dl;
+            if (k.disp_norm) k.disp_norm[o] = bad ? -1.0f : __fdiv_rn((float)dl, (float)k.D);
+            if (k.disp_right) k.disp_right[o] = rowR[xx];
+        }
+    }
+}
+
+}  // namespace
+}  // namespace tdv

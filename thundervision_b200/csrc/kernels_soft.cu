@@ -103,7 +103,8 @@ struct SoftK {
     const long long* ckpt_off;  // [dir][walk] first checkpoint index of the walk
     int W, H, D, ck;
     T p1, p2;
-    T* dpen;  // [2] dP1, dP2
+    T* dpen;     // [2] dP1, dP2
+    T* dpen_part;  // [dir][walk][2] per-walk partial sums (summed in a fixed order)
 };
 
 // L_t from L_{t-1}: returns the choice code of each disparity.
@@ -395,9 +396,26 @@ __global__ void __launch_bounds__(128) soft_bwd_pass(SoftK<T> k, int dx, int dy,
     gp1 = warp_sum(gp1);
     gp2 = warp_sum(gp2);
     if (lane == 0) {
-        atomicAdd(&k.dpen[0], gp1);
-        atomicAdd(&k.dpen[1], gp2);
+        T* part = k.dpen_part + ((size_t)dir * (k.W + k.H) + w) * 2;
+        part[0] = gp1;
+        part[1] = gp2;
     }
+}
+
+// dP = sum of the per-walk partials in a fixed order (deterministic).
+template <typename T>
+__global__ void soft_pen_reduce(const T* part, int ndir, int W, int H, T* dpen) {
+    const int lane = threadIdx.x & 31;
+    const int which = threadIdx.x >> 5;  // 0: P1, 1: P2
+    if (which > 1) return;
+    T acc = 0;
+    for (int d = 0; d < ndir; d++) {
+        const int dx = d == 2 || d == 3 ? 0 : 1, dy = d < 2 ? 0 : 1;
+        const int nw = dy == 0 ? H : (dx == 0 ? W : W + H - 1);
+        for (int w = lane; w < nw; w += 32) acc += part[((size_t)d * (W + H) + w) * 2 + which];
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) dpen[which] = acc;
 }
 
 const int kDirs8[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1}, {-1, 1}, {1, -1}};
@@ -494,18 +512,22 @@ cudaError_t soft_backward_t(const SoftLaunch& L, cudaStream_t st, Timer* tm) {
     k.p1 = (T)L.p1;
     k.p2 = (T)L.p2;
     k.dpen = (T*)L.dpen;
+    k.dpen_part = (T*)L.dpen_part;
     const int npix = L.W * L.H;
-    cudaError_t e = cudaMemsetAsync(L.dpen, 0, 2 * sizeof(T), st);
-    if (e != cudaSuccess) return e;
+    cudaError_t e;
     soft_ds_kernel<T><<<grid_for((size_t)npix * L.D, 256), 256, 0, st>>>(
         (const T*)L.S, (const T*)L.stats, (const T*)L.g, npix, L.D, (T)L.tau, (T*)L.dS);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (tm) tm->mark("soft_dS");
     const bool ck = L.ck > 0;
-    if (L.D <= 32) return bwd_all<T, 1>(k, L.paths, ck, st, tm);
-    if (L.D <= 64) return bwd_all<T, 2>(k, L.paths, ck, st, tm);
-    if (L.D <= 128) return bwd_all<T, 4>(k, L.paths, ck, st, tm);
-    return bwd_all<T, 8>(k, L.paths, ck, st, tm);
+    if (L.D <= 32) e = bwd_all<T, 1>(k, L.paths, ck, st, tm);
+    else if (L.D <= 64) e = bwd_all<T, 2>(k, L.paths, ck, st, tm);
+    else if (L.D <= 128) e = bwd_all<T, 4>(k, L.paths, ck, st, tm);
+    else e = bwd_all<T, 8>(k, L.paths, ck, st, tm);
+    if (e != cudaSuccess) return e;
+    soft_pen_reduce<T><<<1, 64, 0, st>>>(k.dpen_part, L.paths == 4 ? 4 : 8, L.W, L.H, k.dpen);
+    if (tm) tm->mark("soft_pen_reduce");
+    return cudaGetLastError();
 }
 
 }  // namespace

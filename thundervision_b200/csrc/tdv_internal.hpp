@@ -160,6 +160,40 @@ size_t fused_agg_bytes(int W, int H, int D);
 size_t fused_plane_bytes(int W, int H);
 cudaError_t launch_fused(const FusedArgs& a, cudaStream_t st, Timer* tm);
 
+// Batched fused path (kernels_batch.cu): one persistent launch for many
+// integer-domain pairs of uneven size and disparity range.
+struct BatchPairArgs {
+    ImgArg L, R;
+    int W, H, D;
+    uint16_t* disp;
+    float* disp_norm;
+    uint16_t* disp_right;
+    int lr_thr;
+};
+using BatchTiles = tdv_batch_tiles;
+// Device image of the plan: [control words][pair descriptors][work items].
+struct BatchPlan {
+    std::vector<unsigned char> desc;
+    size_t ctl_off = 0, pairs_off = 0, items_off = 0, bytes = 0;
+    int n_pairs = 0, n_items = 0, smem = 0, item_bytes = 0;
+};
+int batch_passes();
+int batch_threads();
+size_t batch_ctl_bytes(int npairs);
+// planes + aggregation volumes of all pairs, each 256-byte aligned
+size_t batch_scratch_bytes(const std::vector<BatchPairArgs>& pairs);
+// Builds the plan for scratch at `scratch` and the descriptor copy at
+// `d_desc` (device addresses, used only to fill pointers); returns an error
+// message, or nullptr on success.
+const char* batch_plan(const std::vector<BatchPairArgs>& pairs, int p1h, int p2h, int paths,
+                       const BatchTiles& t, unsigned char* scratch, unsigned char* d_desc, BatchPlan& out);
+// Opts the persistent kernel into the plan's dynamic shared memory.
+cudaError_t batch_configure(const BatchPlan& plan);
+// Zeroes the control words and launches the persistent kernel (grid blocks);
+// batch_configure must have run for a plan of at least this shared memory.
+cudaError_t batch_launch(const BatchPlan& plan, unsigned char* d_desc, unsigned long long wait_ns, int grid,
+                         cudaStream_t st);
+
 // Differentiable soft-argmin SGM (kernels_soft.cu).
 struct SoftLaunch {
     int f64;
@@ -175,6 +209,7 @@ struct SoftLaunch {
     void* stats;
     const void* g;
     void* dpen;
+    void* dpen_part;
     int W, H, D, paths, ck, record;
     double p1, p2, tau;
 };
