@@ -1022,11 +1022,19 @@ tdv_status tdv_batch_autotune(tdv_batch* b, int32_t reps, tdv_stream stream, tdv
     tdv_batch_tiles best = b->tiles;
     double best_t = HUGE_VAL;
     tdv_status st_all = time_tiles(best, best_t);
-    // coordinate descent over the tile shapes, one axis at a time
-    const int Gs[] = {8, 12, 16, 20, 24};
-    const int Rs[] = {4, 6, 8, 12, 16, 24};
+    // coordinate descent over the tile shapes, one axis at a time; besides
+    // fixed sizes, the sizes that give the largest pair one tile per SM
+    int wmax = 1, hmax = 1;
+    for (const auto& p : b->pairs) {
+        wmax = std::max(wmax, p.W);
+        hmax = std::max(hmax, p.H);
+    }
+    const int g_fit = std::min(24, std::max(1, (wmax + b->grid - 1) / b->grid));
+    const int r_fit = std::min(24, std::max(1, (hmax + b->grid - 1) / b->grid));
+    const int Gs[] = {8, 12, 16, 20, 24, g_fit};
+    const int Rs[] = {4, 6, 8, 12, 16, 24, r_fit};
     for (int axis = 0; axis < 4 && st_all == TDV_OK; axis++) {
-        const int n = axis == 0 ? 5 : (axis == 1 ? 6 : 2);
+        const int n = axis == 0 ? 6 : (axis == 1 ? 7 : 2);
         for (int j = 0; j < n && st_all == TDV_OK; j++) {
             tdv_batch_tiles t = best;
             if (axis == 0) t.lines_per_cta = Gs[j];

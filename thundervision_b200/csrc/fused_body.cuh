@@ -669,6 +669,268 @@ __device__ __forceinline__ void h_body(const FK& k, int dx, int GH, int warp_byt
     }
 }
 
+// ------------------------------------- horizontal passes, producer-fed
+// R consumer warps (one image row each, walking x in direction dx) and one
+// producer warp whose lane r keeps row r's rings full, so the consumers carry
+// no copy bookkeeping.  Per row:
+//   * an S ring of kHpSlots slots, each holding kHpU consecutive pixels of
+//     the row: their S vectors and their left-plane entries (two TMA bulk
+//     copies per slot); a consumer waits once per kHpU steps and releases the
+//     slot (mbarrier arrive) when it has read it;
+//   * a right-plane chunk ring of kChunkSlots chunks of kChunk entries, chunk
+//     c in slot c & 7; the consumer releases a chunk when its disparity
+//     window [x - 64*PPL + 2, x] has left it, the producer refills the slot
+//     with the chunk 8 places further in walk order.
+// The producer lanes never block: each polls its own row's empty barriers and
+// issues what has become free; the warp sleeps briefly when no lane could
+// issue and gives up (TDV_ERR_TIMEOUT) after kWaitNs without progress.
+// The recurrence starts from L = 0, m = 0, which makes the first step L = C
+// without a branch (min(0, 0 + P1, 0 + P2) = 0).
+constexpr int kHpU = 4;      // pixels per S slot
+constexpr int kHpSlots = 4;  // S slots per row
+constexpr int kHpBars = 2 * kHpSlots + 2 * kChunkSlots;
+
+__host__ __device__ inline int hp_slot_bytes(int ppl) { return kHpU * (128 * ppl + 16); }
+__host__ __device__ inline int hp_warp_bytes(int ppl, bool lr, int W) {
+    return align128(kHpSlots * hp_slot_bytes(ppl) + kChunkSlots * kChunkBytes + (lr ? 2 * W * 2 : 0));
+}
+__host__ __device__ inline int hp_smem_bytes(int R, int ppl, bool lr, int W) {
+    return align128(R * kHpBars * 8) + R * hp_warp_bytes(ppl, lr, W);
+}
+
+template <int PPL, int MODE>
+__device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, unsigned char* smem) {
+    constexpr int SB = 128 * PPL;
+    constexpr int DSPAN = 64 * PPL;
+    constexpr int NJ = 2 * PPL;
+    constexpr int SLOT = kHpU * (SB + 16);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int W = k.W;
+    const bool lr = MODE == 2 && k.lr_thr >= 0;
+    const int wb = hp_warp_bytes(PPL, lr, W);
+    uint64_t* bars = (uint64_t*)smem;
+    unsigned char* data = smem + align128(R * kHpBars * 8);
+    const int y0 = blk * R;
+    const int Rb = min(R, k.H - y0);  // rows of this block
+    const int ngroups = (W + kHpU - 1) / kHpU;
+    const int nch = (W + kChunk - 1) / kChunk;
+    const int c0 = dx > 0 ? 0 : nch - 1;  // first chunk in walk order
+    // row r: fullS[kHpSlots] emptyS[kHpSlots] fullC[8] emptyC[8]
+    auto fullS = [&](int r, int s) { return smem_u32(&bars[r * kHpBars + s]); };
+    auto emptyS = [&](int r, int s) { return smem_u32(&bars[r * kHpBars + kHpSlots + s]); };
+    auto fullC = [&](int r, int s) { return smem_u32(&bars[r * kHpBars + 2 * kHpSlots + s]); };
+    auto emptyC = [&](int r, int s) { return smem_u32(&bars[r * kHpBars + 2 * kHpSlots + kChunkSlots + s]); };
+    auto group_lo = [&](int j) { return dx > 0 ? j * kHpU : max(0, W - 1 - j * kHpU - (kHpU - 1)); };
+    auto group_hi = [&](int j) { return dx > 0 ? min(W - 1, j * kHpU + kHpU - 1) : W - 1 - j * kHpU; };
+    auto cl_of = [&](int x) { return max(0, x - DSPAN + 2) >> 6; };
+
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < R * kHpBars; b++) mbar_init(smem_u32(&bars[b]), 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    if (warp == R) {
+        // ---- producer: lane r feeds row r ----
+        const bool mine = lane < Rb;
+        const int y = y0 + lane;
+        unsigned char* wbase = data + (size_t)lane * wb;
+        int g = 0, kc = 0;
+        bool failed = false;
+        uint64_t t_last = global_ns();
+        for (;;) {
+            bool pending = false, did = false;
+            if (mine) {
+                if (g < ngroups) {
+                    pending = true;
+                    const int s = g % kHpSlots;
+                    if (g < kHpSlots || mbar_try(emptyS(lane, s), (uint32_t)((g / kHpSlots) - 1) & 1u)) {
+                        const int xlo = group_lo(g), n = group_hi(g) - xlo + 1;
+                        unsigned char* dst = wbase + s * SLOT;
+                        const uint32_t bar = fullS(lane, s);
+                        mbar_expect_tx(bar, (uint32_t)n * (SB + 16));
+                        tma_load(smem_u32(dst), k.S + ((size_t)y * W + xlo) * k.Dp2, (uint32_t)n * SB, bar);
+                        tma_load(smem_u32(dst + kHpU * SB), k.LP + (size_t)y * W + xlo, (uint32_t)n * 16, bar);
+                        g++;
+                        did = true;
+                    }
+                }
+                if (kc < nch) {
+                    pending = true;
+                    const int c = dx > 0 ? kc : c0 - kc;
+                    const int s = c & (kChunkSlots - 1);
+                    if (kc < kChunkSlots || mbar_try(emptyC(lane, s), (uint32_t)((kc / kChunkSlots) - 1) & 1u)) {
+                        const int ng = min(kChunk / 8, (W + 7) / 8 - c * (kChunk / 8));
+                        const uint32_t bar = fullC(lane, s);
+                        mbar_expect_tx(bar, (uint32_t)ng * kGroupBytes);
+                        tma_load(smem_u32(wbase + kHpSlots * SLOT + s * kChunkBytes),
+                                 k.RPp + (size_t)y * k.Wp + 9 * (c * (kChunk / 8)), (uint32_t)ng * kGroupBytes, bar);
+                        kc++;
+                        did = true;
+                    }
+                }
+            }
+            if (!__any_sync(FULL, pending)) break;
+            if (__any_sync(FULL, did)) {
+                t_last = global_ns();
+            } else {
+                if (global_ns() - t_last > kWaitNs) {
+                    failed = true;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        // the block must not retire with copies in flight
+        if (mine) {
+            const uint64_t lim = failed ? kDrainNs : kWaitNs;
+            for (int j = max(0, g - kHpSlots); j < g; j++)
+                mbar_wait(fullS(lane, j % kHpSlots), (uint32_t)(j / kHpSlots) & 1u, lim);
+            for (int q = max(0, kc - kChunkSlots); q < kc; q++) {
+                const int c = dx > 0 ? q : c0 - q;
+                mbar_wait(fullC(lane, c & (kChunkSlots - 1)), (uint32_t)(q / kChunkSlots) & 1u, lim);
+            }
+        }
+        if (failed && lane == 0) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
+    } else if (warp < Rb) {
+        // ---- consumer: row y0 + warp ----
+        const int r = warp;
+        const int y = y0 + r;
+        unsigned char* wbase = data + (size_t)r * wb;
+        const unsigned char* cring = wbase + kHpSlots * SLOT;
+        uint16_t* rowL = (uint16_t*)(cring + kChunkSlots * kChunkBytes);
+        uint16_t* rowR = rowL + W;
+        const int base_d = lane * 2 * PPL;
+        const bool edge_lane = base_d + 2 * PPL > k.D;
+        uint32_t L[PPL], m = 0, sv[PPL];
+        uint32_t P[NJ];
+#pragma unroll
+        for (int q = 0; q < PPL; q++) L[q] = 0;
+#pragma unroll
+        for (int j = 0; j < NJ; j++) P[j] = FULL;
+        uint32_t* sg = k.S + ((size_t)y * W + (dx > 0 ? 0 : W - 1)) * k.Dp2 + lane * PPL;
+        const long long sstep = (long long)dx * k.Dp2;
+        int waited = dx > 0 ? -1 : c0 + 1;  // last chunk waited for
+        int rel = c0;                       // next chunk to release
+        bool ok = true;
+
+        auto step = [&](int x, const unsigned char* slot, int xlo) {
+            const uint4 lp = *(const uint4*)(slot + kHpU * SB + (x - xlo) * 16);
+            uint32_t c[PPL], Ln[PPL];
+            const int eb = x - base_d;
+#pragma unroll
+            for (int q = 0; q < PPL; q++) {
+                const int e = max(eb - 2 * q, 0);
+                c[q] = bt_pair(lp, *(const uint4*)(cring + ppos(e & (kChunkSlots * kChunk - 1)) * 16));
+            }
+            if (edge_lane || eb < 2 * PPL) {
+                const int lim = min(x + 1, k.D);
+#pragma unroll
+                for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
+            }
+            recur<PPL>(L, m, c, Ln, lane, k);
+            Vec<PPL>::lds((const uint32_t*)(slot + (x - xlo) * SB) + lane * PPL, sv);
+#pragma unroll
+            for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
+            if (MODE == 1) {
+                Vec<PPL>::st(sg, sv);
+            } else {
+                // WTA key (S << 8 | d): lowest S, then lowest d (tdvision/wtacpu.cpp:26-30)
+                uint32_t key[NJ];
+#pragma unroll
+                for (int q = 0; q < PPL; q++) {
+                    key[2 * q] = ((sv[q] & 0xFFFFu) << 8) | (uint32_t)(base_d + 2 * q);
+                    key[2 * q + 1] = ((sv[q] >> 16) << 8) | (uint32_t)(base_d + 2 * q + 1);
+                }
+                uint32_t kmin = key[0];
+#pragma unroll
+                for (int j = 1; j < NJ; j++) kmin = min(kmin, key[j]);
+                kmin = __reduce_min_sync(FULL, kmin);
+                if (lr) {
+#pragma unroll
+                    for (int j = 0; j < NJ; j++) P[j] = min(P[j], key[j]);
+                    uint32_t in = __shfl_down_sync(FULL, P[0], 1);
+                    if (lane == 31) in = FULL;
+                    if (lane == 0) {
+                        rowR[x] = (uint16_t)(P[0] & 0xFFu);
+                        rowL[x] = (uint16_t)(kmin & 0xFFu);
+                    }
+#pragma unroll
+                    for (int j = 0; j < NJ - 1; j++) P[j] = P[j + 1];
+                    P[NJ - 1] = in;
+                } else if (lane == 0) {
+                    const size_t o = (size_t)y * W + x;
+                    const uint16_t dl = (uint16_t)(kmin & 0xFFu);
+                    if (k.disp) k.disp[o] = dl;
+                    if (k.disp_norm) k.disp_norm[o] = __fdiv_rn((float)dl, (float)k.D);
+                }
+            }
+            sg += sstep;
+#pragma unroll
+            for (int q = 0; q < PPL; q++) L[q] = Ln[q];
+            m = warp_min_pairs<PPL>(L);
+        };
+
+        for (int j = 0; j < ngroups; j++) {
+            const int s = j % kHpSlots;
+            const int xlo = group_lo(j), xhi = group_hi(j);
+            // right-plane chunks: release what the window has left, wait for
+            // what this group's window reaches
+            bool good = true;
+            if (dx > 0) {
+                const int lo = cl_of(xlo), need = xhi >> 6;
+                if (lane == 0)
+                    for (; rel < lo; rel++) mbar_arrive(emptyC(r, rel & (kChunkSlots - 1)));
+                while (good && waited < need) {
+                    waited++;
+                    good = mbar_wait(fullC(r, waited & (kChunkSlots - 1)), (uint32_t)(waited / kChunkSlots) & 1u);
+                }
+            } else {
+                const int hi = xhi >> 6, need = cl_of(xlo);
+                if (lane == 0)
+                    for (; rel > hi; rel--) mbar_arrive(emptyC(r, rel & (kChunkSlots - 1)));
+                while (good && waited > need) {
+                    waited--;
+                    good = mbar_wait(fullC(r, waited & (kChunkSlots - 1)),
+                                     (uint32_t)((c0 - waited) / kChunkSlots) & 1u);
+                }
+            }
+            good = good && mbar_wait(fullS(r, s), (uint32_t)(j / kHpSlots) & 1u);
+            if (!__all_sync(FULL, good)) {
+                ok = false;
+                break;
+            }
+            const unsigned char* slot = wbase + s * SLOT;
+            if (xhi - xlo + 1 == kHpU) {
+#pragma unroll
+                for (int i = 0; i < kHpU; i++) step(dx > 0 ? xlo + i : xhi - i, slot, xlo);
+            } else {
+                for (int i = 0; i <= xhi - xlo; i++) step(dx > 0 ? xlo + i : xhi - i, slot, xlo);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(emptyS(r, s));
+        }
+        if (!ok) {
+            if (lane == 0) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
+        } else if (lr) {
+            __syncwarp();
+            for (int xx = lane; xx < W; xx += 32) {
+                const int dl = rowL[xx];
+                const int xr = xx - dl;
+                const bool bad = xr < 0 || abs(dl - (int)rowR[xr]) > k.lr_thr;
+                const size_t o = (size_t)y * W + xx;
+                if (k.disp) k.disp[o] = bad ? (uint16_t)0xFFFF : (uint16_t)dl;
+                if (k.disp_norm) k.disp_norm[o] = bad ? -1.0f : __fdiv_rn((float)dl, (float)k.D);
+                if (k.disp_right) k.disp_right[o] = rowR[xx];
+            }
+        }
+    }
+    // every role is done with the rings: retire the barriers
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int b = 0; b < R * kHpBars; b++) mbar_inval(smem_u32(&bars[b]));
+}
+
 // ------------------------------------------- horizontal passes, split D
 // Two warps per image row: warp h owns disparity pairs [h*32*PH, (h+1)*32*PH)
 // (PH pairs per lane).  Each step they exchange, through shared memory and one

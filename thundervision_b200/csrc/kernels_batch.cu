@@ -99,9 +99,9 @@ __device__ __forceinline__ void run_h(const BPair& P, int dx, int blk, unsigned 
         if (P.ppl == 2) h2_body<1, MODE>(k, dx, P.hrows, P.hwb, P.hrb, blk, smem, false);
         else h2_body<2, MODE>(k, dx, P.hrows, P.hwb, P.hrb, blk, smem, false);
     } else {
-        if (P.ppl == 1) h_body<1, MODE>(k, dx, P.hrows, P.hwb, blk, smem, false);
-        else if (P.ppl == 2) h_body<2, MODE>(k, dx, P.hrows, P.hwb, blk, smem, false);
-        else h_body<4, MODE>(k, dx, P.hrows, P.hwb, blk, smem, false);
+        if (P.ppl == 1) hp_body<1, MODE>(k, dx, P.hrows, blk, smem);
+        else if (P.ppl == 2) hp_body<2, MODE>(k, dx, P.hrows, blk, smem);
+        else hp_body<4, MODE>(k, dx, P.hrows, blk, smem);
     }
 }
 
@@ -257,10 +257,12 @@ const char* batch_plan(const std::vector<BatchPairArgs>& pairs, int p1h, int p2h
             if (rows * (2 * P.hwb + P.hrb) > kSmemBudget) return "horizontal pass tile does not fit in shared memory";
             smem = std::max(smem, rows * (2 * P.hwb + P.hrb));
         } else {
-            P.hwb = h_warp_bytes(P.ppl, lr, a.W);
-            while (rows > 1 && rows * P.hwb > kSmemBudget) rows--;
-            if (rows * P.hwb > kSmemBudget) return "horizontal pass tile does not fit in shared memory";
-            smem = std::max(smem, rows * P.hwb);
+            // producer-fed rows: one consumer warp per row plus the producer warp
+            rows = std::min(rows, kBatchWarps - 1);
+            while (rows > 1 && hp_smem_bytes(rows, P.ppl, lr, a.W) > kSmemBudget) rows--;
+            if (hp_smem_bytes(rows, P.ppl, lr, a.W) > kSmemBudget)
+                return "horizontal pass tile does not fit in shared memory";
+            smem = std::max(smem, hp_smem_bytes(rows, P.ppl, lr, a.W));
         }
         P.hrows = rows;
         P.prep_rows = std::max(1, kPrepPixels / a.W);

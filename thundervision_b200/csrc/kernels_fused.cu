@@ -20,9 +20,9 @@ __global__ void __launch_bounds__((kMaxG + 1) * 32, 1)
 }
 
 template <int PPL, int MODE>
-__global__ void __launch_bounds__(kMaxGH * 32, 1) h_pass(FK k, int dx, int GH, int warp_bytes) {
+__global__ void __launch_bounds__((kMaxG + 1) * 32, 1) hp_pass(FK k, int dx, int R) {
     extern __shared__ __align__(128) unsigned char smem[];
-    h_body<PPL, MODE>(k, dx, GH, warp_bytes, blockIdx.x, smem, true);
+    hp_body<PPL, MODE>(k, dx, R, blockIdx.x, smem);
 }
 
 // ------------------------------------------------------------- host side
@@ -44,26 +44,24 @@ cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
 }
 
 template <int PPL, int MODE>
-cudaError_t launch_h(const FK& k, int dx, cudaStream_t st) {
-    const int warp_bytes = h_warp_bytes(PPL, MODE == 2 && k.lr_thr >= 0, k.W);
-    int GH = kSmemBudget / warp_bytes;
-    GH = GH > kMaxGH ? kMaxGH : GH;
-    if (GH < 1) return cudaErrorInvalidConfiguration;
-    const int smem = GH * warp_bytes;
-    cudaError_t e =
-        cudaFuncSetAttribute(h_pass<PPL, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+cudaError_t launch_hp(const FK& k, int dx, cudaStream_t st) {
+    const bool lr = MODE == 2 && k.lr_thr >= 0;
+    int R = (k.H + 147) / 148;  // rows per block: spread the rows over every SM
+    R = R < 1 ? 1 : (R > kMaxG ? kMaxG : R);
+    while (R > 1 && hp_smem_bytes(R, PPL, lr, k.W) > kSmemBudget) R--;
+    const int smem = hp_smem_bytes(R, PPL, lr, k.W);
+    if (smem > kSmemBudget) return cudaErrorInvalidConfiguration;
+    cudaError_t e = cudaFuncSetAttribute(hp_pass<PPL, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    const int blocks = (k.H + GH - 1) / GH;
-    h_pass<PPL, MODE><<<blocks, GH * 32, smem, st>>>(k, dx, GH, warp_bytes);
+    const int blocks = (k.H + R - 1) / R;
+    hp_pass<PPL, MODE><<<blocks, (R + 1) * 32, smem, st>>>(k, dx, R);
     return cudaGetLastError();
 }
 
-// One warp per row.  (The split-disparity body, two warps per row, doubles
-// the warps per SM but also the instructions per row step, and measured
-// slower at 1920x1080, D=256; the batch path keeps it as a tile option.)
+// One consumer warp per row plus a producer warp per block.
 template <int PPL>
 cudaError_t launch_hpass(const FK& k, int dx, int mode, cudaStream_t st) {
-    return mode == 1 ? launch_h<PPL, 1>(k, dx, st) : launch_h<PPL, 2>(k, dx, st);
+    return mode == 1 ? launch_hp<PPL, 1>(k, dx, st) : launch_hp<PPL, 2>(k, dx, st);
 }
 
 template <int PPL>
