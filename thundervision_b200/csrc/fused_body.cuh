@@ -103,6 +103,21 @@ __host__ __device__ inline int h2_warp_bytes(int ph) {
 }
 __host__ __device__ inline int h2_row_bytes(bool lr, int W) { return align128(128 + (lr ? 2 * W * 2 : 0)); }
 
+// Rows spanned by the path lines [kf, kf+Gb) of a vertical (s = 0) or
+// diagonal (s = +-1) pass, x = kp + s*y (the bounds vd_body walks).
+__host__ __device__ inline int group_rows(int W, int H, int s, int kf, int Gb) {
+    if (s == 0) return H;
+    int ylo, yhi;
+    if (s > 0) {
+        ylo = max(0, -(kf + Gb - 1));
+        yhi = min(H - 1, W - 1 - kf);
+    } else {
+        ylo = max(0, kf - W + 1);
+        yhi = min(H - 1, kf + Gb - 1);
+    }
+    return max(0, yhi - ylo + 1);
+}
+
 // ---------------------------------------------------------------- PTX
 __device__ __forceinline__ uint32_t vmin2(uint32_t a, uint32_t b) {
     uint32_t r;
@@ -310,8 +325,11 @@ __device__ __forceinline__ void recur(const uint32_t* L, uint32_t m, const uint3
 // Warps 0..G-1 consume one row per step; warp G is the producer: its lane 0
 // issues the TMA copies of row i into ring slot i % kRowSlots once every
 // consumer warp has released the slot's previous row (full/empty mbarrier
-// pairs), so no block-wide barrier is taken per row.
-template <int PPL, int MODE>
+// pairs), so no block-wide barrier is taken per row.  DIAG = false (s = 0):
+// a line is one column, so each lane's right-plane offsets are the same on
+// every row and are computed once; the recurrence starts from L = 0, m = 0
+// (first step L = C, as in the horizontal passes).
+template <int PPL, int MODE, bool DIAG>
 __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, int nlines, int G, int blk,
                                         unsigned char* smem) {
     constexpr int SB = 128 * PPL;
@@ -384,8 +402,62 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
                 mbar_wait(smem_u32(&full[r & (kRowSlots - 1)]), (uint32_t)(r / kRowSlots) & 1u,
                           ok ? kWaitNs : kDrainNs);
         }
+    } else if (warp < G && !DIAG) {
+        // ---- consumers, vertical: column x = kp on every row ----
+        const int x = kf + warp;
+        const bool has_line = warp < Gb;
+        const int base_d = lane * 2 * PPL;
+        const int eb = x - base_d;
+        const bool need_mask = base_d + 2 * PPL > k.D || eb < 2 * PPL;
+        const int lim = min(x + 1, k.D);
+        const int roff = -9 * (max(0, kf - DSPAN + 2) >> 3);
+        int rpos[PPL];
+#pragma unroll
+        for (int q = 0; q < PPL; q++) rpos[q] = (ppos(max(eb - 2 * q, 0)) + roff) * 16;
+        const unsigned char* lp_slot = slots + offL + warp * 16;
+        const unsigned char* sv_slot = slots + warp * SB + lane * PPL * 4;
+        const unsigned char* r_slot = slots + offR;
+        uint32_t L[PPL], m = 0;
+#pragma unroll
+        for (int q = 0; q < PPL; q++) L[q] = 0;
+        uint32_t* sg = k.S + ((size_t)y0 * k.W + x) * k.Dp2 + lane * PPL;
+        const long long sstep = (long long)dy * k.W * k.Dp2;
+        for (int i = 0; i < nrows; i++) {
+            const int b = i & (kRowSlots - 1);
+            if (!__all_sync(FULL, mbar_wait(smem_u32(&full[b]), (uint32_t)(i / kRowSlots) & 1u))) {
+                if (lane == 0) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
+                break;
+            }
+            if (has_line) {
+                const int boff = b * slotBytes;
+                const uint4 lp = *(const uint4*)(lp_slot + boff);
+                uint32_t c[PPL], Ln[PPL];
+#pragma unroll
+                for (int q = 0; q < PPL; q++) c[q] = bt_pair(lp, *(const uint4*)(r_slot + boff + rpos[q]));
+                if (need_mask) {
+#pragma unroll
+                    for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
+                }
+                recur<PPL>(L, m, c, Ln, lane, k);
+                if (MODE == 0) {
+                    Vec<PPL>::st(sg, Ln);
+                } else {
+                    uint32_t sv[PPL];
+                    Vec<PPL>::lds((const uint32_t*)(sv_slot + boff), sv);
+#pragma unroll
+                    for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
+                    Vec<PPL>::st(sg, sv);
+                }
+                sg += sstep;
+#pragma unroll
+                for (int q = 0; q < PPL; q++) L[q] = Ln[q];
+                m = warp_min_pairs<PPL>(L);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&empty[b]));
+        }
     } else if (warp < G) {
-        // ---- consumers ----
+        // ---- consumers, diagonal ----
         const int kp = kf + warp;
         const bool has_line = warp < Gb;
         const int base_d = lane * 2 * PPL;
@@ -450,7 +522,9 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
         }
     }
     // every role is done with the ring: retire its barriers so that the
-    // shared memory can be reused by the next work item
+    // shared memory can be reused by the next work item (whose TMA writes
+    // must follow this item's generic reads)
+    fence_proxy_async();
     __syncthreads();
     if (threadIdx.x == 0)
         for (int b = 0; b < 2 * kRowSlots; b++) mbar_inval(smem_u32(&full[b]));

@@ -81,15 +81,15 @@ __device__ bool wait_done(const int* cnt, int target, int* err, uint64_t limit_n
     }
 }
 
-template <int MODE>
+template <int MODE, bool DIAG>
 __device__ __forceinline__ void run_vd(const BPair& P, int pass, int blk, unsigned char* smem) {
     const FK& k = P.k;
     const int dx = kPassDx[pass], dy = kPassDy[pass], s = dx * dy;
     const int nlines = s == 0 ? k.W : k.W + k.H - 1;
     const int kmin = s > 0 ? -(k.H - 1) : 0;
-    if (P.ppl == 1) vd_body<1, MODE>(k, s, dy, kmin, nlines, P.G, blk, smem);
-    else if (P.ppl == 2) vd_body<2, MODE>(k, s, dy, kmin, nlines, P.G, blk, smem);
-    else vd_body<4, MODE>(k, s, dy, kmin, nlines, P.G, blk, smem);
+    if (P.ppl == 1) vd_body<1, MODE, DIAG>(k, s, dy, kmin, nlines, P.G, blk, smem);
+    else if (P.ppl == 2) vd_body<2, MODE, DIAG>(k, s, dy, kmin, nlines, P.G, blk, smem);
+    else vd_body<4, MODE, DIAG>(k, s, dy, kmin, nlines, P.G, blk, smem);
 }
 
 template <int MODE>
@@ -156,9 +156,11 @@ __global__ void __launch_bounds__(kBatchWarps * 32, 1)
             for (int i = threadIdx.x; i < n; i += blockDim.x)
                 prep_pixel(sp.L, sp.R, LP, RPp, k.W, k.Wp, i % k.W, y0 + i / k.W);
         } else if (pass == 1) {
-            run_vd<0>(sp, pass, blk, smem);
+            run_vd<0, false>(sp, pass, blk, smem);
+        } else if (pass == 2) {
+            run_vd<1, false>(sp, pass, blk, smem);
         } else if (pass <= 6) {
-            run_vd<1>(sp, pass, blk, smem);
+            run_vd<1, true>(sp, pass, blk, smem);
         } else if (pass == 7) {
             run_h<1>(sp, 1, blk, smem);
         } else {
@@ -303,8 +305,21 @@ const char* batch_plan(const std::vector<BatchPairArgs>& pairs, int p1h, int p2h
             std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
                 return item_weight(pairs[a], p) > item_weight(pairs[b], p);
             });
-        for (int i : idx)
-            for (int b = 0; b < hp[i].nb[p]; b++) items.push_back(BItem{i * 16 + p, b});
+        for (int i : idx) {
+            // a pair's diagonal line groups span 1..H rows: longest first
+            std::vector<int> blks(hp[i].nb[p]);
+            std::iota(blks.begin(), blks.end(), 0);
+            if (p >= 3 && p <= 6 && t.order == TDV_BATCH_ORDER_LONGEST_FIRST) {
+                const BatchPairArgs& a = pairs[i];
+                const int s = kPassDxHost[p] * kPassDyHost[p];
+                const int nlines = a.W + a.H - 1, kmin = s > 0 ? -(a.H - 1) : 0, G = hp[i].G;
+                std::vector<int> rows(blks.size());
+                for (size_t j = 0; j < blks.size(); j++)
+                    rows[j] = group_rows(a.W, a.H, s, kmin + (int)j * G, std::min(G, nlines - (int)j * G));
+                std::stable_sort(blks.begin(), blks.end(), [&](int x, int y) { return rows[x] > rows[y]; });
+            }
+            for (int b : blks) items.push_back(BItem{i * 16 + p, b});
+        }
     }
 
     out.n_pairs = n;

@@ -1,6 +1,9 @@
 // Per-frame launches of the fused integer-domain path: one kernel per pass
 // (prep, V+, V-, D1+, D1-, D2+, D2-, H+, H- with WTA), each a thin wrapper
 // around the device bodies in fused_body.cuh.
+#include <algorithm>
+#include <vector>
+
 #include "fused_body.cuh"
 
 namespace tdv {
@@ -12,11 +15,26 @@ __global__ void prep_kernel(ImgArg L, ImgArg R, Plane* LP, Plane* RPp, int W, in
     if (x < W) prep_pixel(L, R, LP, RPp, W, Wp, x, blockIdx.y);
 }
 
-template <int PPL, int MODE>
+// Diagonal passes: a line group's row count ramps from 1 to H across the
+// image corners, so groups are paired (a short one after a long one) into
+// blocks of about H rows each; the table travels as a kernel parameter.
+constexpr int kMaxPairedBlocks = 256;
+struct GroupPairs {
+    int16_t first[kMaxPairedBlocks];
+    int16_t second[kMaxPairedBlocks];  // -1: none
+};
+
+template <int PPL, int MODE, bool DIAG>
 __global__ void __launch_bounds__((kMaxG + 1) * 32, 1)
-    vd_pass(FK k, int s, int dy, int kmin, int nlines, int G) {
+    vd_pass(FK k, int s, int dy, int kmin, int nlines, int G, GroupPairs gp, int paired) {
     extern __shared__ __align__(128) unsigned char smem[];
-    vd_body<PPL, MODE>(k, s, dy, kmin, nlines, G, blockIdx.x, smem);
+    if (!paired) {
+        vd_body<PPL, MODE, DIAG>(k, s, dy, kmin, nlines, G, blockIdx.x, smem);
+        return;
+    }
+    vd_body<PPL, MODE, DIAG>(k, s, dy, kmin, nlines, G, gp.first[blockIdx.x], smem);
+    const int j2 = gp.second[blockIdx.x];
+    if (j2 >= 0) vd_body<PPL, MODE, DIAG>(k, s, dy, kmin, nlines, G, j2, smem);
 }
 
 template <int PPL, int MODE>
@@ -26,27 +44,80 @@ __global__ void __launch_bounds__((kMaxG + 1) * 32, 1) hp_pass(FK k, int dx, int
 }
 
 // ------------------------------------------------------------- host side
-template <int PPL, int MODE>
+int sm_count() {
+    static int cache[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cache[dev]) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
+        cache[dev] = n;
+    }
+    return cache[dev];
+}
+
+// Greedy pairing: groups by decreasing row count, each block takes the
+// longest left and, if it fits under the longest, the shortest left.
+// Returns the block count, or -1 if the table would overflow.
+int pair_groups(int W, int H, int s, int kmin, int nlines, int G, GroupPairs& gp) {
+    const int ng = (nlines + G - 1) / G;
+    if (ng > 2 * kMaxPairedBlocks) return -1;
+    std::vector<int> rows(ng), order(ng);
+    for (int j = 0; j < ng; j++) {
+        rows[j] = group_rows(W, H, s, kmin + j * G, std::min(G, nlines - j * G));
+        order[j] = j;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rows[a] > rows[b]; });
+    const int cap = rows[order[0]];
+    int lo = 0, hi = ng - 1, nb = 0;
+    while (lo <= hi) {
+        if (nb >= kMaxPairedBlocks) return -1;
+        const int j = order[lo++];
+        gp.first[nb] = (int16_t)j;
+        gp.second[nb] = -1;
+        if (lo <= hi && rows[j] + rows[order[hi]] <= cap) gp.second[nb] = (int16_t)order[hi--];
+        nb++;
+    }
+    return nb;
+}
+
+template <int PPL, int MODE, bool DIAG>
 cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
     const int s = dx * dy;
     const int nlines = s == 0 ? k.W : k.W + k.H - 1;
     const int kmin = s > 0 ? -(k.H - 1) : 0;
-    int G = (nlines + 147) / 148;
+    const int nsm = sm_count();
+    GroupPairs gp;
+    int paired = 0, blocks = 0;
+    int G = (k.W + nsm - 1) / nsm;
     G = G < 1 ? 1 : (G > kMaxG ? kMaxG : G);
+    if (DIAG) {
+        // smallest G whose paired blocks fit one wave
+        for (; G <= kMaxG; G++) {
+            blocks = pair_groups(k.W, k.H, s, kmin, nlines, G, gp);
+            if (blocks > 0 && blocks <= nsm) break;
+        }
+        if (G > kMaxG) {
+            G = kMaxG;
+            blocks = pair_groups(k.W, k.H, s, kmin, nlines, G, gp);
+        }
+        paired = blocks > 0;
+    }
+    if (!paired) blocks = (nlines + G - 1) / G;
     const int smem = vd_smem_bytes(G, PPL);
     if (smem > kSmemBudget) return cudaErrorInvalidConfiguration;
     cudaError_t e =
-        cudaFuncSetAttribute(vd_pass<PPL, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(vd_pass<PPL, MODE, DIAG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    const int blocks = (nlines + G - 1) / G;
-    vd_pass<PPL, MODE><<<blocks, (G + 1) * 32, smem, st>>>(k, s, dy, kmin, nlines, G);
+    vd_pass<PPL, MODE, DIAG><<<blocks, (G + 1) * 32, smem, st>>>(k, s, dy, kmin, nlines, G, gp, paired);
     return cudaGetLastError();
 }
 
 template <int PPL, int MODE>
 cudaError_t launch_hp(const FK& k, int dx, cudaStream_t st) {
     const bool lr = MODE == 2 && k.lr_thr >= 0;
-    int R = (k.H + 147) / 148;  // rows per block: spread the rows over every SM
+    const int nsm = sm_count();
+    int R = (k.H + nsm - 1) / nsm;  // rows per block: spread the rows over every SM
     R = R < 1 ? 1 : (R > kMaxG ? kMaxG : R);
     while (R > 1 && hp_smem_bytes(R, PPL, lr, k.W) > kSmemBudget) R--;
     const int smem = hp_smem_bytes(R, PPL, lr, k.W);
@@ -70,18 +141,18 @@ cudaError_t run_fused(const FK& k, int paths, cudaStream_t st, Timer* tm) {
     auto mark = [&](const char* n) {
         if (tm) tm->mark(n);
     };
-    if ((e = launch_vd<PPL, 0>(k, 0, 1, st)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 0, false>(k, 0, 1, st)) != cudaSuccess) return e;
     mark("fused_pass_V+");
-    if ((e = launch_vd<PPL, 1>(k, 0, -1, st)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 1, false>(k, 0, -1, st)) != cudaSuccess) return e;
     mark("fused_pass_V-");
     if (paths == 8) {
-        if ((e = launch_vd<PPL, 1>(k, 1, 1, st)) != cudaSuccess) return e;
+        if ((e = launch_vd<PPL, 1, true>(k, 1, 1, st)) != cudaSuccess) return e;
         mark("fused_pass_D1+");
-        if ((e = launch_vd<PPL, 1>(k, -1, -1, st)) != cudaSuccess) return e;
+        if ((e = launch_vd<PPL, 1, true>(k, -1, -1, st)) != cudaSuccess) return e;
         mark("fused_pass_D1-");
-        if ((e = launch_vd<PPL, 1>(k, -1, 1, st)) != cudaSuccess) return e;
+        if ((e = launch_vd<PPL, 1, true>(k, -1, 1, st)) != cudaSuccess) return e;
         mark("fused_pass_D2+");
-        if ((e = launch_vd<PPL, 1>(k, 1, -1, st)) != cudaSuccess) return e;
+        if ((e = launch_vd<PPL, 1, true>(k, 1, -1, st)) != cudaSuccess) return e;
         mark("fused_pass_D2-");
     }
     if ((e = launch_hpass<PPL>(k, 1, 1, st)) != cudaSuccess) return e;
