@@ -151,6 +151,37 @@ void release_buf(tdv_ctx* ctx, tdv_ctx::Buf& b) {
 
 cudaStream_t S(tdv_stream s) { return (cudaStream_t)s; }
 
+// Scratch of the fused path for pairs up to W x H x D: planes and both
+// aggregation volumes.
+tdv_status reserve_fused(tdv_ctx* ctx, int W, int H, int D) {
+    TDV_TRY(ensure(ctx, ctx->planes, tdv::fused_plane_bytes(W, H)));
+    if (D <= tdv::kMaxDispSgm) {
+        TDV_TRY(ensure(ctx, ctx->agg, tdv::fused_agg_bytes(W, H, D)));
+        TDV_TRY(ensure(ctx, ctx->agg2, tdv::fused_agg_bytes(W, H, D)));
+    }
+    TDV_TRY(ensure(ctx, ctx->misc, (size_t)W * H * sizeof(uint16_t)));
+    return TDV_OK;
+}
+
+// The side stream and fork/join events of the fused path's second chain.
+tdv_status ensure_side(tdv_ctx* ctx) {
+    if (ctx->side) return TDV_OK;
+    cudaStream_t s = nullptr;
+    cudaEvent_t f = nullptr, j = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&j, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        if (s) cudaStreamDestroy(s);
+        if (f) cudaEventDestroy(f);
+        return fail(ctx, TDV_ERR_CUDA, "creating the side stream failed: %s", cudaGetErrorString(e));
+    }
+    ctx->side = s;
+    ctx->fork_ev = f;
+    ctx->join_ev = j;
+    return TDV_OK;
+}
+
 // The device error word is allocated (and zeroed) once per context.
 tdv_status ensure_err(tdv_ctx* ctx, cudaStream_t st) {
     if (ctx->err.ptr) return TDV_OK;
@@ -381,11 +412,16 @@ tdv_status tdv_ctx_create(int32_t device, tdv_ctx** out) {
 void tdv_ctx_destroy(tdv_ctx* ctx) {
     if (!ctx) return;
     const bool any = ctx->agg.ptr || ctx->cost.ptr || ctx->planes.ptr || ctx->codes.ptr ||
-                     ctx->misc.ptr || ctx->sched_buf.ptr || ctx->err.ptr || ctx->soft.ptr;
+                     ctx->misc.ptr || ctx->sched_buf.ptr || ctx->err.ptr || ctx->soft.ptr ||
+                     ctx->agg2.ptr || ctx->side;
     if (any) {
         DeviceScope ds(ctx->device);
         cudaDeviceSynchronize();
         release_buf(ctx, ctx->agg);
+        release_buf(ctx, ctx->agg2);
+        if (ctx->side) cudaStreamDestroy(ctx->side);
+        if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+        if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
         release_buf(ctx, ctx->cost);
         release_buf(ctx, ctx->planes);
         release_buf(ctx, ctx->codes);
@@ -420,15 +456,9 @@ tdv_status tdv_ctx_reserve(tdv_ctx* ctx, int32_t W, int32_t H, int32_t D) {
         return fail(ctx, TDV_ERR_INVALID_ARG, "bad reserve size %dx%dx%d", W, H, D);
     if (!ctx->alloc) {
         TDV_DEVICE_SCOPE(ctx);
-        TDV_TRY(ensure(ctx, ctx->planes, tdv::fused_plane_bytes(W, H)));
-        if (D <= tdv::kMaxDispSgm) TDV_TRY(ensure(ctx, ctx->agg, tdv::fused_agg_bytes(W, H, D)));
-        TDV_TRY(ensure(ctx, ctx->misc, (size_t)W * H * sizeof(uint16_t)));
-        return TDV_OK;
+        return reserve_fused(ctx, W, H, D);
     }
-    TDV_TRY(ensure(ctx, ctx->planes, tdv::fused_plane_bytes(W, H)));
-    if (D <= tdv::kMaxDispSgm) TDV_TRY(ensure(ctx, ctx->agg, tdv::fused_agg_bytes(W, H, D)));
-    TDV_TRY(ensure(ctx, ctx->misc, (size_t)W * H * sizeof(uint16_t)));
-    return TDV_OK;
+    return reserve_fused(ctx, W, H, D);
 }
 
 tdv_status tdv_ctx_enable_timing(tdv_ctx* ctx, int32_t enable) {
@@ -436,17 +466,20 @@ tdv_status tdv_ctx_enable_timing(tdv_ctx* ctx, int32_t enable) {
     ctx->timer.on = enable != 0;
     ctx->timer.n = 0;
     ctx->timer.names.clear();
+    ctx->timer.spans.clear();
     return TDV_OK;
 }
 
 int32_t tdv_ctx_timings(tdv_ctx* ctx, float* ms, int32_t max_entries) {
-    if (!ctx || !ctx->timer.on || ctx->timer.n < 2) return 0;
+    if (!ctx || !ctx->timer.on || ctx->timer.spans.empty()) return 0;
     tdv::Timer& t = ctx->timer;
     DeviceScope ds(ctx->device);
-    if (cudaEventSynchronize(t.ev[t.n - 1]) != cudaSuccess) return 0;
-    const int n = t.n - 1;
+    for (int i = 0; i < t.n; i++)
+        if (cudaEventSynchronize(t.ev[i]) != cudaSuccess) return 0;
+    const int n = (int)t.spans.size();
     for (int i = 0; i < n && i < max_entries && ms; i++)
-        if (cudaEventElapsedTime(&ms[i], t.ev[i], t.ev[i + 1]) != cudaSuccess) ms[i] = -1.0f;
+        if (cudaEventElapsedTime(&ms[i], t.ev[t.spans[i].first], t.ev[t.spans[i].second]) != cudaSuccess)
+            ms[i] = -1.0f;
     return n;
 }
 
@@ -707,8 +740,8 @@ tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* 
                        2.0f * params->p2 <= 2560.0f && W >= 1 && H >= 1;
     TDV_DEVICE_SCOPE(ctx);
     if (fused) {
-        TDV_TRY(ensure(ctx, ctx->planes, tdv::fused_plane_bytes(W, H)));
-        TDV_TRY(ensure(ctx, ctx->agg, tdv::fused_agg_bytes(W, H, D)));
+        TDV_TRY(reserve_fused(ctx, W, H, D));
+        TDV_TRY(ensure_side(ctx));
         tdv::FusedArgs a;
         a.L = tdv::make_img(*left);
         a.R = tdv::make_img(*right);
@@ -726,6 +759,10 @@ tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* 
         a.agg = ctx->agg.ptr;
         TDV_TRY(ensure_err(ctx, S(stream)));
         a.err = (int*)ctx->err.ptr;
+        a.agg2 = ctx->agg2.ptr;
+        a.side = ctx->side;
+        a.fork = ctx->fork_ev;
+        a.join = ctx->join_ev;
         TDV_CUDA(tdv::launch_fused(a, S(stream), &ctx->timer));
         return TDV_OK;
     }

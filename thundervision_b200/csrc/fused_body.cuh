@@ -234,6 +234,7 @@ struct FK {
     const Plane* LP;
     const Plane* RPp;  // padded rows of Wp entries
     uint32_t* S;       // aggregation volume, u16 pairs
+    const uint32_t* S2;  // second volume summed by a two-volume last pass (else null)
     int W, H, D, Dp2, Wp;
     uint32_t P1P1, P2P2, BIGBIG;
     uint16_t* disp;
@@ -760,28 +761,31 @@ __device__ __forceinline__ void h_body(const FK& k, int dx, int GH, int warp_byt
 // issue and gives up (TDV_ERR_TIMEOUT) after kWaitNs without progress.
 // The recurrence starts from L = 0, m = 0, which makes the first step L = C
 // without a branch (min(0, 0 + P1, 0 + P2) = 0).
+// TWO: the pass joins two volumes filled by concurrent pass chains, k.S and
+// k.S2 (read-only): a slot also holds the S2 vectors, and the pass stores
+// S + S2 + L into k.S.
 constexpr int kHpU = 4;      // pixels per S slot
 constexpr int kHpSlots = 4;  // S slots per row
 constexpr int kHpBars = 2 * kHpSlots + 2 * kChunkSlots;
 
-__host__ __device__ inline int hp_slot_bytes(int ppl) { return kHpU * (128 * ppl + 16); }
-__host__ __device__ inline int hp_warp_bytes(int ppl, bool lr, int W) {
-    return align128(kHpSlots * hp_slot_bytes(ppl) + kChunkSlots * kChunkBytes + (lr ? 2 * W * 2 : 0));
+__host__ __device__ inline int hp_slot_bytes(int ppl, bool two) { return kHpU * (128 * ppl * (two ? 2 : 1) + 16); }
+__host__ __device__ inline int hp_warp_bytes(int ppl, bool lr, int W, bool two) {
+    return align128(kHpSlots * hp_slot_bytes(ppl, two) + kChunkSlots * kChunkBytes + (lr ? 2 * W * 2 : 0));
 }
-__host__ __device__ inline int hp_smem_bytes(int R, int ppl, bool lr, int W) {
-    return align128(R * kHpBars * 8) + R * hp_warp_bytes(ppl, lr, W);
+__host__ __device__ inline int hp_smem_bytes(int R, int ppl, bool lr, int W, bool two) {
+    return align128(R * kHpBars * 8) + R * hp_warp_bytes(ppl, lr, W, two);
 }
 
-template <int PPL, int MODE>
+template <int PPL, int MODE, bool TWO>
 __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, unsigned char* smem) {
     constexpr int SB = 128 * PPL;
     constexpr int DSPAN = 64 * PPL;
     constexpr int NJ = 2 * PPL;
-    constexpr int SLOT = kHpU * (SB + 16);
+    constexpr int SLOT = kHpU * ((TWO ? 2 : 1) * SB + 16);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int W = k.W;
     const bool lr = MODE == 2 && k.lr_thr >= 0;
-    const int wb = hp_warp_bytes(PPL, lr, W);
+    const int wb = hp_warp_bytes(PPL, lr, W, TWO);
     uint64_t* bars = (uint64_t*)smem;
     unsigned char* data = smem + align128(R * kHpBars * 8);
     const int y0 = blk * R;
@@ -822,9 +826,12 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                         const int xlo = group_lo(g), n = group_hi(g) - xlo + 1;
                         unsigned char* dst = wbase + s * SLOT;
                         const uint32_t bar = fullS(lane, s);
-                        mbar_expect_tx(bar, (uint32_t)n * (SB + 16));
+                        mbar_expect_tx(bar, (uint32_t)n * ((TWO ? 2 : 1) * SB + 16));
                         tma_load(smem_u32(dst), k.S + ((size_t)y * W + xlo) * k.Dp2, (uint32_t)n * SB, bar);
                         tma_load(smem_u32(dst + kHpU * SB), k.LP + (size_t)y * W + xlo, (uint32_t)n * 16, bar);
+                        if (TWO)
+                            tma_load(smem_u32(dst + kHpU * (SB + 16)), k.S2 + ((size_t)y * W + xlo) * k.Dp2,
+                                     (uint32_t)n * SB, bar);
                         g++;
                         did = true;
                     }
@@ -906,6 +913,12 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
             Vec<PPL>::lds((const uint32_t*)(slot + (x - xlo) * SB) + lane * PPL, sv);
 #pragma unroll
             for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
+            if (TWO) {
+                uint32_t s2[PPL];
+                Vec<PPL>::lds((const uint32_t*)(slot + kHpU * (SB + 16) + (x - xlo) * SB) + lane * PPL, s2);
+#pragma unroll
+                for (int q = 0; q < PPL; q++) sv[q] += s2[q];
+            }
             if (MODE == 1) {
                 Vec<PPL>::st(sg, sv);
             } else {

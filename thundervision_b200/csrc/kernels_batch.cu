@@ -99,9 +99,9 @@ __device__ __forceinline__ void run_h(const BPair& P, int dx, int blk, unsigned 
         if (P.ppl == 2) h2_body<1, MODE>(k, dx, P.hrows, P.hwb, P.hrb, blk, smem, false);
         else h2_body<2, MODE>(k, dx, P.hrows, P.hwb, P.hrb, blk, smem, false);
     } else {
-        if (P.ppl == 1) hp_body<1, MODE>(k, dx, P.hrows, blk, smem);
-        else if (P.ppl == 2) hp_body<2, MODE>(k, dx, P.hrows, blk, smem);
-        else hp_body<4, MODE>(k, dx, P.hrows, blk, smem);
+        if (P.ppl == 1) hp_body<1, MODE, false>(k, dx, P.hrows, blk, smem);
+        else if (P.ppl == 2) hp_body<2, MODE, false>(k, dx, P.hrows, blk, smem);
+        else hp_body<4, MODE, false>(k, dx, P.hrows, blk, smem);
     }
 }
 
@@ -237,6 +237,7 @@ const char* batch_plan(const std::vector<BatchPairArgs>& pairs, int p1h, int p2h
         k.disp_right = a.disp_right;
         k.lr_thr = a.lr_thr;
         k.err = (int*)(d_desc + out.ctl_off) + 1;
+        k.S2 = nullptr;
         P.L = a.L;
         P.R = a.R;
 
@@ -261,10 +262,10 @@ const char* batch_plan(const std::vector<BatchPairArgs>& pairs, int p1h, int p2h
         } else {
             // producer-fed rows: one consumer warp per row plus the producer warp
             rows = std::min(rows, kBatchWarps - 1);
-            while (rows > 1 && hp_smem_bytes(rows, P.ppl, lr, a.W) > kSmemBudget) rows--;
-            if (hp_smem_bytes(rows, P.ppl, lr, a.W) > kSmemBudget)
+            while (rows > 1 && hp_smem_bytes(rows, P.ppl, lr, a.W, false) > kSmemBudget) rows--;
+            if (hp_smem_bytes(rows, P.ppl, lr, a.W, false) > kSmemBudget)
                 return "horizontal pass tile does not fit in shared memory";
-            smem = std::max(smem, hp_smem_bytes(rows, P.ppl, lr, a.W));
+            smem = std::max(smem, hp_smem_bytes(rows, P.ppl, lr, a.W, false));
         }
         P.hrows = rows;
         P.prep_rows = std::max(1, kPrepPixels / a.W);

@@ -37,10 +37,10 @@ __global__ void __launch_bounds__((kMaxG + 1) * 32, 1)
     if (j2 >= 0) vd_body<PPL, MODE, DIAG>(k, s, dy, kmin, nlines, G, j2, smem);
 }
 
-template <int PPL, int MODE>
+template <int PPL, int MODE, bool TWO>
 __global__ void __launch_bounds__((kMaxG + 1) * 32, 1) hp_pass(FK k, int dx, int R) {
     extern __shared__ __align__(128) unsigned char smem[];
-    hp_body<PPL, MODE>(k, dx, R, blockIdx.x, smem);
+    hp_body<PPL, MODE, TWO>(k, dx, R, blockIdx.x, smem);
 }
 
 // ------------------------------------------------------------- host side
@@ -113,52 +113,82 @@ cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-template <int PPL, int MODE>
-cudaError_t launch_hp(const FK& k, int dx, cudaStream_t st) {
+// rows per block: spread the rows over every SM, at most max_rows (a pass
+// that shares the SMs with a concurrent chain keeps its blocks small)
+template <int PPL, int MODE, bool TWO>
+cudaError_t launch_hp(const FK& k, int dx, int max_rows, cudaStream_t st) {
     const bool lr = MODE == 2 && k.lr_thr >= 0;
     const int nsm = sm_count();
-    int R = (k.H + nsm - 1) / nsm;  // rows per block: spread the rows over every SM
-    R = R < 1 ? 1 : (R > kMaxG ? kMaxG : R);
-    while (R > 1 && hp_smem_bytes(R, PPL, lr, k.W) > kSmemBudget) R--;
-    const int smem = hp_smem_bytes(R, PPL, lr, k.W);
+    int R = (k.H + nsm - 1) / nsm;
+    R = R < 1 ? 1 : (R > max_rows ? max_rows : R);
+    while (R > 1 && hp_smem_bytes(R, PPL, lr, k.W, TWO) > kSmemBudget) R--;
+    const int smem = hp_smem_bytes(R, PPL, lr, k.W, TWO);
     if (smem > kSmemBudget) return cudaErrorInvalidConfiguration;
-    cudaError_t e = cudaFuncSetAttribute(hp_pass<PPL, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(hp_pass<PPL, MODE, TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     const int blocks = (k.H + R - 1) / R;
-    hp_pass<PPL, MODE><<<blocks, (R + 1) * 32, smem, st>>>(k, dx, R);
+    hp_pass<PPL, MODE, TWO><<<blocks, (R + 1) * 32, smem, st>>>(k, dx, R);
     return cudaGetLastError();
 }
 
-// One consumer warp per row plus a producer warp per block.
 template <int PPL>
-cudaError_t launch_hpass(const FK& k, int dx, int mode, cudaStream_t st) {
-    return mode == 1 ? launch_hp<PPL, 1>(k, dx, st) : launch_hp<PPL, 2>(k, dx, st);
-}
-
-template <int PPL>
-cudaError_t run_fused(const FK& k, int paths, cudaStream_t st, Timer* tm) {
+cudaError_t run_fused(const FK& k, const FusedArgs& a, cudaStream_t st, Timer* tm) {
     cudaError_t e;
-    auto mark = [&](const char* n) {
-        if (tm) tm->mark(n);
+    auto mark = [&](const char* n, cudaStream_t s) {
+        if (tm) tm->mark_on(n, s);
     };
-    if ((e = launch_vd<PPL, 0, false>(k, 0, 1, st)) != cudaSuccess) return e;
-    mark("fused_pass_V+");
-    if ((e = launch_vd<PPL, 1, false>(k, 0, -1, st)) != cudaSuccess) return e;
-    mark("fused_pass_V-");
-    if (paths == 8) {
-        if ((e = launch_vd<PPL, 1, true>(k, 1, 1, st)) != cudaSuccess) return e;
-        mark("fused_pass_D1+");
-        if ((e = launch_vd<PPL, 1, true>(k, -1, -1, st)) != cudaSuccess) return e;
-        mark("fused_pass_D1-");
-        if ((e = launch_vd<PPL, 1, true>(k, -1, 1, st)) != cudaSuccess) return e;
-        mark("fused_pass_D2+");
-        if ((e = launch_vd<PPL, 1, true>(k, 1, -1, st)) != cudaSuccess) return e;
-        mark("fused_pass_D2-");
+    const bool chains = a.paths == 8 && a.agg2 && a.side && a.fork && a.join;
+    if (!chains) {
+        if ((e = launch_vd<PPL, 0, false>(k, 0, 1, st)) != cudaSuccess) return e;
+        mark("fused_pass_V+", st);
+        if ((e = launch_vd<PPL, 1, false>(k, 0, -1, st)) != cudaSuccess) return e;
+        mark("fused_pass_V-", st);
+        if (a.paths == 8) {
+            if ((e = launch_vd<PPL, 1, true>(k, 1, 1, st)) != cudaSuccess) return e;
+            mark("fused_pass_D1+", st);
+            if ((e = launch_vd<PPL, 1, true>(k, -1, -1, st)) != cudaSuccess) return e;
+            mark("fused_pass_D1-", st);
+            if ((e = launch_vd<PPL, 1, true>(k, -1, 1, st)) != cudaSuccess) return e;
+            mark("fused_pass_D2+", st);
+            if ((e = launch_vd<PPL, 1, true>(k, 1, -1, st)) != cudaSuccess) return e;
+            mark("fused_pass_D2-", st);
+        }
+        if ((e = launch_hp<PPL, 1, false>(k, 1, kMaxG, st)) != cudaSuccess) return e;
+        mark("fused_pass_H+", st);
+        if ((e = launch_hp<PPL, 2, false>(k, -1, kMaxG, st)) != cudaSuccess) return e;
+        mark("fused_pass_H-_wta", st);
+        return cudaSuccess;
     }
-    if ((e = launch_hpass<PPL>(k, 1, 1, st)) != cudaSuccess) return e;
-    mark("fused_pass_H+");
-    if ((e = launch_hpass<PPL>(k, -1, 2, st)) != cudaSuccess) return e;
-    mark("fused_pass_H-_wta");
+    // two chains: V+ V- D1+ into S on the call's stream, D1- D2+ D2- into S2
+    // on the side stream (V+ and D1- store their volume, the first touch);
+    // then H+ joins them (S += S2 + L) and H- finishes S
+    FK kb = k;
+    kb.S = (uint32_t*)a.agg2;
+    if ((e = cudaEventRecord(a.fork, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(a.side, a.fork, 0)) != cudaSuccess) return e;
+    if (tm) tm->fork(a.side);
+    if ((e = launch_vd<PPL, 0, true>(kb, -1, -1, a.side)) != cudaSuccess) return e;
+    mark("fused_pass_D1-", a.side);
+    if ((e = launch_vd<PPL, 0, false>(k, 0, 1, st)) != cudaSuccess) return e;
+    mark("fused_pass_V+", st);
+    if ((e = launch_vd<PPL, 1, true>(kb, -1, 1, a.side)) != cudaSuccess) return e;
+    mark("fused_pass_D2+", a.side);
+    if ((e = launch_vd<PPL, 1, false>(k, 0, -1, st)) != cudaSuccess) return e;
+    mark("fused_pass_V-", st);
+    if ((e = launch_vd<PPL, 1, true>(kb, 1, -1, a.side)) != cudaSuccess) return e;
+    mark("fused_pass_D2-", a.side);
+    if ((e = launch_vd<PPL, 1, true>(k, 1, 1, st)) != cudaSuccess) return e;
+    mark("fused_pass_D1+", st);
+    if ((e = cudaEventRecord(a.join, a.side)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(st, a.join, 0)) != cudaSuccess) return e;
+    if (tm) tm->join();
+    FK kj = k;
+    kj.S2 = (const uint32_t*)a.agg2;
+    if ((e = launch_hp<PPL, 1, true>(kj, 1, kMaxG, st)) != cudaSuccess) return e;
+    mark("fused_pass_H+", st);
+    if ((e = launch_hp<PPL, 2, false>(k, -1, kMaxG, st)) != cudaSuccess) return e;
+    mark("fused_pass_H-_wta", st);
     return cudaSuccess;
 }
 
@@ -200,9 +230,10 @@ cudaError_t launch_fused(const FusedArgs& a, cudaStream_t st, Timer* tm) {
     k.disp_right = a.disp_right;
     k.lr_thr = a.lr_thr;
     k.err = a.err;
-    if (ppl == 1) return run_fused<1>(k, a.paths, st, tm);
-    if (ppl == 2) return run_fused<2>(k, a.paths, st, tm);
-    return run_fused<4>(k, a.paths, st, tm);
+    k.S2 = nullptr;
+    if (ppl == 1) return run_fused<1>(k, a, st, tm);
+    if (ppl == 2) return run_fused<2>(k, a, st, tm);
+    return run_fused<4>(k, a, st, tm);
 }
 
 }  // namespace tdv

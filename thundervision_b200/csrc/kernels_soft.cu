@@ -273,6 +273,7 @@ __global__ void __launch_bounds__(128) soft_bwd_pass(SoftK<T> k, int dx, int dy,
     constexpr int WARPS = 4;
     constexpr int KMAX = 32;
     __shared__ uint16_t sk[WARPS][KMAX + 1];
+    __shared__ uint32_t segc[WARPS][KMAX][32];  // CK: codes of the segment's steps, per lane
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
     if (w >= nwalks) return;
@@ -291,7 +292,6 @@ __global__ void __launch_bounds__(128) soft_bwd_pass(SoftK<T> k, int dx, int dy,
 #pragma unroll
     for (int j = 0; j < NPL; j++) carry[j] = 0;
     T gp1 = 0, gp2 = 0;
-    uint32_t segc[KMAX];  // CK: codes of the segment's steps (this lane)
 
     int seg_lo = 0;  // CK: steps (seg_lo, seg_hi] have codes in segc / sk
     int t = len - 1;
@@ -332,22 +332,14 @@ __global__ void __launch_bounds__(128) soft_bwd_pass(SoftK<T> k, int dx, int dy,
                     soft_step<T, NPL>(L, m, c, k.p1, k.p2, lane, d0, D, Ln, cwu);
 #pragma unroll
                     for (int j = 0; j < NPL; j++) L[j] = Ln[j];
-                    // segc is indexed by a runtime step: keep it in a fully
-                    // unrolled select so it stays in registers
-#pragma unroll
-                    for (int q = 0; q < KMAX; q++)
-                        if (q == u - s0 - 1) segc[q] = cwu;
+                    segc[warp][u - s0 - 1][lane] = cwu;
                     warp_argmin<T, NPL>(L, d0, m, kk);
                     if (lane == 0 && u - s0 < KMAX + 1) sk[warp][u - s0] = (uint16_t)kk;
                 }
                 __syncwarp();
                 seg_lo = s0;
             }
-            const int q = t - seg_lo - 1;
-            cw = 0;
-#pragma unroll
-            for (int r = 0; r < KMAX; r++)
-                if (r == q) cw = segc[r];
+            cw = segc[warp][t - seg_lo - 1][lane];
             ks = sk[warp][t - 1 - seg_lo];
         } else {
             cw = load_codes<T, NPL>(codes + (p * 32 + lane) * CB);
@@ -376,7 +368,7 @@ __global__ void __launch_bounds__(128) soft_bwd_pass(SoftK<T> k, int dx, int dy,
             if (cj == 1u || cj == 2u) gp1 += G[j];
         }
         gp2 += g3;
-        const T gm = warp_sum(g3) - warp_sum(gs);
+        const T gm = warp_sum(g3 - gs);
 #pragma unroll
         for (int j = 0; j < NPL; j++) {
             const uint32_t cj = (cw >> (2 * j)) & 3u;

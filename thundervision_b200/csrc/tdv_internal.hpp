@@ -39,33 +39,56 @@ struct PassSchedule {
     Walk* d_walks = nullptr;  // device copy (ctx scratch)
 };
 
-// Optional per-kernel timing: events recorded on the launch stream before the
-// first and after every kernel of one ABI call.
+// Optional per-kernel timing.  Every kernel of one ABI call is bracketed by
+// CUDA events on the stream it runs on: an entry spans from the previous
+// event recorded on that stream (the call's start, a fork, or the previous
+// kernel there) to the event recorded after the kernel.
 struct Timer {
     bool on = false;
     std::vector<cudaEvent_t> ev;
     std::vector<std::string> names;
+    std::vector<std::pair<int, int>> spans;  // (start event, end event) per entry
     int n = 0;
-    cudaStream_t st = nullptr;
+    cudaStream_t st = nullptr, side = nullptr;
+    int last_main = -1, last_side = -1;
     void begin(cudaStream_t s) {
         if (!on) return;
         n = 0;
         names.clear();
+        spans.clear();
         st = s;
-        rec();
+        side = nullptr;
+        last_main = rec(s);
     }
-    void mark(const char* name) {
+    void mark(const char* name) { mark_on(name, st); }
+    void mark_on(const char* name, cudaStream_t s) {
         if (!on) return;
+        int& last = (s == st || s != side) ? last_main : last_side;
+        const int e = rec(s);
+        if (e < 0) return;
         names.emplace_back(name);
-        rec();
+        spans.emplace_back(last, e);
+        last = e;
     }
-    void rec() {
+    // a second stream joined the call (after it waited on a fork event)
+    void fork(cudaStream_t s) {
+        if (!on) return;
+        side = s;
+        last_side = rec(s);
+    }
+    // the call's stream waited on the second stream's join event
+    void join() {
+        if (!on) return;
+        last_main = rec(st);
+    }
+    int rec(cudaStream_t s) {
         if (n >= (int)ev.size()) {
             cudaEvent_t e;
-            if (cudaEventCreate(&e) != cudaSuccess) return;
+            if (cudaEventCreate(&e) != cudaSuccess) return -1;
             ev.push_back(e);
         }
-        cudaEventRecord(ev[n++], st);
+        cudaEventRecord(ev[n], s);
+        return n++;
     }
 };
 
@@ -90,6 +113,7 @@ struct tdv_ctx {
         size_t bytes = 0;
     };
     Buf agg;      // aggregation volume
+    Buf agg2;     // fused path: second aggregation volume (concurrent pass chains)
     Buf cost;     // cost DSI for tdv_stereo_sgm's general path
     Buf planes;   // fused path: left/right BT planes
     Buf codes;    // DP choice codes
@@ -101,6 +125,9 @@ struct tdv_ctx {
     tdv::PassSchedule sched;
     Buf sched_buf;
     tdv::Timer timer;
+    // fused path: side stream and fork/join events of the two pass chains
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 };
 
 namespace tdv {
@@ -155,6 +182,13 @@ struct FusedArgs {
     void* planes;  // fused_plane_bytes(W, H)
     void* agg;     // fused_agg_bytes(W, H, D)
     int* err;      // device word: kernels record TDV_ERR_TIMEOUT here
+    // Optional second aggregation volume and stream: with both (8 paths),
+    // the passes run as two concurrent chains, V+ V- D1+ into `agg` on the
+    // call's stream and D1- D2+ D2- into `agg2` on `side`; H+ joins them
+    // (agg += agg2 + its L) and H- finishes agg.
+    void* agg2 = nullptr;
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 size_t fused_agg_bytes(int W, int H, int D);
 size_t fused_plane_bytes(int W, int H);
