@@ -273,7 +273,10 @@ tdv_status tdv_ctx_device_status(tdv_ctx* ctx, tdv_stream stream);
  * stream has been synchronised) the device milliseconds of each launch of the
  * most recent call and tdv_ctx_timing_name its kernel name.  This replaces the
  * reference's CudaBenchmarker around each stage update
- * (tdvision/benchmark.cpp:7-31, matchingcost.cpp:35-42). */
+ * (tdvision/benchmark.cpp:7-31, matchingcost.cpp:35-42).  While timing is on,
+ * work a call would run concurrently on two streams (the fused 8-path pass
+ * chains) runs in sequence on the call's stream, so each kernel is timed
+ * alone. */
 tdv_status tdv_ctx_enable_timing(tdv_ctx* ctx, int32_t enable);
 int32_t tdv_ctx_timings(tdv_ctx* ctx, float* ms_out, int32_t max_entries);
 const char* tdv_ctx_timing_name(const tdv_ctx* ctx, int32_t index);

@@ -768,7 +768,11 @@ constexpr int kHpU = 4;      // pixels per S slot
 constexpr int kHpSlots = 4;  // S slots per row
 constexpr int kHpBars = 2 * kHpSlots + 2 * kChunkSlots;
 
-__host__ __device__ inline int hp_slot_bytes(int ppl, bool two) { return kHpU * (128 * ppl * (two ? 2 : 1) + 16); }
+// slot: [S vectors of kHpU pixels][S2 vectors (TWO)][left-plane entries],
+// padded to 128 bytes so every slot's vectors start on a 128-byte line
+__host__ __device__ inline int hp_slot_bytes(int ppl, bool two) {
+    return align128(kHpU * (128 * ppl * (two ? 2 : 1) + 16));
+}
 __host__ __device__ inline int hp_warp_bytes(int ppl, bool lr, int W, bool two) {
     return align128(kHpSlots * hp_slot_bytes(ppl, two) + kChunkSlots * kChunkBytes + (lr ? 2 * W * 2 : 0));
 }
@@ -781,7 +785,8 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
     constexpr int SB = 128 * PPL;
     constexpr int DSPAN = 64 * PPL;
     constexpr int NJ = 2 * PPL;
-    constexpr int SLOT = kHpU * ((TWO ? 2 : 1) * SB + 16);
+    constexpr int SLOT = (kHpU * ((TWO ? 2 : 1) * SB + 16) + 127) & ~127;
+    constexpr int LPOFF = kHpU * (TWO ? 2 : 1) * SB;  // left-plane entries in a slot
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int W = k.W;
     const bool lr = MODE == 2 && k.lr_thr >= 0;
@@ -828,10 +833,10 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                         const uint32_t bar = fullS(lane, s);
                         mbar_expect_tx(bar, (uint32_t)n * ((TWO ? 2 : 1) * SB + 16));
                         tma_load(smem_u32(dst), k.S + ((size_t)y * W + xlo) * k.Dp2, (uint32_t)n * SB, bar);
-                        tma_load(smem_u32(dst + kHpU * SB), k.LP + (size_t)y * W + xlo, (uint32_t)n * 16, bar);
                         if (TWO)
-                            tma_load(smem_u32(dst + kHpU * (SB + 16)), k.S2 + ((size_t)y * W + xlo) * k.Dp2,
+                            tma_load(smem_u32(dst + kHpU * SB), k.S2 + ((size_t)y * W + xlo) * k.Dp2,
                                      (uint32_t)n * SB, bar);
+                        tma_load(smem_u32(dst + LPOFF), k.LP + (size_t)y * W + xlo, (uint32_t)n * 16, bar);
                         g++;
                         did = true;
                     }
@@ -885,8 +890,12 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
         const bool edge_lane = base_d + 2 * PPL > k.D;
         uint32_t L[PPL], m = 0, sv[PPL];
         uint32_t P[NJ];
+        uint32_t dpair[PPL];  // (d, d+1) of each pair, u16 halves
 #pragma unroll
-        for (int q = 0; q < PPL; q++) L[q] = 0;
+        for (int q = 0; q < PPL; q++) {
+            L[q] = 0;
+            dpair[q] = (uint32_t)(base_d + 2 * q) | ((uint32_t)(base_d + 2 * q + 1) << 16);
+        }
 #pragma unroll
         for (int j = 0; j < NJ; j++) P[j] = FULL;
         uint32_t* sg = k.S + ((size_t)y * W + (dx > 0 ? 0 : W - 1)) * k.Dp2 + lane * PPL;
@@ -896,7 +905,7 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
         bool ok = true;
 
         auto step = [&](int x, const unsigned char* slot, int xlo) {
-            const uint4 lp = *(const uint4*)(slot + kHpU * SB + (x - xlo) * 16);
+            const uint4 lp = *(const uint4*)(slot + LPOFF + (x - xlo) * 16);
             uint32_t c[PPL], Ln[PPL];
             const int eb = x - base_d;
 #pragma unroll
@@ -915,19 +924,20 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
             for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
             if (TWO) {
                 uint32_t s2[PPL];
-                Vec<PPL>::lds((const uint32_t*)(slot + kHpU * (SB + 16) + (x - xlo) * SB) + lane * PPL, s2);
+                Vec<PPL>::lds((const uint32_t*)(slot + kHpU * SB + (x - xlo) * SB) + lane * PPL, s2);
 #pragma unroll
                 for (int q = 0; q < PPL; q++) sv[q] += s2[q];
             }
             if (MODE == 1) {
                 Vec<PPL>::st(sg, sv);
             } else {
-                // WTA key (S << 8 | d): lowest S, then lowest d (tdvision/wtacpu.cpp:26-30)
+                // WTA key (S << 8 | d): lowest S, then lowest d (tdvision/wtacpu.cpp:26-30);
+                // one byte permute per key from S and the lane's (d, d+1) register
                 uint32_t key[NJ];
 #pragma unroll
                 for (int q = 0; q < PPL; q++) {
-                    key[2 * q] = ((sv[q] & 0xFFFFu) << 8) | (uint32_t)(base_d + 2 * q);
-                    key[2 * q + 1] = ((sv[q] >> 16) << 8) | (uint32_t)(base_d + 2 * q + 1);
+                    key[2 * q] = __byte_perm(sv[q], dpair[q], 0x5104);
+                    key[2 * q + 1] = __byte_perm(sv[q], dpair[q], 0x7326);
                 }
                 uint32_t kmin = key[0];
 #pragma unroll

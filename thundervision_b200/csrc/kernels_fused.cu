@@ -163,26 +163,35 @@ cudaError_t run_fused(const FK& k, const FusedArgs& a, cudaStream_t st, Timer* t
     // two chains: V+ V- D1+ into S on the call's stream, D1- D2+ D2- into S2
     // on the side stream (V+ and D1- store their volume, the first touch);
     // then H+ joins them (S += S2 + L) and H- finishes S
+    // With per-kernel timing on, the chains run one after the other on the
+    // call's stream (same kernels, same volumes) so that each kernel's
+    // events time it alone.
+    const bool concurrent = !(tm && tm->on);
+    cudaStream_t sd = concurrent ? a.side : st;
     FK kb = k;
     kb.S = (uint32_t*)a.agg2;
-    if ((e = cudaEventRecord(a.fork, st)) != cudaSuccess) return e;
-    if ((e = cudaStreamWaitEvent(a.side, a.fork, 0)) != cudaSuccess) return e;
-    if (tm) tm->fork(a.side);
-    if ((e = launch_vd<PPL, 0, true>(kb, -1, -1, a.side)) != cudaSuccess) return e;
-    mark("fused_pass_D1-", a.side);
+    if (concurrent) {
+        if ((e = cudaEventRecord(a.fork, st)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(sd, a.fork, 0)) != cudaSuccess) return e;
+        if (tm) tm->fork(sd);
+    }
+    if ((e = launch_vd<PPL, 0, true>(kb, -1, -1, sd)) != cudaSuccess) return e;
+    mark("fused_pass_D1-", sd);
     if ((e = launch_vd<PPL, 0, false>(k, 0, 1, st)) != cudaSuccess) return e;
     mark("fused_pass_V+", st);
-    if ((e = launch_vd<PPL, 1, true>(kb, -1, 1, a.side)) != cudaSuccess) return e;
-    mark("fused_pass_D2+", a.side);
+    if ((e = launch_vd<PPL, 1, true>(kb, -1, 1, sd)) != cudaSuccess) return e;
+    mark("fused_pass_D2+", sd);
     if ((e = launch_vd<PPL, 1, false>(k, 0, -1, st)) != cudaSuccess) return e;
     mark("fused_pass_V-", st);
-    if ((e = launch_vd<PPL, 1, true>(kb, 1, -1, a.side)) != cudaSuccess) return e;
-    mark("fused_pass_D2-", a.side);
+    if ((e = launch_vd<PPL, 1, true>(kb, 1, -1, sd)) != cudaSuccess) return e;
+    mark("fused_pass_D2-", sd);
     if ((e = launch_vd<PPL, 1, true>(k, 1, 1, st)) != cudaSuccess) return e;
     mark("fused_pass_D1+", st);
-    if ((e = cudaEventRecord(a.join, a.side)) != cudaSuccess) return e;
-    if ((e = cudaStreamWaitEvent(st, a.join, 0)) != cudaSuccess) return e;
-    if (tm) tm->join();
+    if (concurrent) {
+        if ((e = cudaEventRecord(a.join, sd)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(st, a.join, 0)) != cudaSuccess) return e;
+        if (tm) tm->join();
+    }
     FK kj = k;
     kj.S2 = (const uint32_t*)a.agg2;
     if ((e = launch_hp<PPL, 1, true>(kj, 1, kMaxG, st)) != cudaSuccess) return e;
