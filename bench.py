@@ -62,45 +62,82 @@ def config(extra=None):
 
 # ------------------------------------------------------------------ clocks
 class Clocks:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clocks and clock-event (throttle) reasons of the benchmark's own GPU
+    (found by UUID), sampled on a thread through NVML every 20 ms while a
+    timed region runs; falls back to `nvidia-smi -lms 200` without NVML."""
 
-    def __init__(self, gpu_index):
-        self.idx = gpu_index
+    REASON_BITS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+                   0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, gpu_index, period=0.02):
+        import threading
+        self.rows, self.p, self.nv = [], None, None
+        self.stop_ev = threading.Event()
+        uuid = None
+        try:
+            import torch
+            uuid = "GPU-" + str(torch.cuda.get_device_properties(gpu_index).uuid)
+        except Exception:
+            pass
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid) if uuid else pynvml.nvmlDeviceGetHandleByIndex(gpu_index)
+            self.nv, self.h = pynvml, h
+            self.max_sm = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def run():
+                while not self.stop_ev.is_set():
+                    try:
+                        self.rows.append((pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM), reasons(h)))
+                    except Exception:
+                        pass
+                    self.stop_ev.wait(period)
+
+            self.t = threading.Thread(target=run, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nv = None
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(
-                ["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
-                stderr=subprocess.DEVNULL)
+                ["nvidia-smi", "-i", uuid or str(gpu_index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
 
     def stop(self):
-        if self.p is None:
+        if self.nv is not None:
+            self.stop_ev.set()
+            self.t.join(timeout=5)
+            rows = self.rows
+            mx = self.max_sm
+        elif self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+            self.f.flush()
+            rows, mx = [], None
+            with open(self.f.name) as fh:
+                for ln in fh:
+                    parts = [x.strip() for x in ln.split(",")]
+                    if len(parts) >= 3 and parts[0].replace(".", "").isdigit():
+                        rows.append((float(parts[0]), int(parts[2], 16) if parts[2].startswith("0x") else 0))
+                        mx = float(parts[1]) if parts[1].replace(".", "").isdigit() else mx
+            os.unlink(self.f.name)
+        else:
             return None
-        self.p.terminate()
-        try:
-            self.p.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.p.kill()
-        self.f.flush()
-        rows = []
-        with open(self.f.name) as fh:
-            for ln in fh:
-                parts = [x.strip() for x in ln.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.f.name)
         if not rows:
             return None
-        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
-        mx = max((float(r[2]) for r in rows if r[2].replace(".", "").isdigit()), default=None)
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(rows)}
+        sm = sorted(float(r[0]) for r in rows)
+        reasons = sorted({name for r in rows for bit, name in self.REASON_BITS.items() if int(r[1]) & bit})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
 
 
 # ------------------------------------------------------------- CPU arms
@@ -447,6 +484,7 @@ def run_ours(args):
     dl = torch.empty((H, W), dtype=torch.uint8, device=dev)
     dr = torch.empty((H, W), dtype=torch.uint8, device=dev)
     e2e_ms = 0.0
+    e2e_steps = []
     parts = [0.0, 0.0, 0.0]
     clk2 = Clocks(local)
     for i in range(args.steps):
@@ -462,7 +500,9 @@ def run_ours(args):
         host_out.copy_(out["disp"], non_blocking=True)
         ev[3].record(st)
         ev[3].synchronize()
-        e2e_ms += ev[0].elapsed_time(ev[3])
+        step_ms = ev[0].elapsed_time(ev[3])
+        e2e_steps.append(step_ms)
+        e2e_ms += step_ms
         for j in range(3):
             parts[j] += ev[j].elapsed_time(ev[j + 1])
     clocks_e2e = clk2.stop()
@@ -519,7 +559,9 @@ def run_ours(args):
         "e2e": {"value": e2e_fps, "unit": UNIT, "h2d_bytes_per_step": 2 * W * H,
                 "d2h_bytes_per_step": 2 * W * H,
                 "ms_per_step": {"h2d": parts[0] / args.steps, "stereo_sgm": parts[1] / args.steps,
-                                "d2h": parts[2] / args.steps}, "clocks": clocks_e2e},
+                                "d2h": parts[2] / args.steps},
+                "median_ms_per_step": sorted(e2e_steps)[len(e2e_steps) // 2],
+                "max_ms_per_step": max(e2e_steps), "clocks": clocks_e2e},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "alg_bytes_per_launch": dom_bytes, "avg_launch_ms": avg_ms,

@@ -54,7 +54,8 @@ namespace tdv {
 namespace {
 
 constexpr int kMaxG = 24;       // consumer warps per block, vertical/diagonal passes
-constexpr int kRowSlots = 8;    // ring depth (rows), vertical/diagonal passes (power of 2)
+constexpr int kRowSlots = 8;    // rows in flight, vertical/diagonal passes (power of 2)
+constexpr int kVdRowsPerSlot = 2;  // rows per ring slot (one wait and one release per slot)
 constexpr int kMaxGH = 8;       // warps per block, horizontal passes
 constexpr int kHSlots = 8;      // S ring depth (steps), horizontal passes
 constexpr int kChunk = 64;      // right-plane entries per horizontal refill
@@ -335,11 +336,14 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
                                         unsigned char* smem) {
     constexpr int SB = 128 * PPL;
     constexpr int DSPAN = 64 * PPL;
+    constexpr int U = kVdRowsPerSlot;
+    constexpr int NS = kRowSlots / U;  // ring slots (power of 2)
     const int NRG = (G + DSPAN) / 8 + 2;
     const int offL = G * SB, offR = offL + G * 16;
-    const int slotBytes = align128(offR + NRG * kGroupBytes);
+    const int rowBytes = align128(offR + NRG * kGroupBytes);
+    const int slotBytes = U * rowBytes;
     uint64_t* full = (uint64_t*)smem;
-    uint64_t* empty = full + kRowSlots;
+    uint64_t* empty = full + NS;
     unsigned char* slots = smem + 2 * kRowSlots * 8;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -360,9 +364,10 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
     const int nrows = yhi - ylo + 1;
     if (nrows <= 0) return;  // uniform for the block
     const int y0 = dy > 0 ? ylo : yhi;
+    const int nslots = (nrows + U - 1) / U;
 
     if (threadIdx.x == 0) {
-        for (int b = 0; b < kRowSlots; b++) {
+        for (int b = 0; b < NS; b++) {
             mbar_init(smem_u32(&full[b]), 1);
             mbar_init(smem_u32(&empty[b]), G);
         }
@@ -371,153 +376,131 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
     __syncthreads();
 
     if (warp == G) {
-        // ---- producer ----
+        // ---- producer: slot j holds rows U*j .. U*j+U-1 ----
         if (lane == 0) {
-            int i = 0;
+            int j = 0;
             bool ok = true;
-            for (; i < nrows; i++) {
-                const int b = i & (kRowSlots - 1);
-                if (i >= kRowSlots && !mbar_wait(smem_u32(&empty[b]), (uint32_t)((i / kRowSlots) - 1) & 1u)) {
+            for (; j < nslots; j++) {
+                const int b = j & (NS - 1);
+                if (j >= NS && !mbar_wait(smem_u32(&empty[b]), (uint32_t)((j / NS) - 1) & 1u)) {
                     ok = false;
                     break;
                 }
-                const int y = y0 + dy * i;
-                const int xf = kf + s * y;
-                const int xlo = max(xf, 0), xhi = min(xf + Gb, k.W);
-                const int npx = xhi - xlo;
-                const int g0 = max(0, xlo - DSPAN + 2) >> 3, g1 = (xhi - 1) >> 3;
-                unsigned char* base = slots + b * slotBytes;
                 const uint32_t bar = smem_u32(&full[b]);
-                const uint32_t sb = MODE != 0 ? (uint32_t)npx * SB : 0u;
-                const uint32_t lb = (uint32_t)npx * 16;
-                const uint32_t rb = (uint32_t)(g1 - g0 + 1) * kGroupBytes;
-                mbar_expect_tx(bar, sb + lb + rb);
-                if (MODE != 0)
-                    tma_load(smem_u32(base + (xlo - xf) * SB), k.S + ((size_t)y * k.W + xlo) * k.Dp2, sb, bar);
-                tma_load(smem_u32(base + offL + (xlo - xf) * 16), k.LP + (size_t)y * k.W + xlo, lb, bar);
-                tma_load(smem_u32(base + offR), k.RPp + (size_t)y * k.Wp + 9 * g0, rb, bar);
+                uint32_t total = 0;
+                for (int r = 0; r < U && U * j + r < nrows; r++) {
+                    const int y = y0 + dy * (U * j + r);
+                    const int xf = kf + s * y;
+                    const int xlo = max(xf, 0), xhi = min(xf + Gb, k.W);
+                    const int g0 = max(0, xlo - DSPAN + 2) >> 3, g1 = (xhi - 1) >> 3;
+                    total += (uint32_t)(xhi - xlo) * ((MODE != 0 ? SB : 0) + 16) + (uint32_t)(g1 - g0 + 1) * kGroupBytes;
+                }
+                mbar_expect_tx(bar, total);
+                for (int r = 0; r < U && U * j + r < nrows; r++) {
+                    const int y = y0 + dy * (U * j + r);
+                    const int xf = kf + s * y;
+                    const int xlo = max(xf, 0), xhi = min(xf + Gb, k.W);
+                    const int npx = xhi - xlo;
+                    const int g0 = max(0, xlo - DSPAN + 2) >> 3, g1 = (xhi - 1) >> 3;
+                    unsigned char* base = slots + b * slotBytes + r * rowBytes;
+                    if (MODE != 0)
+                        tma_load(smem_u32(base + (xlo - xf) * SB), k.S + ((size_t)y * k.W + xlo) * k.Dp2,
+                                 (uint32_t)npx * SB, bar);
+                    tma_load(smem_u32(base + offL + (xlo - xf) * 16), k.LP + (size_t)y * k.W + xlo,
+                             (uint32_t)npx * 16, bar);
+                    tma_load(smem_u32(base + offR), k.RPp + (size_t)y * k.Wp + 9 * g0,
+                             (uint32_t)(g1 - g0 + 1) * kGroupBytes, bar);
+                }
             }
             if (!ok) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
             // the block must not retire with copies in flight
-            for (int r = max(0, i - kRowSlots); r < i; r++)
-                mbar_wait(smem_u32(&full[r & (kRowSlots - 1)]), (uint32_t)(r / kRowSlots) & 1u,
-                          ok ? kWaitNs : kDrainNs);
-        }
-    } else if (warp < G && !DIAG) {
-        // ---- consumers, vertical: column x = kp on every row ----
-        const int x = kf + warp;
-        const bool has_line = warp < Gb;
-        const int base_d = lane * 2 * PPL;
-        const int eb = x - base_d;
-        const bool need_mask = base_d + 2 * PPL > k.D || eb < 2 * PPL;
-        const int lim = min(x + 1, k.D);
-        const int roff = -9 * (max(0, kf - DSPAN + 2) >> 3);
-        int rpos[PPL];
-#pragma unroll
-        for (int q = 0; q < PPL; q++) rpos[q] = (ppos(max(eb - 2 * q, 0)) + roff) * 16;
-        const unsigned char* lp_slot = slots + offL + warp * 16;
-        const unsigned char* sv_slot = slots + warp * SB + lane * PPL * 4;
-        const unsigned char* r_slot = slots + offR;
-        uint32_t L[PPL], m = 0;
-#pragma unroll
-        for (int q = 0; q < PPL; q++) L[q] = 0;
-        uint32_t* sg = k.S + ((size_t)y0 * k.W + x) * k.Dp2 + lane * PPL;
-        const long long sstep = (long long)dy * k.W * k.Dp2;
-        for (int i = 0; i < nrows; i++) {
-            const int b = i & (kRowSlots - 1);
-            if (!__all_sync(FULL, mbar_wait(smem_u32(&full[b]), (uint32_t)(i / kRowSlots) & 1u))) {
-                if (lane == 0) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
-                break;
-            }
-            if (has_line) {
-                const int boff = b * slotBytes;
-                const uint4 lp = *(const uint4*)(lp_slot + boff);
-                uint32_t c[PPL], Ln[PPL];
-#pragma unroll
-                for (int q = 0; q < PPL; q++) c[q] = bt_pair(lp, *(const uint4*)(r_slot + boff + rpos[q]));
-                if (need_mask) {
-#pragma unroll
-                    for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
-                }
-                recur<PPL>(L, m, c, Ln, lane, k);
-                if (MODE == 0) {
-                    Vec<PPL>::st(sg, Ln);
-                } else {
-                    uint32_t sv[PPL];
-                    Vec<PPL>::lds((const uint32_t*)(sv_slot + boff), sv);
-#pragma unroll
-                    for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
-                    Vec<PPL>::st(sg, sv);
-                }
-                sg += sstep;
-#pragma unroll
-                for (int q = 0; q < PPL; q++) L[q] = Ln[q];
-                m = warp_min_pairs<PPL>(L);
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&empty[b]));
+            for (int r = max(0, j - NS); r < j; r++)
+                mbar_wait(smem_u32(&full[r & (NS - 1)]), (uint32_t)(r / NS) & 1u, ok ? kWaitNs : kDrainNs);
         }
     } else if (warp < G) {
-        // ---- consumers, diagonal ----
-        const int kp = kf + warp;
+        // ---- consumers ----
         const bool has_line = warp < Gb;
         const int base_d = lane * 2 * PPL;
         const bool edge_lane = base_d + 2 * PPL > k.D;  // holds disparities >= D
-        const uint32_t* lp_slot = (const uint32_t*)(slots + offL + warp * 16);
-        const uint32_t* sv_slot = (const uint32_t*)(slots + warp * SB) + lane * PPL;
-        const long long step_px = (long long)dy * (k.W + s);  // pixel-index step per row
-        bool started = false;
+        const unsigned char* lp_slot = slots + offL + warp * 16;
+        const unsigned char* sv_slot = slots + warp * SB + lane * PPL * 4;
         uint32_t L[PPL], m = 0;
-        uint32_t* sg = nullptr;
+#pragma unroll
+        for (int q = 0; q < PPL; q++) L[q] = 0;
+        // vertical (s = 0): column x = kp on every row, offsets computed once
+        const int xs = kf + warp;
+        const int ebs = xs - base_d;
+        const bool need_mask_s = edge_lane || ebs < 2 * PPL;
+        const int lim_s = min(xs + 1, k.D);
+        int rpos[PPL];
+        {
+            const int roff = -9 * (max(0, kf - DSPAN + 2) >> 3);
+#pragma unroll
+            for (int q = 0; q < PPL; q++) rpos[q] = (ppos(max(ebs - 2 * q, 0)) + roff) * 16;
+        }
+        uint32_t* sg_s = k.S + ((size_t)y0 * k.W + xs) * k.Dp2 + lane * PPL;
+        const long long sstep = (long long)dy * k.W * k.Dp2;
 
-        for (int i = 0; i < nrows; i++) {
-            const int b = i & (kRowSlots - 1);
-            if (!__all_sync(FULL, mbar_wait(smem_u32(&full[b]), (uint32_t)(i / kRowSlots) & 1u))) {
-                if (lane == 0) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
-                break;
-            }
-            const int y = y0 + dy * i;
-            const int x = kp + s * y;
-            if (has_line && x >= 0 && x < k.W) {
-                const int boff = b * slotBytes;
-                const uint4 lp = *(const uint4*)((const unsigned char*)lp_slot + boff);
+        auto row = [&](int i, int boff) {
+            uint32_t c[PPL], Ln[PPL];
+            uint32_t* sg;
+            const uint4 lp = *(const uint4*)(lp_slot + boff);
+            if (!DIAG) {
+                if (!has_line) return;
+#pragma unroll
+                for (int q = 0; q < PPL; q++) c[q] = bt_pair(lp, *(const uint4*)(slots + offR + boff + rpos[q]));
+                if (need_mask_s) {
+#pragma unroll
+                    for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim_s, k.BIGBIG);
+                }
+                sg = sg_s;
+                sg_s += sstep;
+            } else {
+                const int y = y0 + dy * i;
+                const int x = xs + s * y;
+                if (!has_line || x < 0 || x >= k.W) return;
                 const int xlo = max(kf + s * y, 0);
                 const int roff = -9 * (max(0, xlo - DSPAN + 2) >> 3);
                 const Plane* rseg = (const Plane*)(slots + boff + offR);
-                uint32_t c[PPL], Ln[PPL];
                 const int eb = x - base_d;
-                #pragma unroll
+#pragma unroll
                 for (int q = 0; q < PPL; q++) {
                     const int e = max(eb - 2 * q, 0);
                     c[q] = bt_pair(lp, *(const uint4*)&rseg[ppos(e) + roff]);
                 }
-                const int lim = min(x + 1, k.D);
                 if (edge_lane || eb < 2 * PPL) {
-                    #pragma unroll
+                    const int lim = min(x + 1, k.D);
+#pragma unroll
                     for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
                 }
-                if (!started) {
-                    #pragma unroll
-                    for (int q = 0; q < PPL; q++) Ln[q] = c[q];
-                    started = true;
-                    sg = k.S + ((size_t)y * k.W + x) * k.Dp2 + lane * PPL;
-                } else {
-                    recur<PPL>(L, m, c, Ln, lane, k);
-                    sg += step_px * k.Dp2;
-                }
-                if (MODE == 0) {
-                    Vec<PPL>::st(sg, Ln);
-                } else {
-                    uint32_t sv[PPL];
-                    Vec<PPL>::lds((const uint32_t*)((const unsigned char*)sv_slot + boff), sv);
-                    #pragma unroll
-                    for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
-                    Vec<PPL>::st(sg, sv);
-                }
-                #pragma unroll
-                for (int q = 0; q < PPL; q++) L[q] = Ln[q];
-                m = warp_min_pairs<PPL>(L);
+                sg = k.S + ((size_t)y * k.W + x) * k.Dp2 + lane * PPL;
             }
+            recur<PPL>(L, m, c, Ln, lane, k);  // from L = 0, m = 0 the first step gives L = C
+            if (MODE == 0) {
+                Vec<PPL>::st(sg, Ln);
+            } else {
+                uint32_t sv[PPL];
+                Vec<PPL>::lds((const uint32_t*)(sv_slot + boff), sv);
+#pragma unroll
+                for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
+                Vec<PPL>::st(sg, sv);
+            }
+#pragma unroll
+            for (int q = 0; q < PPL; q++) L[q] = Ln[q];
+            m = warp_min_pairs<PPL>(L);
+        };
+
+        for (int j = 0; j < nslots; j++) {
+            const int b = j & (NS - 1);
+            if (!__all_sync(FULL, mbar_wait(smem_u32(&full[b]), (uint32_t)(j / NS) & 1u))) {
+                if (lane == 0) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
+                break;
+            }
+            const int boff = b * slotBytes;
+            row(U * j, boff);
+#pragma unroll
+            for (int r = 1; r < U; r++)
+                if (U * j + r < nrows) row(U * j + r, boff + r * rowBytes);
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&empty[b]));
         }
@@ -528,7 +511,7 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
     fence_proxy_async();
     __syncthreads();
     if (threadIdx.x == 0)
-        for (int b = 0; b < 2 * kRowSlots; b++) mbar_inval(smem_u32(&full[b]));
+        for (int b = 0; b < 2 * NS; b++) mbar_inval(smem_u32(&full[b]));
 }
 
 // ------------------------------------------------------ horizontal passes

@@ -105,7 +105,8 @@ __device__ __forceinline__ void run_h(const BPair& P, int dx, int blk, unsigned 
     }
 }
 
-__global__ void __launch_bounds__(kBatchWarps * 32, 1)
+// 800 threads x 80 registers = 64000 of the SM's 65536: one block per SM
+__global__ void __maxnreg__(80)
     batch_kernel(const BPair* __restrict__ pairs, int npairs, const BItem* __restrict__ items, int nitems,
                  int* ctl, unsigned long long wait_ns) {
     extern __shared__ __align__(128) unsigned char smem[];

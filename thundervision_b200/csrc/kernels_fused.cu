@@ -2,6 +2,9 @@
 // (prep, V+, V-, D1+, D1-, D2+, D2-, H+, H- with WTA), each a thin wrapper
 // around the device bodies in fused_body.cuh.
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "fused_body.cuh"
@@ -56,6 +59,22 @@ int sm_count() {
     return cache[dev];
 }
 
+// Opts a kernel into `bytes` of dynamic shared memory on the current device,
+// once: later launches needing no more skip the driver call.
+cudaError_t opt_in_smem(const void* fn, int bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    int& cur = done[{fn, dev}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
 // Greedy pairing: groups by decreasing row count, each block takes the
 // longest left and, if it fits under the longest, the shortest left.
 // Returns the block count, or -1 if the table would overflow.
@@ -68,6 +87,7 @@ int pair_groups(int W, int H, int s, int kmin, int nlines, int G, GroupPairs& gp
         order[j] = j;
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rows[a] > rows[b]; });
+    for (int b = 0; b < kMaxPairedBlocks; b++) gp.first[b] = gp.second[b] = -1;
     const int cap = rows[order[0]];
     int lo = 0, hi = ng - 1, nb = 0;
     while (lo <= hi) {
@@ -81,6 +101,12 @@ int pair_groups(int W, int H, int s, int kmin, int nlines, int G, GroupPairs& gp
     return nb;
 }
 
+int pair_count(const GroupPairs& gp) {
+    int n = 0;
+    while (n < kMaxPairedBlocks && gp.first[n] >= 0) n++;
+    return n;
+}
+
 template <int PPL, int MODE, bool DIAG>
 cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
     const int s = dx * dy;
@@ -92,22 +118,34 @@ cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
     int G = (k.W + nsm - 1) / nsm;
     G = G < 1 ? 1 : (G > kMaxG ? kMaxG : G);
     if (DIAG) {
-        // smallest G whose paired blocks fit one wave
-        for (; G <= kMaxG; G++) {
-            blocks = pair_groups(k.W, k.H, s, kmin, nlines, G, gp);
-            if (blocks > 0 && blocks <= nsm) break;
+        // smallest G whose paired blocks fit one wave (cached per shape)
+        static std::mutex mu;
+        static std::map<std::tuple<int, int, int, int>, std::pair<int, GroupPairs>> cache;
+        const auto key = std::make_tuple(k.W, k.H, s, nsm);
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it == cache.end()) {
+            int g = G, nb = -1;
+            for (; g <= kMaxG; g++) {
+                nb = pair_groups(k.W, k.H, s, kmin, nlines, g, gp);
+                if (nb > 0 && nb <= nsm) break;
+            }
+            if (g > kMaxG) {
+                g = kMaxG;
+                nb = pair_groups(k.W, k.H, s, kmin, nlines, g, gp);
+            }
+            if (cache.size() > 64) cache.clear();
+            it = cache.emplace(key, std::make_pair(nb > 0 ? g : -g, gp)).first;
         }
-        if (G > kMaxG) {
-            G = kMaxG;
-            blocks = pair_groups(k.W, k.H, s, kmin, nlines, G, gp);
-        }
-        paired = blocks > 0;
+        G = it->second.first > 0 ? it->second.first : -it->second.first;
+        paired = it->second.first > 0;
+        gp = it->second.second;
+        blocks = paired ? pair_count(gp) : 0;
     }
     if (!paired) blocks = (nlines + G - 1) / G;
     const int smem = vd_smem_bytes(G, PPL);
     if (smem > kSmemBudget) return cudaErrorInvalidConfiguration;
-    cudaError_t e =
-        cudaFuncSetAttribute(vd_pass<PPL, MODE, DIAG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = opt_in_smem((const void*)vd_pass<PPL, MODE, DIAG>, smem);
     if (e != cudaSuccess) return e;
     vd_pass<PPL, MODE, DIAG><<<blocks, (G + 1) * 32, smem, st>>>(k, s, dy, kmin, nlines, G, gp, paired);
     return cudaGetLastError();
@@ -124,8 +162,7 @@ cudaError_t launch_hp(const FK& k, int dx, int max_rows, cudaStream_t st) {
     while (R > 1 && hp_smem_bytes(R, PPL, lr, k.W, TWO) > kSmemBudget) R--;
     const int smem = hp_smem_bytes(R, PPL, lr, k.W, TWO);
     if (smem > kSmemBudget) return cudaErrorInvalidConfiguration;
-    cudaError_t e =
-        cudaFuncSetAttribute(hp_pass<PPL, MODE, TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = opt_in_smem((const void*)hp_pass<PPL, MODE, TWO>, smem);
     if (e != cudaSuccess) return e;
     const int blocks = (k.H + R - 1) / R;
     hp_pass<PPL, MODE, TWO><<<blocks, (R + 1) * 32, smem, st>>>(k, dx, R);
