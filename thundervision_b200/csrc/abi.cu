@@ -520,13 +520,10 @@ tdv_status tdv_soft_sgm_forward(tdv_ctx* ctx, const tdv_volume* cost, const tdv_
         return fail(ctx, TDV_ERR_INVALID_ARG, "tape of %zu bytes < %zu needed", tape_bytes, lay.total);
     TDV_DEVICE_SCOPE(ctx);
     ctx->timer.begin(S(stream));
-    unsigned char* base;
-    if (tape) {
-        base = (unsigned char*)tape;
-    } else {
-        TDV_TRY(ensure(ctx, ctx->soft, lay.stats + al256((size_t)W * H * 3 * es)));
-        base = (unsigned char*)ctx->soft.ptr;
-    }
+    // scratch: one L volume per direction, then (without a tape) the statistics
+    const size_t parts = (size_t)soft_ndir(p->paths) * al256((size_t)W * H * D * es);
+    TDV_TRY(ensure(ctx, ctx->soft, parts + al256((size_t)W * H * 3 * es)));
+    unsigned char* base = tape ? (unsigned char*)tape : nullptr;
     if (tape && p->checkpoint > 0)
         TDV_CUDA(cudaMemcpyAsync(base + lay.off, ctx->ckpt_off_host.data(),
                                  ctx->ckpt_off_host.size() * sizeof(long long), cudaMemcpyHostToDevice,
@@ -534,8 +531,9 @@ tdv_status tdv_soft_sgm_forward(tdv_ctx* ctx, const tdv_volume* cost, const tdv_
     tdv::SoftLaunch a{};
     a.f64 = es == 8;
     a.cost = cost->ptr;
-    a.S = base + lay.S;
-    a.stats = base + lay.stats;
+    a.part = ctx->soft.ptr;
+    a.S = tape ? base + lay.S : nullptr;
+    a.stats = tape ? base + lay.stats : (unsigned char*)ctx->soft.ptr + parts;
     a.dhat = dhat;
     a.W = W;
     a.H = H;
@@ -574,8 +572,10 @@ tdv_status tdv_soft_sgm_backward(tdv_ctx* ctx, const tdv_volume* cost, const tdv
         return fail(ctx, TDV_ERR_INVALID_ARG, "tape of %zu bytes < %zu needed", tape_bytes, lay.total);
     TDV_DEVICE_SCOPE(ctx);
     ctx->timer.begin(S(stream));
+    // scratch: dS, one dC contribution volume per direction, per-walk penalty sums
     const size_t ds_bytes = al256((size_t)W * H * D * es);
-    TDV_TRY(ensure(ctx, ctx->soft, ds_bytes + (size_t)8 * (W + H) * 2 * es));
+    const size_t parts = (size_t)soft_ndir(p->paths) * ds_bytes;
+    TDV_TRY(ensure(ctx, ctx->soft, ds_bytes + parts + (size_t)8 * (W + H) * 2 * es));
     unsigned char* base = (unsigned char*)tape;
     tdv::SoftLaunch a{};
     a.f64 = es == 8;
@@ -583,7 +583,8 @@ tdv_status tdv_soft_sgm_backward(tdv_ctx* ctx, const tdv_volume* cost, const tdv
     a.S = base + lay.S;
     a.stats = base + lay.stats;
     a.dS = ctx->soft.ptr;
-    a.dpen_part = (unsigned char*)ctx->soft.ptr + ds_bytes;
+    a.part = (unsigned char*)ctx->soft.ptr + ds_bytes;
+    a.dpen_part = (unsigned char*)ctx->soft.ptr + ds_bytes + parts;
     a.dcost = dcost->ptr;
     a.g = g_dhat;
     a.dpen = dpen;

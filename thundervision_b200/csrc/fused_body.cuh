@@ -387,12 +387,15 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
                     break;
                 }
                 const uint32_t bar = smem_u32(&full[b]);
+                // the right-plane segment of a row starts (virtually) at group
+                // g0v = floor((xf - DSPAN + 2) / 8), which may be negative:
+                // groups left of the image are not copied (their cells are masked)
                 uint32_t total = 0;
                 for (int r = 0; r < U && U * j + r < nrows; r++) {
                     const int y = y0 + dy * (U * j + r);
                     const int xf = kf + s * y;
                     const int xlo = max(xf, 0), xhi = min(xf + Gb, k.W);
-                    const int g0 = max(0, xlo - DSPAN + 2) >> 3, g1 = (xhi - 1) >> 3;
+                    const int g0 = max(0, (xf - DSPAN + 2) >> 3), g1 = (xhi - 1) >> 3;
                     total += (uint32_t)(xhi - xlo) * ((MODE != 0 ? SB : 0) + 16) + (uint32_t)(g1 - g0 + 1) * kGroupBytes;
                 }
                 mbar_expect_tx(bar, total);
@@ -401,14 +404,15 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
                     const int xf = kf + s * y;
                     const int xlo = max(xf, 0), xhi = min(xf + Gb, k.W);
                     const int npx = xhi - xlo;
-                    const int g0 = max(0, xlo - DSPAN + 2) >> 3, g1 = (xhi - 1) >> 3;
+                    const int g0v = (xf - DSPAN + 2) >> 3;  // arithmetic shift: floor division
+                    const int g0 = max(0, g0v), g1 = (xhi - 1) >> 3;
                     unsigned char* base = slots + b * slotBytes + r * rowBytes;
                     if (MODE != 0)
                         tma_load(smem_u32(base + (xlo - xf) * SB), k.S + ((size_t)y * k.W + xlo) * k.Dp2,
                                  (uint32_t)npx * SB, bar);
                     tma_load(smem_u32(base + offL + (xlo - xf) * 16), k.LP + (size_t)y * k.W + xlo,
                              (uint32_t)npx * 16, bar);
-                    tma_load(smem_u32(base + offR), k.RPp + (size_t)y * k.Wp + 9 * g0,
+                    tma_load(smem_u32(base + offR + (g0 - g0v) * kGroupBytes), k.RPp + (size_t)y * k.Wp + 9 * g0,
                              (uint32_t)(g1 - g0 + 1) * kGroupBytes, bar);
                 }
             }
@@ -432,11 +436,16 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
         const int ebs = xs - base_d;
         const bool need_mask_s = edge_lane || ebs < 2 * PPL;
         const int lim_s = min(xs + 1, k.D);
-        int rpos[PPL];
-        {
-            const int roff = -9 * (max(0, kf - DSPAN + 2) >> 3);
+        // right-plane entry e of a row sits at ppos(e - 8*g0v) in the segment
+        // (g0v its virtual first group, a multiple of 8 entries below e): for
+        // the line x = xf + warp that is ppos(cq + phase), with the per-lane
+        // constant cq = DSPAN - 2 + warp - base_d - 2q and the per-row phase
+        // (xf - DSPAN + 2) & 7; vertical lines have one phase for every row
+        int cq[PPL], rpos[PPL];
 #pragma unroll
-            for (int q = 0; q < PPL; q++) rpos[q] = (ppos(max(ebs - 2 * q, 0)) + roff) * 16;
+        for (int q = 0; q < PPL; q++) {
+            cq[q] = DSPAN - 2 + warp - base_d - 2 * q;
+            rpos[q] = ppos(cq[q] + ((kf - DSPAN + 2) & 7)) * 16;
         }
         uint32_t* sg_s = k.S + ((size_t)y0 * k.W + xs) * k.Dp2 + lane * PPL;
         const long long sstep = (long long)dy * k.W * k.Dp2;
@@ -459,15 +468,11 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
                 const int y = y0 + dy * i;
                 const int x = xs + s * y;
                 if (!has_line || x < 0 || x >= k.W) return;
-                const int xlo = max(kf + s * y, 0);
-                const int roff = -9 * (max(0, xlo - DSPAN + 2) >> 3);
-                const Plane* rseg = (const Plane*)(slots + boff + offR);
+                const int phase = (kf + s * y - DSPAN + 2) & 7;
+                const unsigned char* rseg = slots + boff + offR;
                 const int eb = x - base_d;
 #pragma unroll
-                for (int q = 0; q < PPL; q++) {
-                    const int e = max(eb - 2 * q, 0);
-                    c[q] = bt_pair(lp, *(const uint4*)&rseg[ppos(e) + roff]);
-                }
+                for (int q = 0; q < PPL; q++) c[q] = bt_pair(lp, *(const uint4*)(rseg + ppos(cq[q] + phase) * 16));
                 if (edge_lane || eb < 2 * PPL) {
                     const int lim = min(x + 1, k.D);
 #pragma unroll

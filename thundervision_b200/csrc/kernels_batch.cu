@@ -105,8 +105,9 @@ __device__ __forceinline__ void run_h(const BPair& P, int dx, int blk, unsigned 
     }
 }
 
-// 800 threads x 80 registers = 64000 of the SM's 65536: one block per SM
-__global__ void __maxnreg__(80)
+// one 800-thread block per SM (the register budget this bound leaves is what
+// the launch can hold)
+__global__ void __launch_bounds__(kBatchWarps * 32, 1)
     batch_kernel(const BPair* __restrict__ pairs, int npairs, const BItem* __restrict__ items, int nitems,
                  int* ctl, unsigned long long wait_ns) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -338,6 +339,10 @@ const char* batch_plan(const std::vector<BatchPairArgs>& pairs, int p1h, int p2h
 }
 
 cudaError_t batch_configure(const BatchPlan& plan) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, batch_kernel);
+    if (e != cudaSuccess) return e;
+    if (fa.maxThreadsPerBlock < kBatchWarps * 32) return cudaErrorInvalidConfiguration;
     return cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, plan.smem);
 }
 

@@ -12,6 +12,12 @@
 //     the lowest argmin of L (the m used by the next step);
 //   * tape mode "checkpoint k": L at every k-th step of each path; the
 //     adjoint recomputes the codes of one k-step segment at a time.
+// All directions run in one launch (a block's warps take consecutive walks of
+// one direction): the forward stores each direction's L into its own volume
+// and the argmin kernel sums them in direction order; the adjoint stores each
+// direction's dC contribution into its own volume and a sum kernel adds them
+// in direction order -- the same sums, in the same order, as accumulating one
+// direction after another, so results are deterministic.
 // Adjoint, walking each path from its end: G_t = dS_t + carry;
 // dC_t += G_t; carry_{t-1}(d) = [c_t(d)=0] G_t(d) + [c_t(d+1)=1] G_t(d+1) +
 // [c_t(d-1)=2] G_t(d-1) + [d = k*_{t-1}] (sum_{c=3} G_t - sum G_t);
@@ -94,9 +100,8 @@ struct Lane {
 template <typename T>
 struct SoftK {
     const T* C;   // HWD cost
-    T* S;         // HWD aggregation
+    T* part;      // [dir][pixel][D]: per-direction L (forward) or dC contribution (backward)
     T* dS;        // HWD dLoss/dS (backward)
-    T* dC;        // HWD dLoss/dC (backward)
     uint8_t* codes;   // [dir][pixel][32 lanes][kBytes]
     uint16_t* kstar;  // [dir][pixel]
     T* ckpt;          // [dir][sum over walks of ceil(len/k)][D]
@@ -106,6 +111,29 @@ struct SoftK {
     T* dpen;     // [2] dP1, dP2
     T* dpen_part;  // [dir][walk][2] per-walk partial sums (summed in a fixed order)
 };
+
+__constant__ int kSoftDx[8] = {1, -1, 0, 0, 1, -1, -1, 1};
+__constant__ int kSoftDy[8] = {0, 0, 1, -1, 1, -1, 1, -1};
+
+__device__ __forceinline__ int nwalks_dev(int dx, int dy, int W, int H) {
+    return dy == 0 ? H : (dx == 0 ? W : W + H - 1);
+}
+
+// This block's direction and walk-block (4 walks per block, directions in
+// order); false past the last direction.
+__device__ __forceinline__ bool block_dir(int nd, int W, int H, int& dir, int& wblk) {
+    int b = blockIdx.x;
+    for (int d = 0; d < nd; d++) {
+        const int nb = (nwalks_dev(kSoftDx[d], kSoftDy[d], W, H) + 3) / 4;
+        if (b < nb) {
+            dir = d;
+            wblk = b;
+            return true;
+        }
+        b -= nb;
+    }
+    return false;
+}
 
 // L_t from L_{t-1}: returns the choice code of each disparity.
 template <typename T, int NPL>
@@ -161,10 +189,13 @@ __device__ __forceinline__ uint32_t load_codes(const uint8_t* src) {
 
 // REC: 0 = no tape (inference), 1 = codes, 2 = checkpoints.
 template <typename T, int NPL, int REC>
-__global__ void __launch_bounds__(128) soft_fwd_pass(SoftK<T> k, int dx, int dy, int nwalks, int first,
-                                                     int dir) {
+__global__ void __launch_bounds__(128) soft_fwd_pass(SoftK<T> k, int nd) {
     const int lane = threadIdx.x & 31;
-    const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    int dir, wblk;
+    if (!block_dir(nd, k.W, k.H, dir, wblk)) return;
+    const int dx = kSoftDx[dir], dy = kSoftDy[dir];
+    const int nwalks = nwalks_dev(dx, dy, k.W, k.H);
+    const int w = wblk * 4 + (threadIdx.x >> 5);
     if (w >= nwalks) return;
     int sx, sy, len;
     walk_geom(w, dx, dy, k.W, k.H, sx, sy, len);
@@ -176,6 +207,7 @@ __global__ void __launch_bounds__(128) soft_fwd_pass(SoftK<T> k, int dx, int dy,
     uint8_t* codes = k.codes ? k.codes + (size_t)dir * npix * 32 * CB : nullptr;
     uint16_t* kst = k.kstar ? k.kstar + (size_t)dir * npix : nullptr;
     T* ck = (REC == 2) ? k.ckpt + (size_t)k.ckpt_off[(size_t)dir * (k.W + k.H) + w] * D : nullptr;
+    T* Lout = k.part + (size_t)dir * npix * D;
 
     T L[NPL], c[NPL], Ln[NPL];
     int x = sx, y = sy;
@@ -185,7 +217,7 @@ __global__ void __launch_bounds__(128) soft_fwd_pass(SoftK<T> k, int dx, int dy,
         const int d = d0 + j;
         c[j] = d < D ? k.C[p * D + d] : inf;
         L[j] = c[j];
-        if (d < D) k.S[p * D + d] = first ? L[j] : k.S[p * D + d] + L[j];
+        if (d < D) Lout[p * D + d] = L[j];
         if (REC == 2 && d < D) ck[d] = L[j];
     }
     T m;
@@ -207,7 +239,7 @@ __global__ void __launch_bounds__(128) soft_fwd_pass(SoftK<T> k, int dx, int dy,
         for (int j = 0; j < NPL; j++) {
             const int d = d0 + j;
             L[j] = Ln[j];
-            if (d < D) k.S[p * D + d] = first ? L[j] : k.S[p * D + d] + L[j];
+            if (d < D) Lout[p * D + d] = L[j];
         }
         if (REC == 1) store_codes<T, NPL>(codes + (p * 32 + lane) * CB, cw);
         if (REC == 2 && t % k.ck == 0) {
@@ -221,21 +253,39 @@ __global__ void __launch_bounds__(128) soft_fwd_pass(SoftK<T> k, int dx, int dy,
     }
 }
 
-// Soft-argmin per pixel (warp per pixel): stats = (Smin, 1/Z, dhat).
+// S = sum of the directions' L in direction order, then the soft-argmin per
+// pixel (warp per pixel): stats = (Smin, 1/Z, dhat); S stored when S_out.
 template <typename T>
-__global__ void soft_argmin_kernel(const T* S, int npix, int D, T tau, T* dhat, T* stats) {
+__global__ void soft_argmin_kernel(const T* part, int nd, int npix, int D, T tau, T* dhat, T* stats,
+                                   T* S_out) {
     const int lane = threadIdx.x & 31;
+    const size_t vol = (size_t)npix * D;
+    constexpr int KMAXD = 8;  // D <= 256: at most 8 disparities per lane
     for (size_t p = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < (size_t)npix;
          p += ((size_t)gridDim.x * blockDim.x) >> 5) {
-        const T* s = S + p * D;
+        T sv[KMAXD];
         T mn = inf_v<T>();
-        for (int d = lane; d < D; d += 32) mn = fmin(mn, s[d]);
+#pragma unroll
+        for (int i = 0; i < KMAXD; i++) {
+            const int d = lane + 32 * i;
+            if (d < D) {
+                T acc = part[p * D + d];
+                for (int r = 1; r < nd; r++) acc = acc + part[r * vol + p * D + d];
+                sv[i] = acc;
+                if (S_out) S_out[p * D + d] = acc;
+                mn = fmin(mn, acc);
+            }
+        }
         mn = warp_minv(mn);
         T z = 0, num = 0;
-        for (int d = lane; d < D; d += 32) {
-            const T e = exp(-(s[d] - mn) / tau);
-            z += e;
-            num += (T)d * e;
+#pragma unroll
+        for (int i = 0; i < KMAXD; i++) {
+            const int d = lane + 32 * i;
+            if (d < D) {
+                const T e = exp(-(sv[i] - mn) / tau);
+                z += e;
+                num += (T)d * e;
+            }
         }
         z = warp_sum(z);
         num = warp_sum(num);
@@ -268,14 +318,17 @@ __global__ void soft_ds_kernel(const T* S, const T* stats, const T* g, int npix,
 // tape (CK = false) or are recomputed per k-step segment from the stored
 // checkpoints into shared memory (CK = true, k <= 32).
 template <typename T, int NPL, bool CK>
-__global__ void __launch_bounds__(128) soft_bwd_pass(SoftK<T> k, int dx, int dy, int nwalks, int first,
-                                                     int dir) {
+__global__ void __launch_bounds__(128) soft_bwd_pass(SoftK<T> k, int nd) {
     constexpr int WARPS = 4;
     constexpr int KMAX = 32;
     __shared__ uint16_t sk[WARPS][KMAX + 1];
     __shared__ uint32_t segc[WARPS][KMAX][32];  // CK: codes of the segment's steps, per lane
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    int dir, wblk;
+    if (!block_dir(nd, k.W, k.H, dir, wblk)) return;
+    const int dx = kSoftDx[dir], dy = kSoftDy[dir];
+    const int nwalks = nwalks_dev(dx, dy, k.W, k.H);
+    const int w = wblk * 4 + warp;
     if (w >= nwalks) return;
     int sx, sy, len;
     walk_geom(w, dx, dy, k.W, k.H, sx, sy, len);
@@ -284,6 +337,7 @@ __global__ void __launch_bounds__(128) soft_bwd_pass(SoftK<T> k, int dx, int dy,
     const T inf = inf_v<T>();
     const size_t npix = (size_t)k.W * k.H;
     constexpr int CB = CodeWord<NPL>::kBytes;
+    T* dCout = k.part + (size_t)dir * npix * D;
     const uint8_t* codes = CK ? nullptr : k.codes + (size_t)dir * npix * 32 * CB;
     const uint16_t* kst = CK ? nullptr : k.kstar + (size_t)dir * npix;
     const T* ckp = CK ? k.ckpt + (size_t)k.ckpt_off[(size_t)dir * (k.W + k.H) + w] * D : nullptr;
@@ -303,7 +357,7 @@ __global__ void __launch_bounds__(128) soft_bwd_pass(SoftK<T> k, int dx, int dy,
         for (int j = 0; j < NPL; j++) {
             const int d = d0 + j;
             G[j] = d < D ? k.dS[p * D + d] + carry[j] : (T)0;
-            if (d < D) k.dC[p * D + d] = first ? G[j] : k.dC[p * D + d] + G[j];
+            if (d < D) dCout[p * D + d] = G[j];
         }
         if (t == 0) break;
         uint32_t cw;
@@ -410,6 +464,16 @@ __global__ void soft_pen_reduce(const T* part, int ndir, int W, int H, T* dpen) 
     if (lane == 0) dpen[which] = acc;
 }
 
+// dC = sum of the directions' contributions in direction order.
+template <typename T>
+__global__ void soft_dc_sum(const T* part, int nd, size_t vol, T* dC) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < vol; i += (size_t)gridDim.x * blockDim.x) {
+        T acc = part[i];
+        for (int r = 1; r < nd; r++) acc = acc + part[r * vol + i];
+        dC[i] = acc;
+    }
+}
+
 const int kDirs8[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1}, {-1, 1}, {1, -1}};
 
 int nwalks_of(int dx, int dy, int W, int H) {
@@ -418,36 +482,34 @@ int nwalks_of(int dx, int dy, int W, int H) {
     return W + H - 1;
 }
 
+int soft_blocks(int nd, int W, int H) {
+    int b = 0;
+    for (int i = 0; i < nd; i++) b += (nwalks_of(kDirs8[i][0], kDirs8[i][1], W, H) + 3) / 4;
+    return b;
+}
+
 template <typename T, int NPL>
 cudaError_t fwd_all(SoftK<T> k, int paths, int rec, cudaStream_t st, Timer* tm) {
     const int nd = paths == 4 ? 4 : 8;
-    for (int i = 0; i < nd; i++) {
-        const int dx = kDirs8[i][0], dy = kDirs8[i][1];
-        const int nw = nwalks_of(dx, dy, k.W, k.H);
-        const int blocks = (nw + 3) / 4;
-        if (rec == 0) soft_fwd_pass<T, NPL, 0><<<blocks, 128, 0, st>>>(k, dx, dy, nw, i == 0, i);
-        else if (rec == 1) soft_fwd_pass<T, NPL, 1><<<blocks, 128, 0, st>>>(k, dx, dy, nw, i == 0, i);
-        else soft_fwd_pass<T, NPL, 2><<<blocks, 128, 0, st>>>(k, dx, dy, nw, i == 0, i);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        if (tm) tm->mark("soft_fwd_pass");
-    }
+    const int blocks = soft_blocks(nd, k.W, k.H);
+    if (rec == 0) soft_fwd_pass<T, NPL, 0><<<blocks, 128, 0, st>>>(k, nd);
+    else if (rec == 1) soft_fwd_pass<T, NPL, 1><<<blocks, 128, 0, st>>>(k, nd);
+    else soft_fwd_pass<T, NPL, 2><<<blocks, 128, 0, st>>>(k, nd);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (tm) tm->mark("soft_fwd_pass");
     return cudaSuccess;
 }
 
 template <typename T, int NPL>
 cudaError_t bwd_all(SoftK<T> k, int paths, bool ck, cudaStream_t st, Timer* tm) {
     const int nd = paths == 4 ? 4 : 8;
-    for (int i = 0; i < nd; i++) {
-        const int dx = kDirs8[i][0], dy = kDirs8[i][1];
-        const int nw = nwalks_of(dx, dy, k.W, k.H);
-        const int blocks = (nw + 3) / 4;
-        if (ck) soft_bwd_pass<T, NPL, true><<<blocks, 128, 0, st>>>(k, dx, dy, nw, i == 0, i);
-        else soft_bwd_pass<T, NPL, false><<<blocks, 128, 0, st>>>(k, dx, dy, nw, i == 0, i);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        if (tm) tm->mark("soft_bwd_pass");
-    }
+    const int blocks = soft_blocks(nd, k.W, k.H);
+    if (ck) soft_bwd_pass<T, NPL, true><<<blocks, 128, 0, st>>>(k, nd);
+    else soft_bwd_pass<T, NPL, false><<<blocks, 128, 0, st>>>(k, nd);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (tm) tm->mark("soft_bwd_pass");
     return cudaSuccess;
 }
 
@@ -461,7 +523,7 @@ template <typename T>
 cudaError_t soft_forward_t(const SoftLaunch& L, cudaStream_t st, Timer* tm) {
     SoftK<T> k{};
     k.C = (const T*)L.cost;
-    k.S = (T*)L.S;
+    k.part = (T*)L.part;
     k.codes = (uint8_t*)L.codes;
     k.kstar = (uint16_t*)L.kstar;
     k.ckpt = (T*)L.ckpt;
@@ -481,7 +543,7 @@ cudaError_t soft_forward_t(const SoftLaunch& L, cudaStream_t st, Timer* tm) {
     if (e != cudaSuccess) return e;
     const int npix = L.W * L.H;
     soft_argmin_kernel<T><<<grid_for((size_t)npix * 32, 256), 256, 0, st>>>(
-        (const T*)L.S, npix, L.D, (T)L.tau, (T*)L.dhat, (T*)L.stats);
+        (const T*)L.part, L.paths == 4 ? 4 : 8, npix, L.D, (T)L.tau, (T*)L.dhat, (T*)L.stats, (T*)L.S);
     if (tm) tm->mark("soft_argmin");
     return cudaGetLastError();
 }
@@ -490,9 +552,8 @@ template <typename T>
 cudaError_t soft_backward_t(const SoftLaunch& L, cudaStream_t st, Timer* tm) {
     SoftK<T> k{};
     k.C = (const T*)L.cost;
-    k.S = (T*)L.S;
+    k.part = (T*)L.part;
     k.dS = (T*)L.dS;
-    k.dC = (T*)L.dcost;
     k.codes = (uint8_t*)L.codes;
     k.kstar = (uint16_t*)L.kstar;
     k.ckpt = (T*)L.ckpt;
@@ -517,6 +578,10 @@ cudaError_t soft_backward_t(const SoftLaunch& L, cudaStream_t st, Timer* tm) {
     else if (L.D <= 128) e = bwd_all<T, 4>(k, L.paths, ck, st, tm);
     else e = bwd_all<T, 8>(k, L.paths, ck, st, tm);
     if (e != cudaSuccess) return e;
+    const size_t vol = (size_t)npix * L.D;
+    soft_dc_sum<T><<<grid_for(vol, 256), 256, 0, st>>>((const T*)L.part, L.paths == 4 ? 4 : 8, vol, (T*)L.dcost);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (tm) tm->mark("soft_dc_sum");
     soft_pen_reduce<T><<<1, 64, 0, st>>>(k.dpen_part, L.paths == 4 ? 4 : 8, L.W, L.H, k.dpen);
     if (tm) tm->mark("soft_pen_reduce");
     return cudaGetLastError();

@@ -232,6 +232,7 @@ cudaError_t batch_launch(const BatchPlan& plan, unsigned char* d_desc, unsigned 
 struct SoftLaunch {
     int f64;
     const void* cost;
+    void* part;  // scratch: one volume per direction (forward L, backward dC contributions)
     void* S;
     void* dS;
     void* dcost;
