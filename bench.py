@@ -507,11 +507,10 @@ def run_ours(args):
             parts[j] += ev[j].elapsed_time(ev[j + 1])
     clocks_e2e = clk2.stop()
 
-    t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
+    from thundervision_b200.replicas import max_over_ranks
+    total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], device=dev)
     if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    total_ms, e2e_ms = float(t[0]), float(t[1])
     if rank != 0:
         ctx.close()
         if world > 1:
