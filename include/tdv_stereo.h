@@ -182,6 +182,9 @@ typedef struct {
     int32_t split_disparity; /* horizontal passes, D > 64: 1 = two warps share a row's
                                 disparity range, 0 = one warp per row */
     int32_t order;           /* tdv_batch_order: pairs inside each pass of the queue */
+    int32_t ctas_per_sm;     /* 1: one 25-warp block per SM; 2: two 13-warp blocks per SM,
+                                each taking its own work items (lines and rows per block
+                                then at most 12) */
 } tdv_batch_tiles;
 
 typedef struct tdv_batch tdv_batch;

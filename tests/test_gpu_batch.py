@@ -59,6 +59,8 @@ def _batch(ctx, pairs, paths=8):
     {"split_disparity": 1, "rows_per_cta": 5},
     {"lines_per_cta": 24, "rows_per_cta": 25, "split_disparity": 1},
     {"lines_per_cta": 7, "rows_per_cta": 12, "split_disparity": 0},
+    {"ctas_per_sm": 2},
+    {"ctas_per_sm": 2, "lines_per_cta": 24, "rows_per_cta": 25, "split_disparity": 1},
 ])
 def test_batch_matches_per_pair(ctx, paths, tiles):
     pairs = _pairs(SHAPES, seed=paths)

@@ -73,7 +73,8 @@ class tdv_batch_pair(ctypes.Structure):
 
 class tdv_batch_tiles(ctypes.Structure):
     _fields_ = [("lines_per_cta", ctypes.c_int32), ("rows_per_cta", ctypes.c_int32),
-                ("split_disparity", ctypes.c_int32), ("order", ctypes.c_int32)]
+                ("split_disparity", ctypes.c_int32), ("order", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32)]
 
 
 ALLOC_FN = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)

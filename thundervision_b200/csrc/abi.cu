@@ -922,6 +922,7 @@ tdv_status tdv_batch_create(tdv_ctx* ctx, const tdv_batch_pair* pairs, int32_t n
     t.rows_per_cta = 8;
     t.split_disparity = 0;
     t.order = TDV_BATCH_ORDER_LONGEST_FIRST;
+    t.ctas_per_sm = 1;
     const tdv_status st = batch_replan(b, t);
     if (st != TDV_OK) {
         tdv_batch_destroy(b);
@@ -949,6 +950,8 @@ tdv_status tdv_batch_set_tiles(tdv_batch* b, const tdv_batch_tiles* tiles) {
         return fail(ctx, TDV_ERR_INVALID_ARG, "bad queue order %d", tiles->order);
     if (tiles->split_disparity != 0 && tiles->split_disparity != 1)
         return fail(ctx, TDV_ERR_INVALID_ARG, "split_disparity must be 0 or 1");
+    if (tiles->ctas_per_sm != 1 && tiles->ctas_per_sm != 2)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "ctas_per_sm must be 1 or 2");
     TDV_DEVICE_SCOPE(ctx);
     TDV_CUDA(cudaDeviceSynchronize());
     return batch_replan(b, *tiles);
@@ -1060,32 +1063,45 @@ tdv_status tdv_batch_autotune(tdv_batch* b, int32_t reps, tdv_stream stream, tdv
     tdv_batch_tiles best = b->tiles;
     double best_t = HUGE_VAL;
     tdv_status st_all = time_tiles(best, best_t);
-    // coordinate descent over the tile shapes, one axis at a time; besides
-    // fixed sizes, the sizes that give the largest pair one tile per SM
     int wmax = 1, hmax = 1;
     for (const auto& p : b->pairs) {
         wmax = std::max(wmax, p.W);
         hmax = std::max(hmax, p.H);
     }
-    const int g_fit = std::min(24, std::max(1, (wmax + b->grid - 1) / b->grid));
-    const int r_fit = std::min(24, std::max(1, (hmax + b->grid - 1) / b->grid));
-    const int Gs[] = {8, 12, 16, 20, 24, g_fit};
-    const int Rs[] = {4, 6, 8, 12, 16, 24, r_fit};
-    for (int axis = 0; axis < 4 && st_all == TDV_OK; axis++) {
-        const int n = axis == 0 ? 6 : (axis == 1 ? 7 : 2);
-        for (int j = 0; j < n && st_all == TDV_OK; j++) {
-            tdv_batch_tiles t = best;
-            if (axis == 0) t.lines_per_cta = Gs[j];
-            else if (axis == 1) t.rows_per_cta = Rs[j];
-            else if (axis == 2) t.split_disparity = j;
-            else t.order = j;
-            if (memcmp(&t, &best, sizeof(t)) == 0) continue;
-            double ms;
-            st_all = time_tiles(t, ms);
-            if (st_all == TDV_OK && ms < best_t) {
-                best_t = ms;
-                best = t;
+    // one coordinate descent per blocks-per-SM setting (it bounds the lines
+    // and rows a block can take), over lines, rows, split and queue order;
+    // besides fixed sizes, the sizes that give the largest pair one tile per
+    // block slot
+    for (int ctas = 1; ctas <= 2 && st_all == TDV_OK; ctas++) {
+        tdv_batch_tiles cur = b->tiles;
+        cur.ctas_per_sm = ctas;
+        double cur_t;
+        st_all = time_tiles(cur, cur_t);
+        const int slots = ctas * b->grid;
+        const int g_fit = std::min(24, std::max(1, (wmax + slots - 1) / slots));
+        const int r_fit = std::min(24, std::max(1, (hmax + slots - 1) / slots));
+        const int Gs[] = {8, 12, 16, 20, 24, g_fit};
+        const int Rs[] = {4, 6, 8, 12, 16, 24, r_fit};
+        for (int axis = 0; axis < 4 && st_all == TDV_OK; axis++) {
+            const int n = axis == 0 ? 6 : (axis == 1 ? 7 : 2);
+            for (int j = 0; j < n && st_all == TDV_OK; j++) {
+                tdv_batch_tiles t = cur;
+                if (axis == 0) t.lines_per_cta = Gs[j];
+                else if (axis == 1) t.rows_per_cta = Rs[j];
+                else if (axis == 2) t.split_disparity = j;
+                else t.order = j;
+                if (memcmp(&t, &cur, sizeof(t)) == 0) continue;
+                double ms;
+                st_all = time_tiles(t, ms);
+                if (st_all == TDV_OK && ms < cur_t) {
+                    cur_t = ms;
+                    cur = t;
+                }
             }
+        }
+        if (st_all == TDV_OK && cur_t < best_t) {
+            best_t = cur_t;
+            best = cur;
         }
     }
     cudaEventDestroy(e0);

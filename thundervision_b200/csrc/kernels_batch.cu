@@ -32,7 +32,9 @@ namespace tdv {
 namespace {
 
 constexpr int kPasses = 9;  // prep, V+, V-, D1+, D1-, D2+, D2-, H+, H-(WTA)
-constexpr int kBatchWarps = kMaxG + 1;
+constexpr int kBatchWarps = kMaxG + 1;  // one block per SM
+constexpr int kBatchWarps2 = 13;        // two blocks per SM
+constexpr int kSmemBudget2 = 110 * 1024;  // dynamic shared memory per block at two per SM
 constexpr int kPrepPixels = 16384;  // pixels per prep item
 constexpr int kCtlHeader = 4;       // ints: queue head, error word, 2 spare
 
@@ -105,9 +107,10 @@ __device__ __forceinline__ void run_h(const BPair& P, int dx, int blk, unsigned 
     }
 }
 
-// one 800-thread block per SM (the register budget this bound leaves is what
-// the launch can hold)
-__global__ void __launch_bounds__(kBatchWarps * 32, 1)
+// NW warps per block: one 800-thread block per SM (NW = 25) or two 416-thread
+// blocks per SM (NW = 13), each taking its own work items
+template <int NW>
+__global__ void __launch_bounds__(NW * 32, NW == kBatchWarps ? 1 : 2)
     batch_kernel(const BPair* __restrict__ pairs, int npairs, const BItem* __restrict__ items, int nitems,
                  int* ctl, unsigned long long wait_ns) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -209,6 +212,9 @@ const char* batch_plan(const std::vector<BatchPairArgs>& pairs, int p1h, int p2h
     const int n = (int)pairs.size();
     if (t.lines_per_cta < 1 || t.lines_per_cta > kMaxG) return "lines_per_cta must be in [1, 24]";
     if (t.rows_per_cta < 1 || t.rows_per_cta > kBatchWarps) return "rows_per_cta must be in [1, 25]";
+    if (t.ctas_per_sm != 1 && t.ctas_per_sm != 2) return "ctas_per_sm must be 1 or 2";
+    const int NW = t.ctas_per_sm == 2 ? kBatchWarps2 : kBatchWarps;
+    const int budget = t.ctas_per_sm == 2 ? kSmemBudget2 : kSmemBudget;
     std::vector<BPair> hp(n);
     out.ctl_off = 0;
     int smem = 0;
@@ -244,9 +250,9 @@ const char* batch_plan(const std::vector<BatchPairArgs>& pairs, int p1h, int p2h
         P.R = a.R;
 
         // vertical / diagonal: G lines per item
-        int G = std::min(t.lines_per_cta, std::max(a.W, 1));
-        while (G > 1 && vd_smem_bytes(G, P.ppl) > kSmemBudget) G--;
-        if (vd_smem_bytes(G, P.ppl) > kSmemBudget) return "vertical pass tile does not fit in shared memory";
+        int G = std::min(std::min(t.lines_per_cta, NW - 1), std::max(a.W, 1));
+        while (G > 1 && vd_smem_bytes(G, P.ppl) > budget) G--;
+        if (vd_smem_bytes(G, P.ppl) > budget) return "vertical pass tile does not fit in shared memory";
         P.G = G;
         smem = std::max(smem, vd_smem_bytes(G, P.ppl));
         // horizontal: rows per item; the L-R rows only in the last pass
@@ -255,17 +261,17 @@ const char* batch_plan(const std::vector<BatchPairArgs>& pairs, int p1h, int p2h
         int rows = t.rows_per_cta;
         if (P.hsplit) {
             const int ph = P.ppl / 2;
-            rows = std::min(rows, std::min(kBatchWarps / 2, kMaxRowsH2 * 2 - 1));
+            rows = std::min(rows, std::min(NW / 2, kMaxRowsH2 * 2 - 1));
             P.hwb = h2_warp_bytes(ph);
             P.hrb = h2_row_bytes(lr, a.W);
-            while (rows > 1 && rows * (2 * P.hwb + P.hrb) > kSmemBudget) rows--;
-            if (rows * (2 * P.hwb + P.hrb) > kSmemBudget) return "horizontal pass tile does not fit in shared memory";
+            while (rows > 1 && rows * (2 * P.hwb + P.hrb) > budget) rows--;
+            if (rows * (2 * P.hwb + P.hrb) > budget) return "horizontal pass tile does not fit in shared memory";
             smem = std::max(smem, rows * (2 * P.hwb + P.hrb));
         } else {
             // producer-fed rows: one consumer warp per row plus the producer warp
-            rows = std::min(rows, kBatchWarps - 1);
-            while (rows > 1 && hp_smem_bytes(rows, P.ppl, lr, a.W, false) > kSmemBudget) rows--;
-            if (hp_smem_bytes(rows, P.ppl, lr, a.W, false) > kSmemBudget)
+            rows = std::min(rows, NW - 1);
+            while (rows > 1 && hp_smem_bytes(rows, P.ppl, lr, a.W, false) > budget) rows--;
+            if (hp_smem_bytes(rows, P.ppl, lr, a.W, false) > budget)
                 return "horizontal pass tile does not fit in shared memory";
             smem = std::max(smem, hp_smem_bytes(rows, P.ppl, lr, a.W, false));
         }
@@ -328,6 +334,7 @@ const char* batch_plan(const std::vector<BatchPairArgs>& pairs, int p1h, int p2h
     out.n_pairs = n;
     out.n_items = (int)items.size();
     out.smem = smem;
+    out.ctas_per_sm = t.ctas_per_sm;
     out.pairs_off = align256(batch_ctl_bytes(n));
     out.items_off = out.pairs_off + align256(sizeof(BPair) * n);
     out.bytes = out.items_off + sizeof(BItem) * items.size();
@@ -338,21 +345,32 @@ const char* batch_plan(const std::vector<BatchPairArgs>& pairs, int p1h, int p2h
     return nullptr;
 }
 
-cudaError_t batch_configure(const BatchPlan& plan) {
+template <int NW>
+cudaError_t configure_nw(const BatchPlan& plan) {
     cudaFuncAttributes fa;
-    cudaError_t e = cudaFuncGetAttributes(&fa, batch_kernel);
+    cudaError_t e = cudaFuncGetAttributes(&fa, batch_kernel<NW>);
     if (e != cudaSuccess) return e;
-    if (fa.maxThreadsPerBlock < kBatchWarps * 32) return cudaErrorInvalidConfiguration;
-    return cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, plan.smem);
+    if (fa.maxThreadsPerBlock < NW * 32) return cudaErrorInvalidConfiguration;
+    return cudaFuncSetAttribute(batch_kernel<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, plan.smem);
+}
+
+cudaError_t batch_configure(const BatchPlan& plan) {
+    return plan.ctas_per_sm == 2 ? configure_nw<kBatchWarps2>(plan) : configure_nw<kBatchWarps>(plan);
 }
 
 cudaError_t batch_launch(const BatchPlan& plan, unsigned char* d_desc, unsigned long long wait_ns, int grid,
                          cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(d_desc + plan.ctl_off, 0, batch_ctl_bytes(plan.n_pairs), st);
     if (e != cudaSuccess) return e;
-    batch_kernel<<<grid, kBatchWarps * 32, plan.smem, st>>>(
-        (const BPair*)(d_desc + plan.pairs_off), plan.n_pairs, (const BItem*)(d_desc + plan.items_off),
-        plan.n_items, (int*)(d_desc + plan.ctl_off), wait_ns);
+    const BPair* pairs = (const BPair*)(d_desc + plan.pairs_off);
+    const BItem* items = (const BItem*)(d_desc + plan.items_off);
+    int* ctl = (int*)(d_desc + plan.ctl_off);
+    if (plan.ctas_per_sm == 2)
+        batch_kernel<kBatchWarps2><<<2 * grid, kBatchWarps2 * 32, plan.smem, st>>>(pairs, plan.n_pairs, items,
+                                                                                   plan.n_items, ctl, wait_ns);
+    else
+        batch_kernel<kBatchWarps><<<grid, kBatchWarps * 32, plan.smem, st>>>(pairs, plan.n_pairs, items,
+                                                                             plan.n_items, ctl, wait_ns);
     return cudaGetLastError();
 }
 

@@ -209,7 +209,7 @@ using BatchTiles = tdv_batch_tiles;
 struct BatchPlan {
     std::vector<unsigned char> desc;
     size_t ctl_off = 0, pairs_off = 0, items_off = 0, bytes = 0;
-    int n_pairs = 0, n_items = 0, smem = 0, item_bytes = 0;
+    int n_pairs = 0, n_items = 0, smem = 0, item_bytes = 0, ctas_per_sm = 1;
 };
 int batch_passes();
 int batch_threads();

@@ -95,7 +95,7 @@ class VideoLoop:
                       torch.empty((H, W), dtype=torch.uint8, device=device)) for _ in range(2)]
         self.batches = [api.Batch(ctx, [(l, r, D, lr)], p1, p2, paths=paths) for (l, r) in self.bufs]
         if autotune:
-            tiles, _ = self.batches[0].autotune(reps=2)
+            tiles, _ = self.batches[0].autotune(reps=5)
             self.batches[1].set_tiles(**tiles)
             self.tiles = tiles
         else:
