@@ -319,6 +319,36 @@ def measure_soft(ctx, dev, reps=5):
             "ratio_vs_plain_forward": t_fb / t_f, "ratio_vs_hard_sgm": t_fb / t_h}
 
 
+def measure_plain(ctx, dev, reps=3):
+    """The drop-in stage chain a reference user calls (the plain method):
+    BT cost DSI in the reference's layout from [0,1] float images (tdv_cost),
+    then SGM + WTA with the reference's path table, GPU semantics and P2
+    divided by the intensity step (tdv_sgm, P1 = 30/255, P2 = 150/255), at
+    640x480, D=64 and 1920x1080, D=256; device time per pair."""
+    import torch
+
+    from thundervision_b200 import synthetic
+    st = torch.cuda.current_stream()
+    out = {}
+    for (w, h, d) in ((640, 480, 64), (1920, 1080, 256)):
+        l, r, _, _ = synthetic.pair_sized(w, h, d, 3)
+        lf = torch.from_numpy(l).to(dev).float() * (1.0 / 255.0)
+        rf = torch.from_numpy(r).to(dev).float() * (1.0 / 255.0)
+        dsi = torch.empty((w, h, d), dtype=torch.float32, device=dev)
+
+        def run():
+            ctx.cost(lf, rf, d, layout="ref", out=dsi)
+            ctx.sgm(dsi, 30.0 / 255.0, 150.0 / 255.0, guide=lf, p2_mode="adjust", table="ref",
+                    semantics="ref_gpu", layout="ref")
+
+        ms = _event_ms(run, reps, 1, st)
+        out[f"{w}x{h}_D{d}"] = {"ms": ms, "fps": 1000.0 / ms, "gcells_per_s": w * h * d * 8 / (ms / 1000.0) / 1e9}
+        del dsi
+    out["workload"] = ("tdv_cost (BT, REF_WHD, [0,1] floats) + tdv_sgm (REF table, REF_GPU semantics, "
+                       "P2 adjusted, 8 paths) + WTA")
+    return out
+
+
 def measure_video(ctx, dev, n_frames=300, refit_steps=50):
     """Full-HD video: 300 frames (12 moving rectangles over a slanted plane,
     sensor noise sigma 2), D=256, fused BT + SGM + WTA + L-R check, through a
@@ -580,7 +610,8 @@ def run_ours(args):
         "clocks": clocks,
     }
     if not args.no_extras:
-        for key, fn in (("batch", measure_batch), ("soft", measure_soft), ("video", measure_video)):
+        for key, fn in (("batch", measure_batch), ("soft", measure_soft), ("plain", measure_plain),
+                        ("video", measure_video)):
             try:
                 line[key] = fn(ctx, dev)
             except Exception as exc:  # an extra never hides the headline line
