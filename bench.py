@@ -352,9 +352,9 @@ def measure_plain(ctx, dev, reps=3):
 def measure_video(ctx, dev, n_frames=300, refit_steps=50):
     """Full-HD video: 300 frames (12 moving rectangles over a slanted plane,
     sensor noise sigma 2), D=256, fused BT + SGM + WTA + L-R check, through a
-    double-buffered loop of graph-replayed persistent launches with every
-    frame copied from pinned host memory and its map copied back (timed),
-    4-path vs 8-path; then P1/P2 fitted by 50 Adam steps on the soft-argmin L1
+    double-buffered loop of per-frame graph replays (the fused kernels, and
+    beside them the persistent batch kernel) with every frame copied from
+    pinned host memory and its map copied back (timed), 4-path vs 8-path; then P1/P2 fitted by 50 Adam steps on the soft-argmin L1
     loss (FP32 BT volume, adjoint kernels) and the refit vs default accuracy
     of the 8-path maps over all frames."""
     import torch
@@ -375,12 +375,13 @@ def measure_video(ctx, dev, n_frames=300, refit_steps=50):
     res = {"workload": f"{n_frames} frames {W}x{H}, D={D}, moving rectangles, noise sigma 2, "
                        "pinned host in/out, double-buffered, graph replay"}
     for paths in (4, 8):
-        loop = video.VideoLoop(ctx, W, H, D, P1, P2, paths=paths, lr=LR)
-        ms = loop.run(host, out_host)
-        maps = [o.to(dev) for o in out_host]
-        res[f"paths{paths}"] = {"fps": n_frames / (ms / 1000.0), "ms_per_frame": ms / n_frames,
-                                "tiles": loop.tiles, **mean_acc(maps)}
-        loop.close()
+        for engine, key in (("launches", f"paths{paths}"), ("persistent", f"paths{paths}_persistent")):
+            loop = video.VideoLoop(ctx, W, H, D, P1, P2, paths=paths, lr=LR, engine=engine)
+            ms = loop.run(host, out_host)
+            maps = [o.to(dev) for o in out_host]
+            res[key] = {"engine": engine, "fps": n_frames / (ms / 1000.0), "ms_per_frame": ms / n_frames,
+                        **({"tiles": loop.tiles} if loop.tiles else {}), **mean_acc(maps)}
+            loop.close()
     # P1/P2 refit through the adjoint, then the 8-path maps with both settings
     fit_frames = [(l, r, gt.to(torch.int64), occ) for (l, r, gt, occ) in frames[:refit_steps]]
     p1r, p2r, hist = video.refit_penalties(ctx, fit_frames, D, P1, P2, steps=refit_steps)

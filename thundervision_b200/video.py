@@ -7,10 +7,11 @@ per pipeline update, tdvision/devstereomatcher.cpp:36-48).
   texture, rectangle tracks and forward warp, with torch's seeded generators
   for the per-frame noise, so 300 full-HD frames take seconds instead of
   minutes of host time.
-* ``VideoLoop`` -- frames from pinned host memory through one persistent batch
-  launch per frame, replayed from a CUDA graph: the copy of frame t+1 runs on
-  a copy stream while frame t is aggregated (two input buffer sets), and each
-  frame's disparity map is copied back to pinned host memory.
+* ``VideoLoop`` -- frames from pinned host memory through one CUDA graph
+  replay per frame (a persistent batch launch, or the per-frame fused kernels
+  of tdv_stereo_sgm with their two concurrent chains): the copy of frame t+1
+  runs on a copy stream while frame t is aggregated (two input buffer sets),
+  and each frame's disparity map is copied back to pinned host memory.
 * ``refit_penalties`` -- fits P1, P2 by gradient steps on the soft-argmin L1
   loss against ground truth (tdv_soft_sgm_forward / _backward).
 * ``accuracy`` -- bad-pixel rate and density of a disparity map against
@@ -83,35 +84,86 @@ def accuracy(disp, gt, occl, thr=1):
 
 
 class VideoLoop:
-    """Double-buffered frame loop over one persistent batch launch per frame.
+    """Double-buffered frame loop, one CUDA graph replay per frame.
 
+    ``engine="launches"`` (default): each frame is the per-frame fused
+    kernels of tdv_stereo_sgm (two concurrent pass chains), captured into one
+    CUDA graph per buffer set.  ``engine="persistent"``: each frame is one
+    persistent batch launch (tdv_batch_graph_launch, tiles autotuned once).
     ``paths`` 4 or 8; P1/P2 must be multiples of 1/2 (the integer-domain
-    fused path).  ``graph`` replays each buffer set's launch from a CUDA graph.
+    fused path).
     """
 
-    def __init__(self, ctx, W, H, D, p1, p2, paths=8, lr=1, graph=True, autotune=True, device="cuda"):
-        self.ctx, self.graph = ctx, graph
+    def __init__(self, ctx, W, H, D, p1, p2, paths=8, lr=1, graph=True, autotune=True, device="cuda",
+                 engine="launches"):
+        self.ctx, self.graph, self.engine = ctx, graph, engine
         self.bufs = [(torch.empty((H, W), dtype=torch.uint8, device=device),
                       torch.empty((H, W), dtype=torch.uint8, device=device)) for _ in range(2)]
-        self.batches = [api.Batch(ctx, [(l, r, D, lr)], p1, p2, paths=paths) for (l, r) in self.bufs]
-        if autotune:
-            tiles, _ = self.batches[0].autotune(reps=5)
-            self.batches[1].set_tiles(**tiles)
-            self.tiles = tiles
-        else:
-            self.tiles = self.batches[0].tiles
         self.copy_stream = torch.cuda.Stream(device=device)
-        # capture both graphs now, outside any timed loop
+        self.tiles = None
+        if engine == "persistent":
+            self.batches = [api.Batch(ctx, [(l, r, D, lr)], p1, p2, paths=paths) for (l, r) in self.bufs]
+            if autotune:
+                tiles, _ = self.batches[0].autotune(reps=5)
+                self.batches[1].set_tiles(**tiles)
+                self.tiles = tiles
+            else:
+                self.tiles = self.batches[0].tiles
+            self.outputs = [b.outputs[0]["disp"] for b in self.batches]
+        elif engine == "launches":
+            # the graphs hold the context's scratch pointers: a private
+            # context keeps other callers from growing (reallocating) them
+            self.batches = []
+            idx = torch.device(device).index
+            ctx = self.ctx = self._own_ctx = api.Context(torch.cuda.current_device() if idx is None else idx)
+            ctx.reserve(W, H, D)
+            self.outputs = [torch.empty((H, W), dtype=torch.uint16, device=device) for _ in range(2)]
+            prm = api.L.tdv_sgm_params(float(p1), float(p2), api.L.P2_CONST, paths, api.L.TABLE_FULL,
+                                       api.L.SEM_STANDARD)
+            calls = []
+            for (l, r), o in zip(self.bufs, self.outputs):
+                calls.append((api._image(l), api._image(r), api.L.tdv_disparity(o.data_ptr(), None, None,
+                                                                                 -1 if lr is None else lr)))
+            self._prm, self._calls, self._D = prm, calls, D
+            self._graphs = [None, None]
+            if graph:
+                cs = torch.cuda.Stream(device=device)
+                for b in range(2):
+                    with torch.cuda.stream(cs):
+                        self._call(b)  # first use: kernel attributes, scratch (outside the capture)
+                    torch.cuda.synchronize()
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(g, stream=cs):
+                        self._call(b)
+                    self._graphs[b] = g
+        else:
+            raise ValueError("engine must be 'persistent' or 'launches'")
+        # first launches (graph captures) now, outside any timed loop
         for b in range(2):
             self._launch(b)
         torch.cuda.synchronize()
 
+    def _call(self, b):
+        import ctypes
+        li, ri, o = self._calls[b]
+        self.ctx.check(api.L.lib().tdv_stereo_sgm(self.ctx.handle, ctypes.byref(li), ctypes.byref(ri), self._D,
+                                                  ctypes.byref(self._prm), ctypes.byref(o), api._stream()))
+
     def close(self):
         for b in self.batches:
             b.close()
+        if self.engine == "launches":
+            torch.cuda.synchronize()
+            self._graphs = [None, None]
+            self._own_ctx.close()
 
     def _launch(self, b):
-        (self.batches[b].graph_launch if self.graph else self.batches[b].run)()
+        if self.engine == "persistent":
+            (self.batches[b].graph_launch if self.graph else self.batches[b].run)()
+        elif self._graphs[b] is not None:
+            self._graphs[b].replay()
+        else:
+            self._call(b)
 
     def run(self, host_frames, host_out):
         """host_frames: list of pinned (left, right) uint8 tensors; host_out:
@@ -144,12 +196,14 @@ class VideoLoop:
                 upload(t + 1)
             ks.wait_event(copied[b])
             self._launch(b)
-            host_out[t].copy_(self.batches[b].outputs[0]["disp"], non_blocking=True)
+            host_out[t].copy_(self.outputs[b], non_blocking=True)
             done[b].record(ks)
         t1.record(ks)
         t1.synchronize()
         for b in self.batches:
             b.status()
+        if self.engine == "launches":
+            self.ctx.device_status()
         return t0.elapsed_time(t1)
 
     def disparity(self, left, right):
@@ -157,7 +211,7 @@ class VideoLoop:
         self.bufs[0][0].copy_(left)
         self.bufs[0][1].copy_(right)
         self._launch(0)
-        return self.batches[0].outputs[0]["disp"]
+        return self.outputs[0]
 
 
 def refit_penalties(ctx, frames, max_disp, p1, p2, steps=50, lr=0.05, tau=1.0, paths=8, checkpoint=32):
