@@ -46,6 +46,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "tdv_internal.hpp"
 
@@ -277,6 +278,15 @@ struct Vec<4> {
         v[3] = t.w;
     }
 };
+
+// Compile-time loop: f(integral_constant<int, I>) for I in [I0, N).
+template <int I, int N, typename F>
+__device__ __forceinline__ void static_for(F&& f) {
+    if constexpr (I < N) {
+        f(std::integral_constant<int, I>{});
+        static_for<I + 1, N>(f);
+    }
+}
 
 // BT of one disparity pair from a left entry and a right entry.
 __device__ __forceinline__ uint32_t bt_pair(const uint4& lp, const uint4& rp) {
@@ -875,126 +885,208 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
         uint16_t* rowL = (uint16_t*)(cring + kChunkSlots * kChunkBytes);
         uint16_t* rowR = rowL + W;
         const int base_d = lane * 2 * PPL;
-        const bool edge_lane = base_d + 2 * PPL > k.D;
-        uint32_t L[PPL], m = 0, sv[PPL];
-        uint32_t P[NJ];
-        uint32_t dpair[PPL];  // (d, d+1) of each pair, u16 halves
-#pragma unroll
-        for (int q = 0; q < PPL; q++) {
-            L[q] = 0;
-            dpair[q] = (uint32_t)(base_d + 2 * q) | ((uint32_t)(base_d + 2 * q + 1) << 16);
-        }
-#pragma unroll
-        for (int j = 0; j < NJ; j++) P[j] = FULL;
-        uint32_t* sg = k.S + ((size_t)y * W + (dx > 0 ? 0 : W - 1)) * k.Dp2 + lane * PPL;
-        const long long sstep = (long long)dx * k.Dp2;
-        int waited = dx > 0 ? -1 : c0 + 1;  // last chunk waited for
-        int rel = c0;                       // next chunk to release
-        bool ok = true;
+        constexpr int NR = kChunkSlots * kChunk;  // right-plane entries in the chunk ring
+        static_assert(8 % NJ == 0, "the window ring must divide the 8-step unroll");
 
-        auto step = [&](int x, const unsigned char* slot, int xlo) {
-            const uint4 lp = *(const uint4*)(slot + LPOFF + (x - xlo) * 16);
-            uint32_t c[PPL], Ln[PPL];
-            const int eb = x - base_d;
+        // One walk of the row in direction DXP (x increasing) with the
+        // left-right chain on or off.  Lane l at column x needs the
+        // right-plane entries x - base_d - o, o in [0, NJ) (pair q uses
+        // o = 2q); they sit in a register window, a ring of NJ entries, and
+        // slide one entry per step: the entry a lane no longer needs is the
+        // one its neighbour needs next (one shuffle), and the edge lane
+        // (lane 0 walking right, lane 31 walking left) loads the entry that
+        // enters the warp's window.  Steps run eight at a time (two S slots)
+        // so that every ring position is a compile-time index.
+        auto consume = [&](auto dxc, auto lrc) -> bool {
+            constexpr bool DXP = decltype(dxc)::value;
+            constexpr bool LR = decltype(lrc)::value;
+            uint32_t L[PPL], m = 0;
+            uint32_t WI[NJ], WN[NJ], WX[NJ];  // window: I, half-sample min, half-sample max
+            uint32_t P[NJ];                   // right-view chain (ring, logical j at (T + j) % NJ)
+            uint32_t dpair[PPL];              // (d, d+1) of each pair, u16 halves
 #pragma unroll
             for (int q = 0; q < PPL; q++) {
-                const int e = max(eb - 2 * q, 0);
-                c[q] = bt_pair(lp, *(const uint4*)(cring + ppos(e & (kChunkSlots * kChunk - 1)) * 16));
+                L[q] = 0;
+                dpair[q] = (uint32_t)(base_d + 2 * q) | ((uint32_t)(base_d + 2 * q + 1) << 16);
             }
-            if (edge_lane || eb < 2 * PPL) {
-                const int lim = min(x + 1, k.D);
 #pragma unroll
-                for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
+            for (int j = 0; j < NJ; j++) {
+                WI[j] = WN[j] = WX[j] = 0;
+                P[j] = FULL;
             }
-            recur<PPL>(L, m, c, Ln, lane, k);
-            Vec<PPL>::lds((const uint32_t*)(slot + (x - xlo) * SB) + lane * PPL, sv);
-#pragma unroll
-            for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
-            if (TWO) {
-                uint32_t s2[PPL];
-                Vec<PPL>::lds((const uint32_t*)(slot + kHpU * SB + (x - xlo) * SB) + lane * PPL, s2);
-#pragma unroll
-                for (int q = 0; q < PPL; q++) sv[q] += s2[q];
-            }
-            if (MODE == 1) {
-                Vec<PPL>::st(sg, sv);
-            } else {
-                // WTA key (S << 8 | d): lowest S, then lowest d (tdvision/wtacpu.cpp:26-30);
-                // one byte permute per key from S and the lane's (d, d+1) register
-                uint32_t key[NJ];
+            const bool loader = DXP ? lane == 0 : lane == 31;
+            uint32_t* sg = k.S + ((size_t)y * W + (DXP ? 0 : W - 1)) * k.Dp2 + lane * PPL;
+            const long long sstep = (long long)(DXP ? 1 : -1) * k.Dp2;
+            int waited = DXP ? -1 : c0 + 1;  // last chunk waited for
+            int rel = c0;                    // next chunk to release
+            auto ring_entry = [&](int e) { return *(const uint4*)(cring + ppos(e & (NR - 1)) * 16); };
+
+            // release the chunks the walk has left, wait for those group j reaches
+            auto chunks_for = [&](int j) -> bool {
+                const int xlo = group_lo(j), xhi = group_hi(j);
+                bool good = true;
+                if (DXP) {
+                    const int lo = cl_of(xlo), need = xhi >> 6;
+                    if (lane == 0)
+                        for (; rel < lo; rel++) mbar_arrive(emptyC(r, rel & (kChunkSlots - 1)));
+                    while (good && waited < need) {
+                        waited++;
+                        good = mbar_wait(fullC(r, waited & (kChunkSlots - 1)), (uint32_t)(waited / kChunkSlots) & 1u);
+                    }
+                } else {
+                    // the edge lane loads entry x - DSPAN + 1, one below the window
+                    const int hi = xhi >> 6, need = max(0, xlo - DSPAN + 1) >> 6;
+                    if (lane == 0)
+                        for (; rel > hi; rel--) mbar_arrive(emptyC(r, rel & (kChunkSlots - 1)));
+                    while (good && waited > need) {
+                        waited--;
+                        good = mbar_wait(fullC(r, waited & (kChunkSlots - 1)),
+                                         (uint32_t)((c0 - waited) / kChunkSlots) & 1u);
+                    }
+                }
+                return good;
+            };
+
+            // window position T (mod 8); MASK: cells with d > x or d >= D may occur
+            auto step = [&](auto Tc, auto Mc, int x, const unsigned char* slot, int xo) {
+                constexpr int T = decltype(Tc)::value;
+                constexpr bool MASK = decltype(Mc)::value;
+                constexpr int N = T % NJ;
+                {
+                    uint32_t vi, vn, vx;
+                    if (DXP) {
+                        vi = __shfl_up_sync(FULL, WI[N], 1);
+                        vn = __shfl_up_sync(FULL, WN[N], 1);
+                        vx = __shfl_up_sync(FULL, WX[N], 1);
+                    } else {
+                        vi = __shfl_down_sync(FULL, WI[N], 1);
+                        vn = __shfl_down_sync(FULL, WN[N], 1);
+                        vx = __shfl_down_sync(FULL, WX[N], 1);
+                    }
+                    if (loader) {
+                        const uint4 v = ring_entry(DXP ? x : max(x - DSPAN + 1, 0));
+                        vi = v.x;
+                        vn = v.y;
+                        vx = v.z;
+                    }
+                    WI[N] = vi;
+                    WN[N] = vn;
+                    WX[N] = vx;
+                }
+                const uint4 lp = *(const uint4*)(slot + LPOFF + xo * 16);
+                uint32_t c[PPL], Ln[PPL], sv[PPL];
 #pragma unroll
                 for (int q = 0; q < PPL; q++) {
-                    key[2 * q] = __byte_perm(sv[q], dpair[q], 0x5104);
-                    key[2 * q + 1] = __byte_perm(sv[q], dpair[q], 0x7326);
+                    const int w = DXP ? ((T - 2 * q) % NJ + NJ) % NJ : (T + 2 * q + 1) % NJ;
+                    c[q] = bt_pair(lp, make_uint4(WI[w], WN[w], WX[w], 0u));
                 }
-                uint32_t kmin = key[0];
+                if (MASK) {
+                    const int lim = min(x + 1, k.D);
 #pragma unroll
-                for (int j = 1; j < NJ; j++) kmin = min(kmin, key[j]);
-                kmin = __reduce_min_sync(FULL, kmin);
-                if (lr) {
+                    for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
+                }
+                recur<PPL>(L, m, c, Ln, lane, k);
+                Vec<PPL>::lds((const uint32_t*)(slot + xo * SB) + lane * PPL, sv);
 #pragma unroll
-                    for (int j = 0; j < NJ; j++) P[j] = min(P[j], key[j]);
-                    uint32_t in = __shfl_down_sync(FULL, P[0], 1);
-                    if (lane == 31) in = FULL;
-                    if (lane == 0) {
-                        rowR[x] = (uint16_t)(P[0] & 0xFFu);
-                        rowL[x] = (uint16_t)(kmin & 0xFFu);
+                for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
+                if (TWO) {
+                    uint32_t s2[PPL];
+                    Vec<PPL>::lds((const uint32_t*)(slot + kHpU * SB + xo * SB) + lane * PPL, s2);
+#pragma unroll
+                    for (int q = 0; q < PPL; q++) sv[q] += s2[q];
+                }
+                if (MODE == 1) {
+                    Vec<PPL>::st(sg, sv);
+                } else {
+                    // WTA key (S << 8 | d): lowest S, then lowest d (tdvision/wtacpu.cpp:26-30);
+                    // one byte permute per key from S and the lane's (d, d+1) register
+                    uint32_t key[NJ];
+#pragma unroll
+                    for (int q = 0; q < PPL; q++) {
+                        key[2 * q] = __byte_perm(sv[q], dpair[q], 0x5104);
+                        key[2 * q + 1] = __byte_perm(sv[q], dpair[q], 0x7326);
                     }
+                    uint32_t kmin = key[0];
 #pragma unroll
-                    for (int j = 0; j < NJ - 1; j++) P[j] = P[j + 1];
-                    P[NJ - 1] = in;
-                } else if (lane == 0) {
-                    const size_t o = (size_t)y * W + x;
-                    const uint16_t dl = (uint16_t)(kmin & 0xFFu);
-                    if (k.disp) k.disp[o] = dl;
-                    if (k.disp_norm) k.disp_norm[o] = __fdiv_rn((float)dl, (float)k.D);
+                    for (int j = 1; j < NJ; j++) kmin = min(kmin, key[j]);
+                    kmin = __reduce_min_sync(FULL, kmin);
+                    if (LR) {
+                        // logical P[j] (right pixel x - base_d - j) at ring position (T + j) % NJ
+#pragma unroll
+                        for (int j = 0; j < NJ; j++) P[(T + j) % NJ] = min(P[(T + j) % NJ], key[j]);
+                        uint32_t in = __shfl_down_sync(FULL, P[N], 1);
+                        if (lane == 31) in = FULL;
+                        if (lane == 0) {
+                            rowR[x] = (uint16_t)(P[N] & 0xFFu);
+                            rowL[x] = (uint16_t)(kmin & 0xFFu);
+                        }
+                        P[N] = in;
+                    } else if (lane == 0) {
+                        const size_t o = (size_t)y * W + x;
+                        const uint16_t dl = (uint16_t)(kmin & 0xFFu);
+                        if (k.disp) k.disp[o] = dl;
+                        if (k.disp_norm) k.disp_norm[o] = __fdiv_rn((float)dl, (float)k.D);
+                    }
+                }
+                sg += sstep;
+#pragma unroll
+                for (int q = 0; q < PPL; q++) L[q] = Ln[q];
+                m = warp_min_pairs<PPL>(L);
+            };
+
+            // group j at window positions T0 .. T0+3: wait, run, release its slot
+            auto group = [&](auto T0c, int j) -> bool {
+                constexpr int T0 = decltype(T0c)::value;
+                const int s = j % kHpSlots;
+                bool good = chunks_for(j);
+                good = good && mbar_wait(fullS(r, s), (uint32_t)(j / kHpSlots) & 1u);
+                if (!__all_sync(FULL, good)) return false;
+                const unsigned char* slot = wbase + s * SLOT;
+                const int xlo = group_lo(j), xhi = group_hi(j), n = xhi - xlo + 1;
+                if (n == kHpU && xlo >= DSPAN && k.D >= DSPAN) {
+                    static_for<0, kHpU>([&](auto ic) {
+                        constexpr int i = decltype(ic)::value;
+                        step(std::integral_constant<int, T0 + i>{}, std::false_type{}, DXP ? xlo + i : xhi - i, slot,
+                             DXP ? i : kHpU - 1 - i);
+                    });
+                } else {
+                    static_for<0, kHpU>([&](auto ic) {
+                        constexpr int i = decltype(ic)::value;
+                        if (i < n)
+                            step(std::integral_constant<int, T0 + i>{}, std::true_type{}, DXP ? xlo + i : xhi - i, slot,
+                                 DXP ? i : n - 1 - i);
+                    });
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(emptyS(r, s));
+                return true;
+            };
+
+            if (!DXP) {
+                // walking left the window starts full: entries W - base_d - o
+                // (positions of step "x = W"); entries below 0 belong to masked
+                // cells, entry W is dropped before use
+                if (!__all_sync(FULL, chunks_for(0))) return false;
+#pragma unroll
+                for (int o = 0; o < NJ; o++) {
+                    const uint4 v = ring_entry(min(max(W - base_d - o, 0), W - 1));
+                    WI[o % NJ] = v.x;
+                    WN[o % NJ] = v.y;
+                    WX[o % NJ] = v.z;
                 }
             }
-            sg += sstep;
-#pragma unroll
-            for (int q = 0; q < PPL; q++) L[q] = Ln[q];
-            m = warp_min_pairs<PPL>(L);
+            for (int j = 0; j < ngroups; j += 2) {
+                if (!group(std::integral_constant<int, 0>{}, j)) return false;
+                if (j + 1 < ngroups && !group(std::integral_constant<int, kHpU>{}, j + 1)) return false;
+            }
+            return true;
         };
 
-        for (int j = 0; j < ngroups; j++) {
-            const int s = j % kHpSlots;
-            const int xlo = group_lo(j), xhi = group_hi(j);
-            // right-plane chunks: release what the window has left, wait for
-            // what this group's window reaches
-            bool good = true;
-            if (dx > 0) {
-                const int lo = cl_of(xlo), need = xhi >> 6;
-                if (lane == 0)
-                    for (; rel < lo; rel++) mbar_arrive(emptyC(r, rel & (kChunkSlots - 1)));
-                while (good && waited < need) {
-                    waited++;
-                    good = mbar_wait(fullC(r, waited & (kChunkSlots - 1)), (uint32_t)(waited / kChunkSlots) & 1u);
-                }
-            } else {
-                const int hi = xhi >> 6, need = cl_of(xlo);
-                if (lane == 0)
-                    for (; rel > hi; rel--) mbar_arrive(emptyC(r, rel & (kChunkSlots - 1)));
-                while (good && waited > need) {
-                    waited--;
-                    good = mbar_wait(fullC(r, waited & (kChunkSlots - 1)),
-                                     (uint32_t)((c0 - waited) / kChunkSlots) & 1u);
-                }
-            }
-            good = good && mbar_wait(fullS(r, s), (uint32_t)(j / kHpSlots) & 1u);
-            if (!__all_sync(FULL, good)) {
-                ok = false;
-                break;
-            }
-            const unsigned char* slot = wbase + s * SLOT;
-            if (xhi - xlo + 1 == kHpU) {
-#pragma unroll
-                for (int i = 0; i < kHpU; i++) step(dx > 0 ? xlo + i : xhi - i, slot, xlo);
-            } else {
-                for (int i = 0; i <= xhi - xlo; i++) step(dx > 0 ? xlo + i : xhi - i, slot, xlo);
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(emptyS(r, s));
-        }
+        bool ok;
+        if (dx > 0)
+            ok = lr ? consume(std::true_type{}, std::true_type{}) : consume(std::true_type{}, std::false_type{});
+        else
+            ok = lr ? consume(std::false_type{}, std::true_type{}) : consume(std::false_type{}, std::false_type{});
         if (!ok) {
             if (lane == 0) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
         } else if (lr) {

@@ -40,8 +40,10 @@ __global__ void __launch_bounds__((kMaxG + 1) * 32, 1)
     if (j2 >= 0) vd_body<PPL, MODE, DIAG>(k, s, dy, kmin, nlines, G, j2, smem);
 }
 
+constexpr int kHpMaxRows = 16;  // consumer warps per block, horizontal passes
+
 template <int PPL, int MODE, bool TWO>
-__global__ void __launch_bounds__((kMaxG + 1) * 32, 1) hp_pass(FK k, int dx, int R) {
+__global__ void __launch_bounds__((kHpMaxRows + 1) * 32, 1) hp_pass(FK k, int dx, int R) {
     extern __shared__ __align__(128) unsigned char smem[];
     hp_body<PPL, MODE, TWO>(k, dx, R, blockIdx.x, smem);
 }
@@ -158,6 +160,7 @@ cudaError_t launch_hp(const FK& k, int dx, int max_rows, cudaStream_t st) {
     const bool lr = MODE == 2 && k.lr_thr >= 0;
     const int nsm = sm_count();
     int R = (k.H + nsm - 1) / nsm;
+    if (max_rows > kHpMaxRows) max_rows = kHpMaxRows;
     R = R < 1 ? 1 : (R > max_rows ? max_rows : R);
     while (R > 1 && hp_smem_bytes(R, PPL, lr, k.W, TWO) > kSmemBudget) R--;
     const int smem = hp_smem_bytes(R, PPL, lr, k.W, TWO);
