@@ -379,7 +379,7 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
     if (threadIdx.x == 0) {
         for (int b = 0; b < NS; b++) {
             mbar_init(smem_u32(&full[b]), 1);
-            mbar_init(smem_u32(&empty[b]), G);
+            mbar_init(smem_u32(&empty[b]), Gb);  // warps without a line take no part
         }
         fence_mbar_init();
     }
@@ -431,11 +431,10 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
             for (int r = max(0, j - NS); r < j; r++)
                 mbar_wait(smem_u32(&full[r & (NS - 1)]), (uint32_t)(r / NS) & 1u, ok ? kWaitNs : kDrainNs);
         }
-    } else if (warp < G) {
-        // ---- consumers ----
-        const bool has_line = warp < Gb;
+    } else if (warp < Gb) {
+        // ---- consumers: warp w walks line kf + w ----
         const int base_d = lane * 2 * PPL;
-        const bool edge_lane = base_d + 2 * PPL > k.D;  // holds disparities >= D
+        const bool dmask = k.D < DSPAN;  // some lanes hold disparities >= D
         const unsigned char* lp_slot = slots + offL + warp * 16;
         const unsigned char* sv_slot = slots + warp * SB + lane * PPL * 4;
         uint32_t L[PPL], m = 0;
@@ -443,8 +442,6 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
         for (int q = 0; q < PPL; q++) L[q] = 0;
         // vertical (s = 0): column x = kp on every row, offsets computed once
         const int xs = kf + warp;
-        const int ebs = xs - base_d;
-        const bool need_mask_s = edge_lane || ebs < 2 * PPL;
         const int lim_s = min(xs + 1, k.D);
         // right-plane entry e of a row sits at ppos(e - 8*g0v) in the segment
         // (g0v its virtual first group, a multiple of 8 entries below e): for
@@ -457,38 +454,40 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
             cq[q] = DSPAN - 2 + warp - base_d - 2 * q;
             rpos[q] = ppos(cq[q] + ((kf - DSPAN + 2) & 7)) * 16;
         }
-        uint32_t* sg_s = k.S + ((size_t)y0 * k.W + xs) * k.Dp2 + lane * PPL;
-        const long long sstep = (long long)dy * k.W * k.Dp2;
+        // the line's S vector on row y0, and the step to the next row (x moves by s*dy)
+        uint32_t* sg = k.S + ((long long)y0 * k.W + xs + s * y0) * k.Dp2 + lane * PPL;
+        const long long sstep = (long long)dy * (k.W + s) * k.Dp2;
 
-        auto row = [&](int i, int boff) {
+        // CHECK: the row may lie outside the line's span (diagonal) or hold
+        // cells with d > x or d >= D; without it the row is known clean
+        auto row = [&](auto chk, int i, int boff) {
+            constexpr bool CHECK = decltype(chk)::value;
             uint32_t c[PPL], Ln[PPL];
-            uint32_t* sg;
-            const uint4 lp = *(const uint4*)(lp_slot + boff);
             if (!DIAG) {
-                if (!has_line) return;
+                const uint4 lp = *(const uint4*)(lp_slot + boff);
 #pragma unroll
                 for (int q = 0; q < PPL; q++) c[q] = bt_pair(lp, *(const uint4*)(slots + offR + boff + rpos[q]));
-                if (need_mask_s) {
+                if (CHECK) {
 #pragma unroll
                     for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim_s, k.BIGBIG);
                 }
-                sg = sg_s;
-                sg_s += sstep;
             } else {
                 const int y = y0 + dy * i;
                 const int x = xs + s * y;
-                if (!has_line || x < 0 || x >= k.W) return;
+                if (CHECK && (x < 0 || x >= k.W)) {  // uniform: one line per warp
+                    sg += sstep;
+                    return;
+                }
+                const uint4 lp = *(const uint4*)(lp_slot + boff);
                 const int phase = (kf + s * y - DSPAN + 2) & 7;
                 const unsigned char* rseg = slots + boff + offR;
-                const int eb = x - base_d;
 #pragma unroll
                 for (int q = 0; q < PPL; q++) c[q] = bt_pair(lp, *(const uint4*)(rseg + ppos(cq[q] + phase) * 16));
-                if (edge_lane || eb < 2 * PPL) {
+                if (CHECK && (x < DSPAN || dmask)) {
                     const int lim = min(x + 1, k.D);
 #pragma unroll
                     for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
                 }
-                sg = k.S + ((size_t)y * k.W + x) * k.Dp2 + lane * PPL;
             }
             recur<PPL>(L, m, c, Ln, lane, k);  // from L = 0, m = 0 the first step gives L = C
             if (MODE == 0) {
@@ -500,11 +499,14 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
                 for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
                 Vec<PPL>::st(sg, sv);
             }
+            sg += sstep;
 #pragma unroll
             for (int q = 0; q < PPL; q++) L[q] = Ln[q];
             m = warp_min_pairs<PPL>(L);
         };
 
+        // a vertical line needs masking on every row or on none
+        const bool vcheck = !DIAG && (xs < DSPAN || dmask);
         for (int j = 0; j < nslots; j++) {
             const int b = j & (NS - 1);
             if (!__all_sync(FULL, mbar_wait(smem_u32(&full[b]), (uint32_t)(j / NS) & 1u))) {
@@ -512,10 +514,21 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
                 break;
             }
             const int boff = b * slotBytes;
-            row(U * j, boff);
+            const bool full_slot = U * j + U <= nrows;
+            bool check = vcheck || !full_slot;
+            if (DIAG) {
+                // x = xs + s*y is monotone over the slot's rows: check its ends
+                const int xa = xs + s * (y0 + dy * (U * j)), xb = xa + s * dy * (U - 1);
+                check = check || min(xa, xb) < DSPAN || max(xa, xb) >= k.W || dmask;
+            }
+            if (!check) {
 #pragma unroll
-            for (int r = 1; r < U; r++)
-                if (U * j + r < nrows) row(U * j + r, boff + r * rowBytes);
+                for (int r = 0; r < U; r++) row(std::false_type{}, U * j + r, boff + r * rowBytes);
+            } else {
+#pragma unroll
+                for (int r = 0; r < U; r++)
+                    if (U * j + r < nrows) row(std::true_type{}, U * j + r, boff + r * rowBytes);
+            }
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&empty[b]));
         }

@@ -27,8 +27,12 @@ struct GroupPairs {
     int16_t second[kMaxPairedBlocks];  // -1: none
 };
 
+// Lines per block, vertical/diagonal passes: at most 15 consumer warps and the
+// producer, so that two blocks (one of each concurrent pass chain) share an SM.
+constexpr int kVdMaxG = 15;
+
 template <int PPL, int MODE, bool DIAG>
-__global__ void __launch_bounds__((kMaxG + 1) * 32, 1)
+__global__ void __launch_bounds__((kVdMaxG + 1) * 32, 2)
     vd_pass(FK k, int s, int dy, int kmin, int nlines, int G, GroupPairs gp, int paired) {
     extern __shared__ __align__(128) unsigned char smem[];
     if (!paired) {
@@ -118,7 +122,7 @@ cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
     GroupPairs gp;
     int paired = 0, blocks = 0;
     int G = (k.W + nsm - 1) / nsm;
-    G = G < 1 ? 1 : (G > kMaxG ? kMaxG : G);
+    G = G < 1 ? 1 : (G > kVdMaxG ? kVdMaxG : G);
     if (DIAG) {
         // smallest G whose paired blocks fit one wave (cached per shape)
         static std::mutex mu;
@@ -128,12 +132,12 @@ cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
         auto it = cache.find(key);
         if (it == cache.end()) {
             int g = G, nb = -1;
-            for (; g <= kMaxG; g++) {
+            for (; g <= kVdMaxG; g++) {
                 nb = pair_groups(k.W, k.H, s, kmin, nlines, g, gp);
                 if (nb > 0 && nb <= nsm) break;
             }
-            if (g > kMaxG) {
-                g = kMaxG;
+            if (g > kVdMaxG) {
+                g = kVdMaxG;
                 nb = pair_groups(k.W, k.H, s, kmin, nlines, g, gp);
             }
             if (cache.size() > 64) cache.clear();
