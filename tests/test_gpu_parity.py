@@ -147,12 +147,14 @@ def test_fused_medium(ctx, orc, medium_pair, paths):
 @pytest.mark.parametrize("W,H,D", [(640, 96, 128), (640, 96, 256), (1001, 37, 200),
                                    (257, 64, 129), (1920, 24, 256), (777, 19, 65)])
 @pytest.mark.parametrize("lr", [None, 1])
-def test_fused_wide_large_d(ctx, orc, W, H, D, lr):
-    """Disparity ranges above 64 (two or four disparity pairs per lane, the
-    range split over two warps in the horizontal passes) on rows many
-    right-plane chunks long, including widths that are not chunk multiples."""
+@pytest.mark.parametrize("paths", [8, 4])
+def test_fused_wide_large_d(ctx, orc, W, H, D, lr, paths):
+    """Disparity ranges above 64 (two or four disparity pairs per lane) on
+    rows many right-plane chunks long, including widths that are not chunk
+    multiples (a partial last pixel group in the horizontal passes) and
+    ranges that are not multiples of 64 pairs (lanes holding d >= D)."""
     L, R, _, _ = syn.make_pair(W, H, D, W + 7 * H + D, n_rects=4, slanted=True)
-    _check_fused(ctx, orc, L, R, D, 10, 120, 8, lr)
+    _check_fused(ctx, orc, L, R, D, 10, 120, paths, lr)
 
 
 def _check_fused(ctx, orc, L, R, D, p1, p2, paths, lr):

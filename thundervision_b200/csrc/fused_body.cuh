@@ -90,10 +90,11 @@ __host__ __device__ inline int ppl_for(int D) { return D <= 64 ? 1 : (D <= 128 ?
 constexpr int kSmemBudget = 220 * 1024;  // dynamic shared memory per block
 
 // vertical/diagonal pass, G lines: barriers + kRowSlots ring slots of
-// (S chunk, left entries, shared right segment)
+// (S chunk, left entries, shared right segment) + the diagonal offset tables
+// (8 phases x 4 words per warp)
 __host__ __device__ inline int vd_smem_bytes(int G, int ppl) {
     const int NRG = (G + 64 * ppl) / 8 + 2;
-    return 2 * kRowSlots * 8 + kRowSlots * align128(G * 128 * ppl + G * 16 + NRG * kGroupBytes);
+    return 2 * kRowSlots * 8 + kRowSlots * align128(G * 128 * ppl + G * 16 + NRG * kGroupBytes) + G * 128;
 }
 // horizontal pass, one warp per row: barriers, S ring, chunk ring, L-R rows
 __host__ __device__ inline int h_warp_bytes(int ppl, bool lr, int W) {
@@ -454,6 +455,21 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
             cq[q] = DSPAN - 2 + warp - base_d - 2 * q;
             rpos[q] = ppos(cq[q] + ((kf - DSPAN + 2) & 7)) * 16;
         }
+        // With four pairs per lane (base_d = 8 * lane, a whole group of
+        // entries per lane) the offset splits as ppos(phase + C_q) * 16 -
+        // 144 * lane, C_q = DSPAN - 2 + warp - 2q: the first term depends on
+        // the warp, the pair and the row's phase only, so each warp keeps it
+        // in a table of 8 phases x 4 pairs and a diagonal row reads one entry.
+        const uint32_t* tbl = (const uint32_t*)(slots + kRowSlots * rowBytes) + warp * 32;
+        if constexpr (DIAG && PPL == 4) {
+            if (lane < 8) {
+                uint32_t* t = (uint32_t*)(slots + kRowSlots * rowBytes) + warp * 32 + lane * 4;
+#pragma unroll
+                for (int q = 0; q < 4; q++) t[q] = (uint32_t)ppos(lane + DSPAN - 2 + warp - 2 * q) * 16u;
+            }
+            __syncwarp();
+        }
+        const int rlane = offR - 144 * lane;
         // the line's S vector on row y0, and the step to the next row (x moves by s*dy)
         uint32_t* sg = k.S + ((long long)y0 * k.W + xs + s * y0) * k.Dp2 + lane * PPL;
         const long long sstep = (long long)dy * (k.W + s) * k.Dp2;
@@ -480,9 +496,19 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
                 }
                 const uint4 lp = *(const uint4*)(lp_slot + boff);
                 const int phase = (kf + s * y - DSPAN + 2) & 7;
-                const unsigned char* rseg = slots + boff + offR;
+                if constexpr (PPL == 4) {
+                    const uint4 A = *(const uint4*)(tbl + phase * 4);
+                    const unsigned char* rb = slots + (boff + rlane);
+                    c[0] = bt_pair(lp, *(const uint4*)(rb + A.x));
+                    c[1] = bt_pair(lp, *(const uint4*)(rb + A.y));
+                    c[2] = bt_pair(lp, *(const uint4*)(rb + A.z));
+                    c[3] = bt_pair(lp, *(const uint4*)(rb + A.w));
+                } else {
+                    const unsigned char* rseg = slots + boff + offR;
 #pragma unroll
-                for (int q = 0; q < PPL; q++) c[q] = bt_pair(lp, *(const uint4*)(rseg + ppos(cq[q] + phase) * 16));
+                    for (int q = 0; q < PPL; q++)
+                        c[q] = bt_pair(lp, *(const uint4*)(rseg + ppos(cq[q] + phase) * 16));
+                }
                 if (CHECK && (x < DSPAN || dmask)) {
                     const int lim = min(x + 1, k.D);
 #pragma unroll
