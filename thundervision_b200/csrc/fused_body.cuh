@@ -785,14 +785,15 @@ __device__ __forceinline__ void h_body(const FK& k, int dx, int GH, int warp_byt
 // R consumer warps (one image row each, walking x in direction dx) and one
 // producer warp whose lane r keeps row r's rings full, so the consumers carry
 // no copy bookkeeping.  Per row:
-//   * an S ring of kHpSlots slots, each holding kHpU consecutive pixels of
+//   * an S ring of hp_slots(TWO) slots, each holding kHpU consecutive pixels of
 //     the row: their S vectors and their left-plane entries (two TMA bulk
 //     copies per slot); a consumer waits once per kHpU steps and releases the
 //     slot (mbarrier arrive) when it has read it;
-//   * a right-plane chunk ring of kChunkSlots chunks of kChunk entries, chunk
-//     c in slot c & 7; the consumer releases a chunk when its disparity
-//     window [x - 64*PPL + 2, x] has left it, the producer refills the slot
-//     with the chunk 8 places further in walk order.
+//   * a right-plane chunk ring of kHpChunkSlots chunks of kChunk entries,
+//     chunk c in slot c & 3, read only by the lane that loads the entry
+//     entering the warp's register window; the consumer releases a chunk
+//     once the loads have passed it, the producer refills the slot with the
+//     chunk 4 places further in walk order.
 // The producer lanes never block: each polls its own row's empty barriers and
 // issues what has become free; the warp sleeps briefly when no lane could
 // issue and gives up (TDV_ERR_TIMEOUT) after kWaitNs without progress.
@@ -801,9 +802,12 @@ __device__ __forceinline__ void h_body(const FK& k, int dx, int GH, int warp_byt
 // TWO: the pass joins two volumes filled by concurrent pass chains, k.S and
 // k.S2 (read-only): a slot also holds the S2 vectors, and the pass stores
 // S + S2 + L into k.S.
-constexpr int kHpU = 4;      // pixels per S slot
-constexpr int kHpSlots = 4;  // S slots per row
-constexpr int kHpBars = 2 * kHpSlots + 2 * kChunkSlots;
+constexpr int kHpU = 4;           // pixels per S slot
+constexpr int kHpChunkSlots = 4;  // right-plane chunks per row (power of 2)
+// S slots per row: one row's S (and S2) bytes in flight; the two-volume pass
+// has twice the bytes per slot
+__host__ __device__ constexpr int hp_slots(bool two) { return two ? 5 : 6; }
+__host__ __device__ constexpr int hp_bars(bool two) { return 2 * hp_slots(two) + 2 * kHpChunkSlots; }
 
 // slot: [S vectors of kHpU pixels][S2 vectors (TWO)][left-plane entries],
 // padded to 128 bytes so every slot's vectors start on a 128-byte line
@@ -811,15 +815,18 @@ __host__ __device__ inline int hp_slot_bytes(int ppl, bool two) {
     return align128(kHpU * (128 * ppl * (two ? 2 : 1) + 16));
 }
 __host__ __device__ inline int hp_warp_bytes(int ppl, bool lr, int W, bool two) {
-    return align128(kHpSlots * hp_slot_bytes(ppl, two) + kChunkSlots * kChunkBytes + (lr ? 2 * W * 2 : 0));
+    return align128(hp_slots(two) * hp_slot_bytes(ppl, two) + kHpChunkSlots * kChunkBytes + (lr ? 2 * W * 2 : 0));
 }
 __host__ __device__ inline int hp_smem_bytes(int R, int ppl, bool lr, int W, bool two) {
-    return align128(R * kHpBars * 8) + R * hp_warp_bytes(ppl, lr, W, two);
+    return align128(R * hp_bars(two) * 8) + R * hp_warp_bytes(ppl, lr, W, two);
 }
 
 template <int PPL, int MODE, bool TWO>
 __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, unsigned char* smem) {
     constexpr int SB = 128 * PPL;
+    constexpr int NSL = hp_slots(TWO);   // S slots per row
+    constexpr int CS = kHpChunkSlots;    // right-plane chunks per row
+    constexpr int BARS = hp_bars(TWO);
     constexpr int DSPAN = 64 * PPL;
     constexpr int NJ = 2 * PPL;
     constexpr int SLOT = (kHpU * ((TWO ? 2 : 1) * SB + 16) + 127) & ~127;
@@ -829,23 +836,22 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
     const bool lr = MODE == 2 && k.lr_thr >= 0;
     const int wb = hp_warp_bytes(PPL, lr, W, TWO);
     uint64_t* bars = (uint64_t*)smem;
-    unsigned char* data = smem + align128(R * kHpBars * 8);
+    unsigned char* data = smem + align128(R * BARS * 8);
     const int y0 = blk * R;
     const int Rb = min(R, k.H - y0);  // rows of this block
     const int ngroups = (W + kHpU - 1) / kHpU;
     const int nch = (W + kChunk - 1) / kChunk;
     const int c0 = dx > 0 ? 0 : nch - 1;  // first chunk in walk order
-    // row r: fullS[kHpSlots] emptyS[kHpSlots] fullC[8] emptyC[8]
-    auto fullS = [&](int r, int s) { return smem_u32(&bars[r * kHpBars + s]); };
-    auto emptyS = [&](int r, int s) { return smem_u32(&bars[r * kHpBars + kHpSlots + s]); };
-    auto fullC = [&](int r, int s) { return smem_u32(&bars[r * kHpBars + 2 * kHpSlots + s]); };
-    auto emptyC = [&](int r, int s) { return smem_u32(&bars[r * kHpBars + 2 * kHpSlots + kChunkSlots + s]); };
+    // row r: fullS[NSL] emptyS[NSL] fullC[8] emptyC[8]
+    auto fullS = [&](int r, int s) { return smem_u32(&bars[r * BARS + s]); };
+    auto emptyS = [&](int r, int s) { return smem_u32(&bars[r * BARS + NSL + s]); };
+    auto fullC = [&](int r, int s) { return smem_u32(&bars[r * BARS + 2 * NSL + s]); };
+    auto emptyC = [&](int r, int s) { return smem_u32(&bars[r * BARS + 2 * NSL + CS + s]); };
     auto group_lo = [&](int j) { return dx > 0 ? j * kHpU : max(0, W - 1 - j * kHpU - (kHpU - 1)); };
     auto group_hi = [&](int j) { return dx > 0 ? min(W - 1, j * kHpU + kHpU - 1) : W - 1 - j * kHpU; };
-    auto cl_of = [&](int x) { return max(0, x - DSPAN + 2) >> 6; };
 
     if (threadIdx.x == 0) {
-        for (int b = 0; b < R * kHpBars; b++) mbar_init(smem_u32(&bars[b]), 1);
+        for (int b = 0; b < R * BARS; b++) mbar_init(smem_u32(&bars[b]), 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -863,8 +869,8 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
             if (mine) {
                 if (g < ngroups) {
                     pending = true;
-                    const int s = g % kHpSlots;
-                    if (g < kHpSlots || mbar_try(emptyS(lane, s), (uint32_t)((g / kHpSlots) - 1) & 1u)) {
+                    const int s = g % NSL;
+                    if (g < NSL || mbar_try(emptyS(lane, s), (uint32_t)((g / NSL) - 1) & 1u)) {
                         const int xlo = group_lo(g), n = group_hi(g) - xlo + 1;
                         unsigned char* dst = wbase + s * SLOT;
                         const uint32_t bar = fullS(lane, s);
@@ -881,12 +887,12 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                 if (kc < nch) {
                     pending = true;
                     const int c = dx > 0 ? kc : c0 - kc;
-                    const int s = c & (kChunkSlots - 1);
-                    if (kc < kChunkSlots || mbar_try(emptyC(lane, s), (uint32_t)((kc / kChunkSlots) - 1) & 1u)) {
+                    const int s = c & (CS - 1);
+                    if (kc < CS || mbar_try(emptyC(lane, s), (uint32_t)((kc / CS) - 1) & 1u)) {
                         const int ng = min(kChunk / 8, (W + 7) / 8 - c * (kChunk / 8));
                         const uint32_t bar = fullC(lane, s);
                         mbar_expect_tx(bar, (uint32_t)ng * kGroupBytes);
-                        tma_load(smem_u32(wbase + kHpSlots * SLOT + s * kChunkBytes),
+                        tma_load(smem_u32(wbase + NSL * SLOT + s * kChunkBytes),
                                  k.RPp + (size_t)y * k.Wp + 9 * (c * (kChunk / 8)), (uint32_t)ng * kGroupBytes, bar);
                         kc++;
                         did = true;
@@ -907,11 +913,11 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
         // the block must not retire with copies in flight
         if (mine) {
             const uint64_t lim = failed ? kDrainNs : kWaitNs;
-            for (int j = max(0, g - kHpSlots); j < g; j++)
-                mbar_wait(fullS(lane, j % kHpSlots), (uint32_t)(j / kHpSlots) & 1u, lim);
-            for (int q = max(0, kc - kChunkSlots); q < kc; q++) {
+            for (int j = max(0, g - NSL); j < g; j++)
+                mbar_wait(fullS(lane, j % NSL), (uint32_t)(j / NSL) & 1u, lim);
+            for (int q = max(0, kc - CS); q < kc; q++) {
                 const int c = dx > 0 ? q : c0 - q;
-                mbar_wait(fullC(lane, c & (kChunkSlots - 1)), (uint32_t)(q / kChunkSlots) & 1u, lim);
+                mbar_wait(fullC(lane, c & (CS - 1)), (uint32_t)(q / CS) & 1u, lim);
             }
         }
         if (failed && lane == 0) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
@@ -920,11 +926,11 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
         const int r = warp;
         const int y = y0 + r;
         unsigned char* wbase = data + (size_t)r * wb;
-        const unsigned char* cring = wbase + kHpSlots * SLOT;
-        uint16_t* rowL = (uint16_t*)(cring + kChunkSlots * kChunkBytes);
+        const unsigned char* cring = wbase + NSL * SLOT;
+        uint16_t* rowL = (uint16_t*)(cring + CS * kChunkBytes);
         uint16_t* rowR = rowL + W;
         const int base_d = lane * 2 * PPL;
-        constexpr int NR = kChunkSlots * kChunk;  // right-plane entries in the chunk ring
+        constexpr int NR = CS * kChunk;  // right-plane entries in the chunk ring
         static_assert(8 % NJ == 0, "the window ring must divide the 8-step unroll");
 
         // One walk of the row in direction DXP (x increasing) with the
@@ -960,27 +966,39 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
             int rel = c0;                    // next chunk to release
             auto ring_entry = [&](int e) { return *(const uint4*)(cring + ppos(e & (NR - 1)) * 16); };
 
-            // release the chunks the walk has left, wait for those group j reaches
+            // Chunks are waited for in walk order up to the one group j's
+            // edge-lane loads reach, and a chunk is released once it has been
+            // waited for (its copy has landed) and the edge lane has passed it,
+            // so the producer refills slots only after their copies completed.
+            // Walking right the edge lane reads entry x; walking left entry
+            // x - DSPAN + 1 (clamped at 0), so the chunks a group needs are at
+            // most two and a ring of 4 never blocks.
             auto chunks_for = [&](int j) -> bool {
                 const int xlo = group_lo(j), xhi = group_hi(j);
                 bool good = true;
                 if (DXP) {
-                    const int lo = cl_of(xlo), need = xhi >> 6;
-                    if (lane == 0)
-                        for (; rel < lo; rel++) mbar_arrive(emptyC(r, rel & (kChunkSlots - 1)));
+                    const int keep = xlo >> 6, need = xhi >> 6;
+                    auto release = [&]() {
+                        if (lane == 0)
+                            for (; rel < keep && rel <= waited; rel++) mbar_arrive(emptyC(r, rel & (CS - 1)));
+                    };
+                    release();
                     while (good && waited < need) {
                         waited++;
-                        good = mbar_wait(fullC(r, waited & (kChunkSlots - 1)), (uint32_t)(waited / kChunkSlots) & 1u);
+                        good = mbar_wait(fullC(r, waited & (CS - 1)), (uint32_t)(waited / CS) & 1u);
+                        release();
                     }
                 } else {
-                    // the edge lane loads entry x - DSPAN + 1, one below the window
-                    const int hi = xhi >> 6, need = max(0, xlo - DSPAN + 1) >> 6;
-                    if (lane == 0)
-                        for (; rel > hi; rel--) mbar_arrive(emptyC(r, rel & (kChunkSlots - 1)));
+                    const int keep = max(0, xhi - DSPAN + 1) >> 6, need = max(0, xlo - DSPAN + 1) >> 6;
+                    auto release = [&]() {
+                        if (lane == 0)
+                            for (; rel > keep && rel >= waited; rel--) mbar_arrive(emptyC(r, rel & (CS - 1)));
+                    };
+                    release();
                     while (good && waited > need) {
                         waited--;
-                        good = mbar_wait(fullC(r, waited & (kChunkSlots - 1)),
-                                         (uint32_t)((c0 - waited) / kChunkSlots) & 1u);
+                        good = mbar_wait(fullC(r, waited & (CS - 1)), (uint32_t)((c0 - waited) / CS) & 1u);
+                        release();
                     }
                 }
                 return good;
@@ -1076,9 +1094,9 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
             // group j at window positions T0 .. T0+3: wait, run, release its slot
             auto group = [&](auto T0c, int j) -> bool {
                 constexpr int T0 = decltype(T0c)::value;
-                const int s = j % kHpSlots;
+                const int s = j % NSL;
                 bool good = chunks_for(j);
-                good = good && mbar_wait(fullS(r, s), (uint32_t)(j / kHpSlots) & 1u);
+                good = good && mbar_wait(fullS(r, s), (uint32_t)(j / NSL) & 1u);
                 if (!__all_sync(FULL, good)) return false;
                 const unsigned char* slot = wbase + s * SLOT;
                 const int xlo = group_lo(j), xhi = group_hi(j), n = xhi - xlo + 1;
@@ -1103,12 +1121,15 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
 
             if (!DXP) {
                 // walking left the window starts full: entries W - base_d - o
-                // (positions of step "x = W"); entries below 0 belong to masked
-                // cells, entry W is dropped before use
-                if (!__all_sync(FULL, chunks_for(0))) return false;
+                // (positions of step "x = W"), read once from the padded plane in
+                // global memory (the chunk ring only holds what the edge lane
+                // loads); entries below 0 belong to masked cells, entry W is
+                // dropped before use
+                const Plane* rrow = k.RPp + (size_t)y * k.Wp;
 #pragma unroll
                 for (int o = 0; o < NJ; o++) {
-                    const uint4 v = ring_entry(min(max(W - base_d - o, 0), W - 1));
+                    const int e = min(max(W - base_d - o, 0), W - 1);
+                    const uint4 v = __ldcg((const uint4*)(rrow + e + (e >> 3)));
                     WI[o % NJ] = v.x;
                     WN[o % NJ] = v.y;
                     WX[o % NJ] = v.z;
@@ -1144,7 +1165,7 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
     // every role is done with the rings: retire the barriers
     __syncthreads();
     if (threadIdx.x == 0)
-        for (int b = 0; b < R * kHpBars; b++) mbar_inval(smem_u32(&bars[b]));
+        for (int b = 0; b < R * BARS; b++) mbar_inval(smem_u32(&bars[b]));
 }
 
 // ------------------------------------------- horizontal passes, split D
