@@ -31,8 +31,10 @@
 //   thread issues TMA bulk copies (cp.async.bulk) of the S chunk, the left
 //   plane entries and the shared right-plane segment into a ring of shared
 //   memory slots completed by mbarriers.  Horizontal passes give each warp a
-//   row, an S ring and a sliding window of right-plane chunks, also filled by
-//   TMA bulk copies.  Every mbarrier wait is bounded; a wait that runs out
+//   row fed by a producer warp (an S ring and a ring of right-plane chunks,
+//   TMA bulk copies); the right-plane entries a warp's lanes need slide
+//   through a register window, one shuffle and one edge-lane load per step.
+//   Every mbarrier wait is bounded; a wait that runs out
 //   records TDV_ERR_TIMEOUT, waits (bounded) for its copies in flight and
 //   returns.
 //
@@ -57,7 +59,6 @@ namespace {
 constexpr int kMaxG = 24;       // consumer warps per block, vertical/diagonal passes
 constexpr int kRowSlots = 8;    // rows in flight, vertical/diagonal passes (power of 2)
 constexpr int kVdRowsPerSlot = 2;  // rows per ring slot (one wait and one release per slot)
-constexpr int kMaxGH = 8;       // warps per block, horizontal passes
 constexpr int kHSlots = 8;      // S ring depth (steps), horizontal passes
 constexpr int kChunk = 64;      // right-plane entries per horizontal refill
 constexpr int kChunkSlots = 8;  // resident chunks per horizontal warp
@@ -95,10 +96,6 @@ constexpr int kSmemBudget = 220 * 1024;  // dynamic shared memory per block
 __host__ __device__ inline int vd_smem_bytes(int G, int ppl) {
     const int NRG = (G + 64 * ppl) / 8 + 2;
     return 2 * kRowSlots * 8 + kRowSlots * align128(G * 128 * ppl + G * 16 + NRG * kGroupBytes) + G * 128;
-}
-// horizontal pass, one warp per row: barriers, S ring, chunk ring, L-R rows
-__host__ __device__ inline int h_warp_bytes(int ppl, bool lr, int W) {
-    return align128(128 + kHSlots * 128 * ppl + kChunkSlots * kChunkBytes + (lr ? 2 * W * 2 : 0));
 }
 // horizontal pass, two warps per row: per warp, then per row (exchange + L-R rows)
 __host__ __device__ inline int h2_warp_bytes(int ph) {
@@ -566,219 +563,6 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
     __syncthreads();
     if (threadIdx.x == 0)
         for (int b = 0; b < 2 * NS; b++) mbar_inval(smem_u32(&full[b]));
-}
-
-// ------------------------------------------------------ horizontal passes
-// One warp per image row, walking x in direction dx.  MODE 1: S += L;
-// MODE 2: final S -> WTA (+ right-view disparity and left-right check).
-// The right-view disparity dR(xr) = argmin_d S(xr+d, d) is carried in
-// registers: lane l keeps the running minimum for the 2*PPL right pixels
-// xr = x - base_d - j its disparities reach at column x; stepping to x-1
-// shifts them by one and takes the lane-above's finished entry by shuffle, and
-// lane 0's entry for xr = x is complete.  (Only launched with dx = -1.)
-template <int PPL, int MODE>
-__device__ __forceinline__ void h_body(const FK& k, int dx, int GH, int warp_bytes, int blk,
-                                       unsigned char* smem, bool nc) {
-    constexpr int SB = 128 * PPL;
-    constexpr int DSPAN = 64 * PPL;
-    constexpr int NJ = 2 * PPL;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int y = blk * GH + warp;
-    if (warp >= GH || y >= k.H) return;  // warps are independent: no block-wide barrier below
-    unsigned char* wbase = smem + (size_t)warp * warp_bytes;
-    uint64_t* sbar = (uint64_t*)wbase;  // kHSlots barriers
-    uint64_t* cbar = sbar + kHSlots;    // kChunkSlots barriers
-    unsigned char* sring = wbase + 128;
-    unsigned char* cring = sring + kHSlots * SB;
-    uint16_t* rowL = (uint16_t*)(cring + kChunkSlots * kChunkBytes);
-    uint16_t* rowR = rowL + k.W;
-    const bool lr = MODE == 2 && k.lr_thr >= 0;
-
-    const int W = k.W;
-    const int x0 = dx > 0 ? 0 : W - 1;
-    const int nch = (W + kChunk - 1) / kChunk;
-    const int groups_row = (W + 7) / 8;
-    const Plane* rrow = k.RPp + (size_t)y * k.Wp;
-    const uint32_t* srow = k.S + (size_t)y * W * k.Dp2;
-
-    if (lane == 0) {
-        for (int b = 0; b < kHSlots + kChunkSlots; b++) mbar_init(smem_u32(&sbar[b]), 1);
-        fence_mbar_init();
-    }
-    __syncwarp();
-
-    auto cl_of = [&](int x) { return max(0, x - DSPAN + 2) >> 6; };
-    auto chunk_use = [&](int c) { return dx > 0 ? c / kChunkSlots : (nch - 1 - c) / kChunkSlots; };
-    auto chunk_bar = [&](int c) { return smem_u32(&cbar[c & (kChunkSlots - 1)]); };
-    auto issue_chunk = [&](int c) {
-        const int ng = min(kChunk / 8, groups_row - c * (kChunk / 8));
-        const uint32_t bar = chunk_bar(c);
-        mbar_expect_tx(bar, (uint32_t)ng * kGroupBytes);
-        tma_load(smem_u32(cring + (c & (kChunkSlots - 1)) * kChunkBytes), rrow + 9 * (c * (kChunk / 8)),
-                 (uint32_t)ng * kGroupBytes, bar);
-    };
-    auto issue_s = [&](int t) {
-        const int x = x0 + dx * t;
-        const uint32_t bar = smem_u32(&sbar[t & (kHSlots - 1)]);
-        mbar_expect_tx(bar, SB);
-        tma_load(smem_u32(sring + (t & (kHSlots - 1)) * SB), srow + (size_t)x * k.Dp2, SB, bar);
-    };
-
-    // Right-plane chunks: the window [x-DSPAN+2, x] is resident and kLookC
-    // chunks beyond it are in flight.  `need` is the next chunk to wait for,
-    // `next` the next to issue, both moving in the walk direction.
-    int need, next;
-    if (dx > 0) {
-        need = 0;
-        next = 0;
-        if (lane == 0)
-            for (; next < nch && next <= kLookC; next++) issue_chunk(next);
-    } else {
-        need = nch - 1;
-        next = nch - 1;
-        if (lane == 0)
-            for (; next >= 0 && next >= cl_of(W - 1) - kLookC; next--) issue_chunk(next);
-    }
-    int s_issued = 0;
-    if (lane == 0)
-        for (; s_issued < kHSlots && s_issued < W; s_issued++) issue_s(s_issued);
-    next = __shfl_sync(FULL, next, 0);
-    s_issued = __shfl_sync(FULL, s_issued, 0);
-
-    bool ok = true;
-    const int base_d = lane * 2 * PPL;
-    const bool edge_lane = base_d + 2 * PPL > k.D;
-    uint32_t L[PPL], m = 0, sv[PPL];
-    uint32_t P[NJ];  // right-view running minima (MODE 2, dx = -1)
-    #pragma unroll
-    for (int j = 0; j < NJ; j++) P[j] = FULL;
-    uint4 lp_next = ld_plane(&k.LP[(size_t)y * W + x0], nc);
-    uint32_t* sg = k.S + ((size_t)y * W + x0) * k.Dp2 + lane * PPL;
-    const long long sstep = (long long)dx * k.Dp2;
-
-    int t = 0;
-    for (; t < W; t++) {
-        const int x = x0 + dx * t;
-        bool good = true;
-        if (dx > 0) {
-            if ((x & (kChunk - 1)) == 0) {
-                const int c = x >> 6;
-                if (lane == 0 && next < nch) issue_chunk(next);
-                if (next < nch) next++;
-                good = mbar_wait(chunk_bar(c), (uint32_t)chunk_use(c) & 1u);
-                need = c + 1;
-            }
-        } else {
-            const int cl = cl_of(x);
-            while (good && need >= cl) {
-                good = mbar_wait(chunk_bar(need), (uint32_t)chunk_use(need) & 1u);
-                need--;
-            }
-            if (next >= 0 && next >= cl - kLookC) {
-                if (lane == 0) issue_chunk(next);
-                next--;
-            }
-        }
-        good = good && mbar_wait(smem_u32(&sbar[t & (kHSlots - 1)]), (uint32_t)(t / kHSlots) & 1u);
-        ok = __all_sync(FULL, good);
-        if (!ok) break;
-
-        const uint4 lp = lp_next;
-        if (t + 1 < W) lp_next = ld_plane(&k.LP[(size_t)y * W + x + dx], nc);
-        uint32_t c[PPL], Ln[PPL];
-        const int eb = x - base_d;
-        #pragma unroll
-        for (int q = 0; q < PPL; q++) {
-            const int e = max(eb - 2 * q, 0);
-            c[q] = bt_pair(lp, *(const uint4*)(cring + ppos(e & (kChunkSlots * kChunk - 1)) * 16));
-        }
-        if (edge_lane || eb < 2 * PPL) {
-            const int lim = min(x + 1, k.D);
-            #pragma unroll
-            for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
-        }
-        if (t == 0) {
-            #pragma unroll
-            for (int q = 0; q < PPL; q++) Ln[q] = c[q];
-        } else {
-            recur<PPL>(L, m, c, Ln, lane, k);
-        }
-        Vec<PPL>::lds((const uint32_t*)(sring + (t & (kHSlots - 1)) * SB) + lane * PPL, sv);
-        #pragma unroll
-        for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
-        if (MODE == 1) {
-            Vec<PPL>::st(sg, sv);
-        } else {
-            // WTA key (S << 8 | d): lowest S, then lowest d (tdvision/wtacpu.cpp:26-30)
-            uint32_t key[NJ];
-            #pragma unroll
-            for (int q = 0; q < PPL; q++) {
-                key[2 * q] = ((sv[q] & 0xFFFFu) << 8) | (uint32_t)(base_d + 2 * q);
-                key[2 * q + 1] = ((sv[q] >> 16) << 8) | (uint32_t)(base_d + 2 * q + 1);
-            }
-            uint32_t kmin = key[0];
-            #pragma unroll
-            for (int j = 1; j < NJ; j++) kmin = min(kmin, key[j]);
-            kmin = __reduce_min_sync(FULL, kmin);
-            if (lr) {
-                #pragma unroll
-                for (int j = 0; j < NJ; j++) P[j] = min(P[j], key[j]);
-                uint32_t in = __shfl_down_sync(FULL, P[0], 1);
-                if (lane == 31) in = FULL;
-                if (lane == 0) {
-                    rowR[x] = (uint16_t)(P[0] & 0xFFu);
-                    rowL[x] = (uint16_t)(kmin & 0xFFu);
-                }
-                #pragma unroll
-                for (int j = 0; j < NJ - 1; j++) P[j] = P[j + 1];
-                P[NJ - 1] = in;
-            } else if (lane == 0) {
-                const size_t o = (size_t)y * W + x;
-                const uint16_t dl = (uint16_t)(kmin & 0xFFu);
-                if (k.disp) k.disp[o] = dl;
-                if (k.disp_norm) k.disp_norm[o] = __fdiv_rn((float)dl, (float)k.D);
-            }
-        }
-        sg += sstep;
-        #pragma unroll
-        for (int q = 0; q < PPL; q++) L[q] = Ln[q];
-        m = warp_min_pairs<PPL>(L);
-        __syncwarp();
-        if (s_issued < W) {
-            if (lane == 0) issue_s(s_issued);
-            s_issued++;
-        }
-    }
-
-    // copies still in flight (chunks fetched ahead, or the tail after a
-    // failed wait) must land before the warp's shared memory can be reused
-    if (lane == 0) {
-        const uint64_t lim = ok ? kWaitNs : kDrainNs;
-        for (int r = t + 1; r < s_issued; r++)
-            mbar_wait(smem_u32(&sbar[r & (kHSlots - 1)]), (uint32_t)(r / kHSlots) & 1u, lim);
-        if (!ok) mbar_wait(smem_u32(&sbar[t & (kHSlots - 1)]), (uint32_t)(t / kHSlots) & 1u, lim);
-        if (dx > 0) {
-            for (int c = need; c < next; c++) mbar_wait(chunk_bar(c), (uint32_t)chunk_use(c) & 1u, lim);
-        } else {
-            for (int c = need; c > next; c--) mbar_wait(chunk_bar(c), (uint32_t)chunk_use(c) & 1u, lim);
-        }
-        if (!ok) atomicExch(k.err, (int)TDV_ERR_TIMEOUT);
-        for (int b = 0; b < kHSlots + kChunkSlots; b++) mbar_inval(smem_u32(&sbar[b]));
-    }
-    if (!ok) return;
-
-    if (lr) {
-        __syncwarp();
-        for (int xx = lane; xx < W; xx += 32) {
-            const int dl = rowL[xx];
-            const int xr = xx - dl;
-            const bool bad = xr < 0 || abs(dl - (int)rowR[xr]) > k.lr_thr;
-            const size_t o = (size_t)y * W + xx;
-            if (k.disp) k.disp[o] = bad ? (uint16_t)0xFFFF : (uint16_t)dl;
-            if (k.disp_norm) k.disp_norm[o] = bad ? -1.0f : __fdiv_rn((float)dl, (float)k.D);
-            if (k.disp_right) k.disp_right[o] = rowR[xx];
-        }
-    }
 }
 
 // ------------------------------------- horizontal passes, producer-fed
