@@ -569,9 +569,9 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
 // R consumer warps (one image row each, walking x in direction dx) and one
 // producer warp whose lane r keeps row r's rings full, so the consumers carry
 // no copy bookkeeping.  Per row:
-//   * an S ring of hp_slots(TWO) slots, each holding kHpU consecutive pixels of
+//   * an S ring of hp_slots(TWO) slots, each holding hp_px(TWO) consecutive pixels of
 //     the row: their S vectors and their left-plane entries (two TMA bulk
-//     copies per slot); a consumer waits once per kHpU steps and releases the
+//     copies per slot); a consumer waits once per slot and releases the
 //     slot (mbarrier arrive) when it has read it;
 //   * a right-plane chunk ring of kHpChunkSlots chunks of kChunk entries,
 //     chunk c in slot c & 3, read only by the lane that loads the entry
@@ -586,17 +586,20 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
 // TWO: the pass joins two volumes filled by concurrent pass chains, k.S and
 // k.S2 (read-only): a slot also holds the S2 vectors, and the pass stores
 // S + S2 + L into k.S.
-constexpr int kHpU = 4;           // pixels per S slot
 constexpr int kHpChunkSlots = 4;  // right-plane chunks per row (power of 2)
-// S slots per row: one row's S (and S2) bytes in flight; the two-volume pass
-// has twice the bytes per slot
-__host__ __device__ constexpr int hp_slots(bool two) { return two ? 5 : 6; }
+// Pixels per S slot and S slots per row.  A slot of 8 pixels matches the
+// eight-step unroll: one slot wait per iteration, so the eight steps are one
+// straight-line stretch the compiler schedules across (a wait is an asm
+// barrier to it), and 4 KB copies per volume.  The two-volume join holds two
+// such slots per row, the other passes three.
+__host__ __device__ constexpr int hp_px(bool) { return 8; }
+__host__ __device__ constexpr int hp_slots(bool two) { return two ? 2 : 3; }
 __host__ __device__ constexpr int hp_bars(bool two) { return 2 * hp_slots(two) + 2 * kHpChunkSlots; }
 
-// slot: [S vectors of kHpU pixels][S2 vectors (TWO)][left-plane entries],
+// slot: [S vectors of hp_px(two) pixels][S2 vectors (TWO)][left-plane entries],
 // padded to 128 bytes so every slot's vectors start on a 128-byte line
 __host__ __device__ inline int hp_slot_bytes(int ppl, bool two) {
-    return align128(kHpU * (128 * ppl * (two ? 2 : 1) + 16));
+    return align128(hp_px(two) * (128 * ppl * (two ? 2 : 1) + 16));
 }
 __host__ __device__ inline int hp_warp_bytes(int ppl, bool lr, int W, bool two) {
     return align128(hp_slots(two) * hp_slot_bytes(ppl, two) + kHpChunkSlots * kChunkBytes + (lr ? 2 * W * 2 : 0));
@@ -609,6 +612,7 @@ template <int PPL, int MODE, bool TWO>
 __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, unsigned char* smem) {
     constexpr int SB = 128 * PPL;
     constexpr int NSL = hp_slots(TWO);   // S slots per row
+    constexpr int kHpU = hp_px(TWO);     // pixels per S slot
     constexpr int CS = kHpChunkSlots;    // right-plane chunks per row
     constexpr int BARS = hp_bars(TWO);
     constexpr int DSPAN = 64 * PPL;
@@ -919,9 +923,14 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                     WX[o % NJ] = v.z;
                 }
             }
-            for (int j = 0; j < ngroups; j += 2) {
-                if (!group(std::integral_constant<int, 0>{}, j)) return false;
-                if (j + 1 < ngroups && !group(std::integral_constant<int, kHpU>{}, j + 1)) return false;
+            constexpr int GPI = 8 / kHpU;  // groups per eight-step iteration
+            for (int j = 0; j < ngroups; j += GPI) {
+                bool good = true;
+                static_for<0, GPI>([&](auto gc) {
+                    constexpr int g = decltype(gc)::value;
+                    if (good && j + g < ngroups) good = group(std::integral_constant<int, g * kHpU>{}, j + g);
+                });
+                if (!good) return false;
             }
             return true;
         };
