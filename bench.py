@@ -352,6 +352,61 @@ def measure_plain(ctx, dev, reps=3):
     return out
 
 
+def measure_image(ctx, dev, reps=10):
+    """The image stages either side of the path at 1920x1080: grey
+    conversion, remap (grey F32 and color U8x3), the two pre-filters, the
+    opening and the 3x3 median of a disparity map, sub-pixel refinement from
+    a D=256 F32 volume and Q reprojection with colors.  Each call timed alone
+    with CUDA events (median of `reps`, L2 flushed before each), against the
+    bytes it must read and write."""
+    import torch
+
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    color = torch.randint(0, 256, (H, W, 3), dtype=torch.uint8, device=dev, generator=g)
+    gray = torch.rand((H, W), device=dev, generator=g)
+    yy, xx = torch.meshgrid(torch.arange(H, device=dev, dtype=torch.float32),
+                            torch.arange(W, device=dev, dtype=torch.float32), indexing="ij")
+    # a mild rectifying warp: small rotation and scale about the centre
+    mapx = (0.999 * (xx - W / 2) - 0.01 * (yy - H / 2) + W / 2 + 0.37).contiguous()
+    mapy = (0.01 * (xx - W / 2) + 0.999 * (yy - H / 2) + H / 2 - 0.21).contiguous()
+    dispf = torch.rand((H, W), device=dev, generator=g)
+    disp16 = torch.randint(0, D, (H, W), device=dev, generator=g).to(torch.uint16)
+    S = torch.rand((H, W, D), device=dev, generator=g)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    Q = [1, 0, 0, -W / 2, 0, 1, 0, -H / 2, 0, 0, 0, 1400.0, 0, 0, -1 / 0.12, 0]
+    px = W * H
+    cases = [
+        ("to_gray", lambda: ctx.to_gray(color), 3 * px + 4 * px),
+        ("remap_gray_f32", lambda: ctx.remap(gray, mapx, mapy), 4 * px + 8 * px + 4 * px),
+        ("remap_color_u8x3", lambda: ctx.remap(color, mapx, mapy), 3 * px + 8 * px + 3 * px),
+        ("prefilter_gauss5", lambda: ctx.prefilter(gray, "gauss5"), 8 * px),
+        ("prefilter_median7", lambda: ctx.prefilter(gray, "median7"), 8 * px),
+        ("postfilter_open7_f32", lambda: ctx.postfilter(dispf, "open7"), 16 * px),
+        ("postfilter_median3_u16", lambda: ctx.postfilter(disp16, "median3"), 4 * px),
+        ("subpixel_d256", lambda: ctx.subpixel(S, disp16), (2 + 12 + 4) * px),
+        ("reproject_q_color", lambda: ctx.reproject(dispf, color, "q", q=Q), 4 * px + 3 * px + 24 * px),
+    ]
+    st = torch.cuda.current_stream()
+    res = {"workload": f"{W}x{H} frame; sub-pixel from a D={D} F32 volume; bytes = what each stage must read "
+                       "and write (maps 8 B/px, F32 4 B/px, U8x3 3 B/px)"}
+    for name, fn, nbytes in cases:
+        fn()
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            fn()
+            e1.record(st)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = sorted(ts)[len(ts) // 2]
+        res[name] = {"ms": ms, "gb_per_s": nbytes / (ms / 1000.0) / 1e9}
+    del S
+    return res
+
+
 def measure_video(ctx, dev, n_frames=300, refit_steps=50):
     """Full-HD video: 300 frames (12 moving rectangles over a slanted plane,
     sensor noise sigma 2), D=256, fused BT + SGM + WTA + L-R check, through a
@@ -639,6 +694,7 @@ def run_ours(args):
     }
     if not args.no_extras:
         for key, fn in (("batch", measure_batch), ("soft", measure_soft), ("plain", measure_plain),
+                        ("image_stages", measure_image),
                         ("video", measure_video)):
             try:
                 line[key] = fn(ctx, dev)

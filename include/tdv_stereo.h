@@ -251,6 +251,100 @@ tdv_status tdv_soft_sgm_backward(tdv_ctx* ctx, const tdv_volume* cost, const tdv
                                  const void* tape, size_t tape_bytes, const void* g_dhat,
                                  tdv_volume* dcost, void* dpen, tdv_stream stream);
 
+/* ---- image stages either side of the path ------------------------------
+ * The steps LibThunderVision runs before the cost (input conversion,
+ * rectification remap, pre-filter) and after the disparity reduction
+ * (morphological clean-up, sub-pixel refinement, reprojection to 3D and the
+ * PLY mesh file), as device kernels on caller-owned buffers. */
+
+/* A 2-D array of pixels with interleaved channels. */
+typedef struct {
+    void* ptr;           /* device */
+    int32_t width, height;
+    int32_t pitch_bytes; /* bytes between rows, >= width * channels * element size */
+    int32_t dtype;       /* TDV_U8, TDV_U16 or TDV_F32 */
+    int32_t channels;    /* 1 or 3 */
+} tdv_raster;
+
+/* Grey conversion of an 8-bit 3-channel image into F32: each channel scaled
+ * by 1/255 (in double, rounded to float), then 0.299*c0 + 0.587*c1 + 0.114*c2
+ * with channel 0 weighted as red whatever the capture order, as the reference
+ * converts its BGR frames (tdvision/misc.cpp:29-32). */
+tdv_status tdv_to_gray(tdv_ctx* ctx, const tdv_raster* color, float* gray, tdv_stream stream);
+
+/* Rectification remap: dst(x, y) = src sampled bilinearly at (mapx, mapy)
+ * (float maps of dst's size, dense rows), coordinates rounded to 1/32 pixel,
+ * taps outside src read 0; U8 sources use 15-bit fixed-point weights with
+ * rounding, F32 sources float weights.  Replaces the per-frame cvRemap of
+ * RectificationCV::update (tdvision/rectificationcv.cpp:298-310); src and dst
+ * have the same dtype and channel count. */
+tdv_status tdv_remap(tdv_ctx* ctx, const tdv_raster* src, const float* mapx, const float* mapy,
+                     tdv_raster* dst, tdv_stream stream);
+
+typedef enum {
+    TDV_FILTER_GAUSS5 = 0,  /* separable [1 4 6 4 1]/16, replicated borders: the 5x5 Gaussian
+                               DevStereoMatcher applies by default (MedianFilterCPU =
+                               cvSmooth(CV_GAUSSIAN, 5), tdvision/medianfiltercpu.cpp:15,
+                               devstereomatcher.cpp:11,22-29) */
+    TDV_FILTER_MEDIAN7 = 1  /* 7x7 median, replicated borders: the median the reference's
+                               device filter was written for (tdvision/medianfilter.cu:37-57;
+                               its launcher runs a placeholder instead, :75-76) */
+} tdv_filter_kind;
+
+/* Pre-filter of one image before the cost: `out` is F32, width x height,
+ * dense rows, holding the filtered intensities (value * scale). */
+tdv_status tdv_prefilter(tdv_ctx* ctx, const tdv_image* in, int32_t kind, float* out, tdv_stream stream);
+
+typedef enum {
+    TDV_POST_OPEN7 = 0,   /* 7x7 minimum then 7x7 maximum, windows clipped at the borders:
+                             Dilate's cvErode + cvDilate with 3 iterations of the default 3x3
+                             element (tdvision/dilate.cpp:18-19), run after the matcher in
+                             Reconstruction (tdvision/reconstruction.cpp:30-31) */
+    TDV_POST_MEDIAN3 = 1  /* 3x3 median, replicated borders */
+} tdv_post_kind;
+
+/* Post-filter of a 1-channel disparity map (F32 or U16); in and out have the
+ * same size and dtype and must not overlap. */
+tdv_status tdv_postfilter(tdv_ctx* ctx, const tdv_raster* in, int32_t kind, tdv_raster* out,
+                          tdv_stream stream);
+
+/* Sub-pixel refinement: for each pixel with 0 < d < D-1 and a convex
+ * neighbourhood, d + (S(d-1) - S(d+1)) / (2 (S(d-1) - 2 S(d) + S(d+1))) from the
+ * aggregated volume S (F32, HWD, as tdv_sgm writes it); other pixels keep d,
+ * invalid ones (0xFFFF) give -1.  `out` is F32 width x height. */
+tdv_status tdv_subpixel(tdv_ctx* ctx, const tdv_volume* S, const uint16_t* disp, float* out,
+                        tdv_stream stream);
+
+typedef enum {
+    TDV_REPROJECT_DIRECT = 0, /* (x, H - y, d * zscale): DirectReprojector::reproject
+                                 (tdvision/directreprojector.hpp:17-20) */
+    TDV_REPROJECT_Q = 1       /* Q * (x, H - y, d, 1), divided by w (0 when |w| <= FLT_EPSILON),
+                                 then z * 24: CVReprojector::reproject
+                                 (tdvision/cvreprojector.cpp:45-60) */
+} tdv_reproject_mode;
+
+typedef struct {
+    int32_t mode;  /* tdv_reproject_mode */
+    float zscale;  /* DIRECT */
+    float q[16];   /* Q, row-major (cvStereoRectify's reprojection matrix) */
+} tdv_reproject_params;
+
+/* Reprojection of a disparity map (F32, 1 channel: the values the matcher's
+ * float output holds) to one vertex per pixel, row-major, 3 floats each, and
+ * the pixel's color (U8, 3 channels, may be NULL) to 3 floats in [0, 1]
+ * (channel order kept), as GLReprojection::updateMesh fills the grid mesh
+ * (tdvision/glreprojection.cpp:30-55), into device buffers. */
+tdv_status tdv_reproject(tdv_ctx* ctx, const tdv_raster* disp, const tdv_raster* color,
+                         const tdv_reproject_params* params, float* vertices, float* colors,
+                         tdv_stream stream);
+
+/* Writes the grid mesh (host vertices and colors as tdv_reproject lays them
+ * out) as the reference's ASCII PLY: a vertex per pixel "x y z r g b" with the
+ * colors times 255 truncated, then a quad "4 a b c d" per grid cell
+ * (tdvision/plymeshexporter.cpp:8-76).  colors may be NULL (0 0 0). */
+tdv_status tdv_write_ply(const char* path, const float* vertices, const float* colors, int32_t width,
+                         int32_t height);
+
 /* ---- context ---------------------------------------------------------- */
 typedef void* (*tdv_alloc_fn)(size_t bytes, void* user);
 typedef void (*tdv_free_fn)(void* ptr, void* user);

@@ -33,13 +33,28 @@ EXPORTS = [
     "tdv_batch_create", "tdv_batch_destroy", "tdv_batch_set_tiles", "tdv_batch_get_tiles",
     "tdv_batch_autotune", "tdv_batch_run", "tdv_batch_graph_launch", "tdv_batch_status",
     "tdv_batch_set_wait_limit", "tdv_batch_work_queue",
+    "tdv_to_gray", "tdv_remap", "tdv_prefilter", "tdv_postfilter", "tdv_subpixel", "tdv_reproject",
+    "tdv_write_ply",
 ]
+F32, U16, U8, F64 = 0, 1, 2, 3
+FILTER_GAUSS5, FILTER_MEDIAN7 = 0, 1
+POST_OPEN7, POST_MEDIAN3 = 0, 1
+REPROJECT_DIRECT, REPROJECT_Q = 0, 1
 BATCH_ORDER_LONGEST_FIRST, BATCH_ORDER_INPUT = 0, 1
 
 
 class tdv_image(ctypes.Structure):
     _fields_ = [("ptr", ctypes.c_void_p), ("width", ctypes.c_int32), ("height", ctypes.c_int32),
                 ("pitch", ctypes.c_int32), ("dtype", ctypes.c_int32), ("scale", ctypes.c_float)]
+
+
+class tdv_raster(ctypes.Structure):
+    _fields_ = [("ptr", ctypes.c_void_p), ("width", ctypes.c_int32), ("height", ctypes.c_int32),
+                ("pitch_bytes", ctypes.c_int32), ("dtype", ctypes.c_int32), ("channels", ctypes.c_int32)]
+
+
+class tdv_reproject_params(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int32), ("zscale", ctypes.c_float), ("q", ctypes.c_float * 16)]
 
 
 class tdv_volume(ctypes.Structure):
@@ -132,6 +147,13 @@ def _declare(lib):
         "tdv_batch_status": (st, [vp, vp]),
         "tdv_batch_set_wait_limit": (st, [vp, ctypes.c_double]),
         "tdv_batch_work_queue": (st, [vp, P(vp), P(ctypes.c_int32), P(ctypes.c_int32)]),
+        "tdv_to_gray": (st, [vp, P(tdv_raster), vp, vp]),
+        "tdv_remap": (st, [vp, P(tdv_raster), vp, vp, P(tdv_raster), vp]),
+        "tdv_prefilter": (st, [vp, P(tdv_image), ctypes.c_int32, vp, vp]),
+        "tdv_postfilter": (st, [vp, P(tdv_raster), ctypes.c_int32, P(tdv_raster), vp]),
+        "tdv_subpixel": (st, [vp, P(tdv_volume), vp, vp, vp]),
+        "tdv_reproject": (st, [vp, P(tdv_raster), P(tdv_raster), P(tdv_reproject_params), vp, vp, vp]),
+        "tdv_write_ply": (st, [ctypes.c_char_p, vp, vp, ctypes.c_int32, ctypes.c_int32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

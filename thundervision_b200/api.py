@@ -39,6 +39,30 @@ def _image(t, scale=1.0):
     return L.tdv_image(t.data_ptr(), t.shape[1], t.shape[0], t.stride(0), dt, float(scale))
 
 
+_RASTER_DTYPES = {torch.uint8: (L.U8, 1), torch.uint16: (L.U16, 2), torch.float32: (L.F32, 4)}
+
+
+def _raster(t):
+    """tdv_raster of an (H, W) or (H, W, C) CUDA tensor whose rows may be
+    padded but whose pixels and channels are dense."""
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("rasters must be CUDA tensors")
+    if t.dtype not in _RASTER_DTYPES:
+        raise TypeError("rasters must be uint8, uint16 or float32")
+    dt, size = _RASTER_DTYPES[t.dtype]
+    if t.dim() == 2:
+        ch = 1
+        dense = t.stride(1) == 1
+    elif t.dim() == 3:
+        ch = t.shape[2]
+        dense = t.stride(2) == 1 and t.stride(1) == ch
+    else:
+        raise ValueError("rasters must be (H, W) or (H, W, C)")
+    if not dense:
+        raise ValueError("raster pixels must be dense within a row")
+    return L.tdv_raster(t.data_ptr(), t.shape[1], t.shape[0], t.stride(0) * size, dt, ch)
+
+
 def _volume(t, layout):
     if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float32:
         raise TypeError("volumes must be float32 CUDA tensors")
@@ -180,6 +204,73 @@ class Context:
                                         radius, ctypes.byref(o), _stream()))
         return self._result(disp, dn, dr)
 
+    # ---- image stages either side of the path ------------------------
+    def to_gray(self, color):
+        """(H, W, 3) uint8 -> (H, W) float32 grey in [0, 1] (channel 0 weighted
+        as red, as tdvision/misc.cpp:29-32 converts its frames)."""
+        out = torch.empty(color.shape[:2], dtype=torch.float32, device=color.device)
+        self.check(L.lib().tdv_to_gray(self.handle, ctypes.byref(_raster(color)), out.data_ptr(), _stream()))
+        return out
+
+    def remap(self, src, mapx, mapy):
+        """Rectification remap: src sampled bilinearly at (mapx, mapy), the
+        maps (H, W) float32 of the output's size; src (H', W') or (H', W', 3),
+        uint8 or float32."""
+        if mapx.shape != mapy.shape or mapx.dtype != torch.float32 or mapy.dtype != torch.float32:
+            raise ValueError("maps must be float32 of one shape")
+        mapx, mapy = mapx.contiguous(), mapy.contiguous()
+        out = torch.empty(tuple(mapx.shape) + tuple(src.shape[2:]), dtype=src.dtype, device=src.device)
+        self.check(L.lib().tdv_remap(self.handle, ctypes.byref(_raster(src)), mapx.data_ptr(), mapy.data_ptr(),
+                                     ctypes.byref(_raster(out)), _stream()))
+        return out
+
+    def prefilter(self, img, kind="gauss5", scale=1.0):
+        """Pre-filter before the cost: "gauss5" (DevStereoMatcher's default
+        5x5 Gaussian) or "median7"; returns (H, W) float32 of value * scale."""
+        k = {"gauss5": L.FILTER_GAUSS5, "median7": L.FILTER_MEDIAN7}[kind]
+        out = torch.empty(img.shape, dtype=torch.float32, device=img.device)
+        self.check(L.lib().tdv_prefilter(self.handle, ctypes.byref(_image(img, scale)), k, out.data_ptr(),
+                                         _stream()))
+        return out
+
+    def postfilter(self, disp, kind="open7"):
+        """Disparity clean-up: "open7" (the reference's erode + dilate) or
+        "median3"; float32 or uint16 maps."""
+        k = {"open7": L.POST_OPEN7, "median3": L.POST_MEDIAN3}[kind]
+        out = torch.empty_like(disp)
+        self.check(L.lib().tdv_postfilter(self.handle, ctypes.byref(_raster(disp)), k, ctypes.byref(_raster(out)),
+                                          _stream()))
+        return out
+
+    def subpixel(self, S, disp):
+        """Parabola sub-pixel refinement of a uint16 disparity map from the
+        aggregated volume S ((H, W, D) float32)."""
+        out = torch.empty(disp.shape, dtype=torch.float32, device=disp.device)
+        self.check(L.lib().tdv_subpixel(self.handle, ctypes.byref(_volume(S, "hwd")), disp.contiguous().data_ptr(),
+                                        out.data_ptr(), _stream()))
+        return out
+
+    def reproject(self, disp, color=None, mode="direct", zscale=1.0, q=None):
+        """One vertex per pixel ((H, W, 3) float32) and, with a (H, W, 3)
+        uint8 color image, its color in [0, 1]; mode "direct" or "q" (q: 16
+        floats, row-major)."""
+        prm = L.tdv_reproject_params()
+        prm.mode = {"direct": L.REPROJECT_DIRECT, "q": L.REPROJECT_Q}[mode]
+        prm.zscale = float(zscale)
+        qq = [1.0 if i % 5 == 0 else 0.0 for i in range(16)] if q is None else [float(v) for v in q]
+        if len(qq) != 16:
+            raise ValueError("q must hold 16 values")
+        for i, v in enumerate(qq):
+            prm.q[i] = v
+        H, W = disp.shape
+        verts = torch.empty((H, W, 3), dtype=torch.float32, device=disp.device)
+        cols = torch.empty((H, W, 3), dtype=torch.float32, device=disp.device) if color is not None else None
+        craster = ctypes.byref(_raster(color)) if color is not None else None
+        self.check(L.lib().tdv_reproject(self.handle, ctypes.byref(_raster(disp)), craster, ctypes.byref(prm),
+                                         verts.data_ptr(), cols.data_ptr() if cols is not None else None,
+                                         _stream()))
+        return verts, cols
+
     def stereo_sgm(self, left, right, max_disp, p1, p2, paths=8, p2_mode="const", table="full",
                    semantics="standard", scale=1.0, lr=None, norm=False, right_disp=False):
         """BT + SGM + WTA with the cost recomputed inside the aggregation."""
@@ -293,3 +384,15 @@ def default_context(device=None):
     if device not in _default:
         _default[device] = Context(device)
     return _default[device]
+
+
+def write_ply(path, vertices, colors=None):
+    """Writes a grid mesh ((H, W, 3) float32 vertices, optional (H, W, 3)
+    float32 colors in [0, 1], host or device tensors) as the reference's
+    ASCII PLY (tdvision/plymeshexporter.cpp:8-76)."""
+    v = vertices.detach().to("cpu", torch.float32).contiguous()
+    c = colors.detach().to("cpu", torch.float32).contiguous() if colors is not None else None
+    H, W = v.shape[0], v.shape[1]
+    st = L.lib().tdv_write_ply(str(path).encode(), v.data_ptr(), c.data_ptr() if c is not None else None, W, H)
+    if st != L.TDV_OK:
+        raise L.TdvError(st, f"writing {path}")

@@ -141,6 +141,15 @@ struct ImgArg {
     float scale;
 };
 
+// A 2-D pixel array with interleaved channels (tdv_raster); pitch in bytes,
+// dtype 0 = F32, 1 = U16, 2 = U8.
+struct RasterArg {
+    void* ptr;
+    int W, H;
+    long long pitch;
+    int dtype, ch;
+};
+
 struct VolArg {
     void* ptr;
     int W, H, D;
@@ -191,6 +200,19 @@ struct FusedArgs {
     cudaEvent_t fork = nullptr, join = nullptr;
 };
 size_t fused_agg_bytes(int W, int H, int D);
+
+// Image stages either side of the path (kernels_image.cu).
+cudaError_t launch_to_gray(const RasterArg& color, float* gray, cudaStream_t st);
+cudaError_t launch_remap(const RasterArg& src, const float* mx, const float* my, const RasterArg& dst,
+                         cudaStream_t st);
+cudaError_t launch_prefilter(const ImgArg& in, int kind, float* out, cudaStream_t st);
+// kind 0 (opening) needs `scratch` of W*H elements of the map's dtype
+cudaError_t launch_postfilter(const RasterArg& in, int kind, const RasterArg& out, void* scratch,
+                              cudaStream_t st);
+cudaError_t launch_subpixel(const float* S, int W, int H, int D, const uint16_t* disp, float* out,
+                            cudaStream_t st);
+cudaError_t launch_reproject(const RasterArg& disp, const RasterArg* color, int mode, float zscale,
+                             const float* q, float* verts, float* cols, cudaStream_t st);
 size_t fused_plane_bytes(int W, int H);
 cudaError_t launch_fused(const FusedArgs& a, cudaStream_t st, Timer* tm);
 
