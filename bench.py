@@ -353,8 +353,8 @@ def measure_plain(ctx, dev, reps=3):
 
 
 def measure_image(ctx, dev, reps=10):
-    """The image stages either side of the path at 1920x1080: grey
-    conversion, remap (grey F32 and color U8x3), the two pre-filters, the
+    """The image stages either side of the path at 1920x1080: rectification
+    maps, grey conversion, remap (grey F32 and color U8x3), the two pre-filters, the
     opening and the 3x3 median of a disparity map, sub-pixel refinement from
     a D=256 F32 volume and Q reprojection with colors.  Each call timed alone
     with CUDA events (median of `reps`, L2 flushed before each), against the
@@ -375,8 +375,12 @@ def measure_image(ctx, dev, reps=10):
     S = torch.rand((H, W, D), device=dev, generator=g)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     Q = [1, 0, 0, -W / 2, 0, 1, 0, -H / 2, 0, 0, 0, 1400.0, 0, 0, -1 / 0.12, 0]
+    K = [[1400.0, 0, W / 2 + 0.3], [0, 1398.0, H / 2 - 0.7], [0, 0, 1]]
+    dist = [-0.28, 0.09, 0.0012, -0.0007, -0.011]
+    Rr = [[0.9998, -0.0175, 0.0087], [0.0175, 0.9998, 0.0], [-0.0087, 0.0002, 0.99996]]
     px = W * H
     cases = [
+        ("rectify_maps", lambda: ctx.rectify_maps(K, dist, Rr, K, W, H), 8 * px),
         ("to_gray", lambda: ctx.to_gray(color), 3 * px + 4 * px),
         ("remap_gray_f32", lambda: ctx.remap(gray, mapx, mapy), 4 * px + 8 * px + 4 * px),
         ("remap_color_u8x3", lambda: ctx.remap(color, mapx, mapy), 3 * px + 8 * px + 3 * px),

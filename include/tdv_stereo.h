@@ -272,6 +272,21 @@ typedef struct {
  * converts its BGR frames (tdvision/misc.cpp:29-32). */
 tdv_status tdv_to_gray(tdv_ctx* ctx, const tdv_raster* color, float* gray, tdv_stream stream);
 
+/* Rectification maps of one camera: for each pixel (j, i) of the rectified
+ * width x height image, the source position after R, the new camera P and
+ * the Brown-Conrady distortion of K, dist = (k1, k2, p1, p2, k3, k4, k5, k6)
+ * (zeros for unused terms): (X, Y, W) = inv(P[:, :3] R) (j, i, 1) (inverse by
+ * cofactors), x = X/W, y = Y/W, r2 = x^2 + y^2,
+ * kr = (1 + ((k3 r2 + k2) r2 + k1) r2) / (1 + ((k6 r2 + k5) r2 + k4) r2),
+ * mapx = fx (x kr + 2 p1 x y + p2 (r2 + 2 x^2)) + cx,
+ * mapy = fy (y kr + p1 (r2 + 2 y^2) + 2 p2 x y) + cy, in double, stored as
+ * float.  Replaces the cvInitUndistortRectifyMap calls of RectificationCV
+ * (tdvision/rectificationcv.cpp:114-117, 152-155); K, R, P row-major 3x3
+ * (P's first three columns). */
+tdv_status tdv_rectify_maps(tdv_ctx* ctx, const double* K, const double* dist, const double* R,
+                            const double* P, int32_t width, int32_t height, float* mapx, float* mapy,
+                            tdv_stream stream);
+
 /* Rectification remap: dst(x, y) = src sampled bilinearly at (mapx, mapy)
  * (float maps of dst's size, dense rows), coordinates rounded to 1/32 pixel,
  * taps outside src read 0; U8 sources use 15-bit fixed-point weights with

@@ -11,6 +11,9 @@ tests/golden/ (exact except where noted):
   CV_RGB2GRAY; channel 0 is weighted as red.  OpenCV sums the three products
   in an order of its own; this restatement sums left to right and stays within
   2 ulp of it.
+* rectification maps, tdvision/rectificationcv.cpp:114-117,152-155
+  (cvInitUndistortRectifyMap: Brown-Conrady distortion, inverse of P R by
+  cofactors, double).  Exact.
 * remap, tdvision/rectificationcv.cpp:298-310 (cvRemap, bilinear, constant 0
   border): coordinates rounded to 1/32 pixel, float weights for float images,
   15-bit fixed-point weights with rounding for 8-bit ones.  Exact.
@@ -82,6 +85,40 @@ def remap(src, mapx, mapy):
         s = f32(s + f32(t11.astype(np.float32) * w11))
         out = s.astype(np.float32)
     return out if src.ndim == 3 else out[..., 0]
+
+
+def rectify_maps(K, dist, R, P, W, H):
+    """cvInitUndistortRectifyMap's model (tdvision/rectificationcv.cpp:114-117,
+    152-155), in double: M = P[:, :3] R summed left to right, its inverse by
+    cofactors, then per pixel (j, i) the operations in the order the kernel
+    rounds them.  dist = (k1, k2, p1, p2, k3, k4, k5, k6), zero-padded."""
+    K = np.asarray(K, np.float64).reshape(3, 3)
+    R = np.asarray(R, np.float64).reshape(3, 3)
+    P = np.asarray(P, np.float64).reshape(3, -1)[:, :3]
+    k = np.zeros(8)
+    k[:len(dist)] = np.asarray(dist, np.float64)
+    k1, k2, p1, p2, k3, k4, k5, k6 = k
+    M = np.empty((3, 3))
+    for r in range(3):
+        for c in range(3):
+            M[r, c] = (P[r, 0] * R[0, c] + P[r, 1] * R[1, c]) + P[r, 2] * R[2, c]
+    a, b, c, d, e, f, g, h, i = M.ravel()
+    A, B, C = e * i - f * h, -(d * i - f * g), d * h - e * g
+    det = (a * A + b * B) + c * C
+    iR = np.array([[A, -(b * i - c * h), b * f - c * e], [B, a * i - c * g, -(a * f - c * d)],
+                   [C, -(a * h - b * g), a * e - b * d]]) / det
+    fx, fy, cx, cy = K[0, 0], K[1, 1], K[0, 2], K[1, 2]
+    ii, jj = np.indices((H, W)).astype(np.float64)
+    lin = [(jj * iR[r, 0] + ii * iR[r, 1]) + iR[r, 2] for r in range(3)]
+    w = 1.0 / lin[2]
+    x, y = lin[0] * w, lin[1] * w
+    x2, y2 = x * x, y * y
+    r2 = x2 + y2
+    xy2 = (2.0 * x) * y
+    kr = (1.0 + ((k3 * r2 + k2) * r2 + k1) * r2) / (1.0 + ((k6 * r2 + k5) * r2 + k4) * r2)
+    u = fx * ((x * kr + p1 * xy2) + p2 * (r2 + 2.0 * x2)) + cx
+    v = fy * ((y * kr + p1 * (r2 + 2.0 * y2)) + p2 * xy2) + cy
+    return u.astype(np.float32), v.astype(np.float32)
 
 
 def _intensity(img, scale):

@@ -54,6 +54,15 @@ def main():
     yy, xx = np.indices((H, W))
     pts = np.stack([xx, H - yy, disp], axis=-1).astype(np.float32).reshape(1, -1, 3)
     g["persp"] = cv2.perspectiveTransform(pts, Q).reshape(H, W, 3)
+    # cvInitUndistortRectifyMap with a 5- and an 8-coefficient distortion
+    K = np.array([[820.5, 0, 30.2], [0, 815.1, 21.7], [0, 0, 1]])
+    R = cv2.Rodrigues(np.array([0.01, -0.02, 0.005]))[0]
+    P = np.array([[790.0, 0, 27.5, 0], [0, 790.0, 18.25, 0], [0, 0, 1, 0]])
+    g["K"], g["R"], g["P"] = K, R, P
+    for name, dist in (("5", [-0.28, 0.09, 0.0012, -0.0007, -0.011]),
+                       ("8", [-0.2, 0.05, 0.001, 0.0005, 0.01, 0.02, -0.01, 0.003])):
+        mxr, myr = cv2.initUndistortRectifyMap(K, np.array(dist), R, P, (W, H), cv2.CV_32FC1)
+        g["dist" + name], g["rmapx" + name], g["rmapy" + name] = np.array(dist), mxr, myr
     np.savez_compressed(os.path.join(HERE, "image_ops.npz"), **g)
 
 

@@ -93,6 +93,21 @@ def test_remap(ctx, H, W):
         np.testing.assert_array_equal(host(out), io.remap(src, mx, my))
 
 
+@pytest.mark.parametrize("n", ["5", "8"])
+def test_rectify_maps(ctx, g, n):
+    H, W = g["img"].shape
+    mx, my = ctx.rectify_maps(g["K"], g["dist" + n], g["R"], g["P"], W, H)
+    np.testing.assert_array_equal(host(mx), g["rmapx" + n])
+    np.testing.assert_array_equal(host(my), g["rmapy" + n])
+    # a full-size camera, against the oracle, then remapping with those maps
+    K = [[1400.0, 0, 961.3], [0, 1395.5, 539.2], [0, 0, 1]]
+    P = [[1380.0, 0, 955.0], [0, 1380.0, 541.0], [0, 0, 1]]
+    mx, my = ctx.rectify_maps(K, g["dist" + n], g["R"], P, 1920, 1080)
+    rx, ry = io.rectify_maps(K, g["dist" + n], g["R"], P, 1920, 1080)
+    np.testing.assert_array_equal(host(mx), rx)
+    np.testing.assert_array_equal(host(my), ry)
+
+
 def test_remap_on_golden(ctx, g):
     np.testing.assert_array_equal(host(ctx.remap(dev(g["img"]), dev(g["mapx"]), dev(g["mapy"]))), g["remap_f32"])
     np.testing.assert_array_equal(host(ctx.remap(dev(g["color"]), dev(g["mapx"]), dev(g["mapy"]))), g["remap_u8c3"])

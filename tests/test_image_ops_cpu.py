@@ -62,6 +62,14 @@ def test_remap_matches_opencv(g):
     assert np.array_equal(io.remap(g["color"], g["mapx"], g["mapy"]), g["remap_u8c3"])
 
 
+@pytest.mark.parametrize("n", ["5", "8"])
+def test_rectify_maps_match_opencv(g, n):
+    # cvInitUndistortRectifyMap, tdvision/rectificationcv.cpp:114-117
+    H, W = g["img"].shape
+    mx, my = io.rectify_maps(g["K"], g["dist" + n], g["R"], g["P"], W, H)
+    assert np.array_equal(mx, g["rmapx" + n]) and np.array_equal(my, g["rmapy" + n])
+
+
 def test_reprojection_q_matches_opencv(g):
     # CVReprojector::reproject, tdvision/cvreprojector.cpp:45-60
     v, _ = io.reproject(g["disp_f32"], mode="q", q=g["Q"].ravel())
@@ -136,5 +144,8 @@ def test_image_stage_arguments_are_validated():
         vol = L.tdv_volume(1 << 20, 4, 4, 8, L.LAYOUT_REF_WHD, L.F32)  # sub-pixel reads HWD
         assert lib.tdv_subpixel(h, ctypes.byref(vol), 1 << 21, 1 << 22, None) == L.TDV_ERR_INVALID_ARG
         assert lib.tdv_write_ply(None, 1, None, 2, 2) == L.TDV_ERR_INVALID_ARG
+        z = (ctypes.c_double * 9)()  # a singular P R
+        d8 = (ctypes.c_double * 8)()
+        assert lib.tdv_rectify_maps(h, z, d8, z, z, 4, 4, 1 << 21, 1 << 22, None) == L.TDV_ERR_INVALID_ARG
     finally:
         lib.tdv_ctx_destroy(h)

@@ -33,7 +33,7 @@ EXPORTS = [
     "tdv_batch_create", "tdv_batch_destroy", "tdv_batch_set_tiles", "tdv_batch_get_tiles",
     "tdv_batch_autotune", "tdv_batch_run", "tdv_batch_graph_launch", "tdv_batch_status",
     "tdv_batch_set_wait_limit", "tdv_batch_work_queue",
-    "tdv_to_gray", "tdv_remap", "tdv_prefilter", "tdv_postfilter", "tdv_subpixel", "tdv_reproject",
+    "tdv_to_gray", "tdv_rectify_maps", "tdv_remap", "tdv_prefilter", "tdv_postfilter", "tdv_subpixel", "tdv_reproject",
     "tdv_write_ply",
 ]
 F32, U16, U8, F64 = 0, 1, 2, 3
@@ -148,6 +148,7 @@ def _declare(lib):
         "tdv_batch_set_wait_limit": (st, [vp, ctypes.c_double]),
         "tdv_batch_work_queue": (st, [vp, P(vp), P(ctypes.c_int32), P(ctypes.c_int32)]),
         "tdv_to_gray": (st, [vp, P(tdv_raster), vp, vp]),
+        "tdv_rectify_maps": (st, [vp, vp, vp, vp, vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp]),
         "tdv_remap": (st, [vp, P(tdv_raster), vp, vp, P(tdv_raster), vp]),
         "tdv_prefilter": (st, [vp, P(tdv_image), ctypes.c_int32, vp, vp]),
         "tdv_postfilter": (st, [vp, P(tdv_raster), ctypes.c_int32, P(tdv_raster), vp]),

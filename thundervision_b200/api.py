@@ -212,6 +212,23 @@ class Context:
         self.check(L.lib().tdv_to_gray(self.handle, ctypes.byref(_raster(color)), out.data_ptr(), _stream()))
         return out
 
+    def rectify_maps(self, K, dist, R, P, width, height, device=None):
+        """Rectification maps ((H, W) float32 mapx, mapy) of one camera from
+        its intrinsics K (3x3), distortion (k1, k2, p1, p2, k3[, k4, k5, k6]),
+        rectifying rotation R (3x3) and new camera P (3x3 or 3x4)."""
+        import numpy as np
+        K = np.ascontiguousarray(np.asarray(K, np.float64).reshape(3, 3))
+        R = np.ascontiguousarray(np.asarray(R, np.float64).reshape(3, 3))
+        P = np.ascontiguousarray(np.asarray(P, np.float64).reshape(3, -1)[:, :3])
+        d = np.zeros(8)
+        d[:len(dist)] = np.asarray(dist, np.float64)
+        dev = torch.device("cuda", self.device) if device is None else device
+        mx = torch.empty((height, width), dtype=torch.float32, device=dev)
+        my = torch.empty((height, width), dtype=torch.float32, device=dev)
+        self.check(L.lib().tdv_rectify_maps(self.handle, K.ctypes.data, d.ctypes.data, R.ctypes.data, P.ctypes.data,
+                                            width, height, mx.data_ptr(), my.data_ptr(), _stream()))
+        return mx, my
+
     def remap(self, src, mapx, mapy):
         """Rectification remap: src sampled bilinearly at (mapx, mapy), the
         maps (H, W) float32 of the output's size; src (H', W') or (H', W', 3),

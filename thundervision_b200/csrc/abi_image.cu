@@ -61,6 +61,36 @@ tdv_status tdv_to_gray(tdv_ctx* ctx, const tdv_raster* color, float* gray, tdv_s
     return TDV_OK;
 }
 
+tdv_status tdv_rectify_maps(tdv_ctx* ctx, const double* K, const double* dist, const double* R, const double* P,
+                            int32_t width, int32_t height, float* mapx, float* mapy, tdv_stream stream) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    if (!K || !dist || !R || !P || !mapx || !mapy) return fail(ctx, TDV_ERR_INVALID_ARG, "null argument");
+    if (width <= 0 || height <= 0 || width > kMaxSide || height > kMaxSide)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "bad size %dx%d", width, height);
+    for (int i = 0; i < 9; i++)
+        if (!std::isfinite(K[i]) || !std::isfinite(R[i]) || !std::isfinite(P[i]))
+            return fail(ctx, TDV_ERR_INVALID_ARG, "K, R and P must be finite");
+    for (int i = 0; i < 8; i++)
+        if (!std::isfinite(dist[i])) return fail(ctx, TDV_ERR_INVALID_ARG, "distortion must be finite");
+    // M = P[:, :3] R, then its inverse by cofactors
+    double M[9];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++)
+            M[3 * r + c] = (P[3 * r] * R[c] + P[3 * r + 1] * R[3 + c]) + P[3 * r + 2] * R[6 + c];
+    const double a = M[0], b = M[1], c = M[2], d = M[3], e = M[4], f = M[5], g = M[6], h = M[7], i = M[8];
+    const double A = e * i - f * h, B = -(d * i - f * g), C = d * h - e * g;
+    const double det = (a * A + b * B) + c * C;
+    if (!(std::fabs(det) > 0.0) || !std::isfinite(det))
+        return fail(ctx, TDV_ERR_INVALID_ARG, "P[:, :3] R is singular");
+    const double adj[9] = {A, -(b * i - c * h), b * f - c * e, B, a * i - c * g, -(a * f - c * d),
+                           C, -(a * h - b * g), a * e - b * d};
+    double iR[9];
+    for (int k = 0; k < 9; k++) iR[k] = adj[k] / det;
+    TDV_DEVICE_SCOPE(ctx);
+    TDV_CUDA(tdv::launch_rectify_maps(K, dist, iR, width, height, mapx, mapy, S(stream)));
+    return TDV_OK;
+}
+
 tdv_status tdv_remap(tdv_ctx* ctx, const tdv_raster* src, const float* mapx, const float* mapy,
                      tdv_raster* dst, tdv_stream stream) {
     if (!ctx) return TDV_ERR_INVALID_ARG;

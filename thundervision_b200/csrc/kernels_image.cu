@@ -86,6 +86,41 @@ __global__ void remap_kernel(RasterArg src, const float* __restrict__ mx, const 
     }
 }
 
+// ------------------------------------------------------ rectification maps
+struct RectArg {
+    double ir[9];                       // inv(P[:, :3] R), row-major
+    double fx, fy, cx, cy;
+    double k1, k2, p1, p2, k3, k4, k5, k6;
+};
+
+__global__ void rectify_maps_kernel(RectArg a, int W, int H, float* mapx, float* mapy) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (j >= W) return;
+    const double dj = j, di = i;
+    auto lin = [&](int r) {
+        return __dadd_rn(__dadd_rn(__dmul_rn(dj, a.ir[3 * r]), __dmul_rn(di, a.ir[3 * r + 1])), a.ir[3 * r + 2]);
+    };
+    const double w = __ddiv_rn(1.0, lin(2));
+    const double x = __dmul_rn(lin(0), w), y = __dmul_rn(lin(1), w);
+    const double x2 = __dmul_rn(x, x), y2 = __dmul_rn(y, y);
+    const double r2 = __dadd_rn(x2, y2);
+    const double xy2 = __dmul_rn(__dmul_rn(2.0, x), y);
+    auto poly = [&](double c3, double c2, double c1) {  // 1 + ((c3 r2 + c2) r2 + c1) r2
+        return __dadd_rn(1.0, __dmul_rn(__dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(c3, r2), c2), r2), c1), r2));
+    };
+    const double kr = __ddiv_rn(poly(a.k3, a.k2, a.k1), poly(a.k6, a.k5, a.k4));
+    const double u = __dadd_rn(
+        __dmul_rn(a.fx, __dadd_rn(__dadd_rn(__dmul_rn(x, kr), __dmul_rn(a.p1, xy2)),
+                                  __dmul_rn(a.p2, __dadd_rn(r2, __dmul_rn(2.0, x2))))),
+        a.cx);
+    const double v = __dadd_rn(
+        __dmul_rn(a.fy, __dadd_rn(__dadd_rn(__dmul_rn(y, kr), __dmul_rn(a.p1, __dadd_rn(r2, __dmul_rn(2.0, y2)))),
+                                  __dmul_rn(a.p2, xy2))),
+        a.cy);
+    mapx[(size_t)i * W + j] = __double2float_rn(u);
+    mapy[(size_t)i * W + j] = __double2float_rn(v);
+}
+
 // ---------------------------------------------------------------- tiles
 __device__ __forceinline__ float img_clamped(const ImgArg& im, int x, int y) {
     x = min(max(x, 0), im.W - 1);
@@ -309,6 +344,26 @@ dim3 tiles(int W, int H) { return dim3((W + kTX - 1) / kTX, (H + kTY - 1) / kTY)
 
 cudaError_t launch_to_gray(const RasterArg& c, float* gray, cudaStream_t st) {
     to_gray_kernel<<<dim3((c.W + 127) / 128, c.H), 128, 0, st>>>(c, gray);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rectify_maps(const double* K, const double* dist, const double* iR, int W, int H, float* mapx,
+                               float* mapy, cudaStream_t st) {
+    RectArg a;
+    for (int i = 0; i < 9; i++) a.ir[i] = iR[i];
+    a.fx = K[0];
+    a.fy = K[4];
+    a.cx = K[2];
+    a.cy = K[5];
+    a.k1 = dist[0];
+    a.k2 = dist[1];
+    a.p1 = dist[2];
+    a.p2 = dist[3];
+    a.k3 = dist[4];
+    a.k4 = dist[5];
+    a.k5 = dist[6];
+    a.k6 = dist[7];
+    rectify_maps_kernel<<<dim3((W + 127) / 128, H), 128, 0, st>>>(a, W, H, mapx, mapy);
     return cudaGetLastError();
 }
 

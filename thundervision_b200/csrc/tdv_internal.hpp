@@ -203,6 +203,9 @@ size_t fused_agg_bytes(int W, int H, int D);
 
 // Image stages either side of the path (kernels_image.cu).
 cudaError_t launch_to_gray(const RasterArg& color, float* gray, cudaStream_t st);
+// K row-major 3x3, dist (k1 k2 p1 p2 k3 k4 k5 k6), iR = inv(P[:, :3] R) row-major
+cudaError_t launch_rectify_maps(const double* K, const double* dist, const double* iR, int W, int H, float* mapx,
+                               float* mapy, cudaStream_t st);
 cudaError_t launch_remap(const RasterArg& src, const float* mx, const float* my, const RasterArg& dst,
                          cudaStream_t st);
 cudaError_t launch_prefilter(const ImgArg& in, int kind, float* out, cudaStream_t st);
