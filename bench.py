@@ -411,6 +411,50 @@ def measure_image(ctx, dev, reps=10):
     return res
 
 
+def measure_reconstruction(ctx, dev, frames=20, warmup=3):
+    """The reference's reconstruction chain (color frames -> grey -> remap ->
+    Gaussian -> cost -> optimizer -> opening -> Q reprojection with colors) at
+    1920x1080 through reconstruction.Reconstruction, one CUDA graph per frame;
+    each frame's two color frames are copied from pinned host memory inside
+    the timed region.  Two matchers: the factory default (SSD + WTA, D=64)
+    and BT + SGM (the reference's SemiGlobalDev) at D=256."""
+    import numpy as np
+    import torch
+
+    from thundervision_b200 import reconstruction as rc
+    from thundervision_b200 import synthetic
+
+    K = np.array([[1400.0, 0, W / 2 + 0.3], [0, 1398.0, H / 2 - 0.7], [0, 0, 1]])
+    P = np.array([[1380.0, 0, W / 2, 0], [0, 1380.0, H / 2, 0], [0, 0, 1, 0]])
+    cams = [rc.Camera(K, [-0.28, 0.09, 0.0012, -0.0007, -0.011], np.eye(3), P),
+            rc.Camera(K, [-0.27, 0.085, -0.001, 0.0006, -0.01], np.eye(3), P)]
+    Q = [1, 0, 0, -W / 2, 0, 1, 0, -H / 2, 0, 0, 0, 1380.0, 0, 0, -1 / 0.12, 0]
+    Lh, Rh, _, _ = synthetic.make_pair(W, H, D, 17, n_rects=12)
+    col = lambda g: torch.from_numpy(np.stack([g, g // 2 + 64, 255 - g], -1).astype(np.uint8)).pin_memory()
+    lc, rcol = col(Lh), col(Rh)
+    st = torch.cuda.current_stream()
+    res = {"workload": f"{W}x{H} color pair per frame, pinned host -> device inside the timed region; "
+                       f"median of {frames} frames after {warmup}"}
+    for name, cost, opt, d in (("ssd_wta_d64", "ssd", "wta", 64), ("bt_sgm_d256", "bt", "sgm", D)):
+        rec = rc.Reconstruction(ctx, W, H, cams[0], cams[1], Q=Q,
+                                matcher=rc.StereoMatcher(ctx, max_disp=d, cost=cost, optimizer=opt))
+        try:
+            ts = []
+            for i in range(warmup + frames):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                rec.update(lc, rcol)
+                e1.record(st)
+                e1.synchronize()
+                if i >= warmup:
+                    ts.append(e0.elapsed_time(e1))
+            ms = sorted(ts)[len(ts) // 2]
+            res[name] = {"ms_per_frame": ms, "fps": 1000.0 / ms}
+        finally:
+            rec.close()
+    return res
+
+
 def measure_video(ctx, dev, n_frames=300, refit_steps=50):
     """Full-HD video: 300 frames (12 moving rectangles over a slanted plane,
     sensor noise sigma 2), D=256, fused BT + SGM + WTA + L-R check, through a
@@ -698,7 +742,7 @@ def run_ours(args):
     }
     if not args.no_extras:
         for key, fn in (("batch", measure_batch), ("soft", measure_soft), ("plain", measure_plain),
-                        ("image_stages", measure_image),
+                        ("image_stages", measure_image), ("reconstruction", measure_reconstruction),
                         ("video", measure_video)):
             try:
                 line[key] = fn(ctx, dev)

@@ -16,6 +16,15 @@
 //   DynamicProgDev (dynamicprogdev.hpp)         DynamicProgDev
 //   FastWTAMatcher (fastwtamatcher.hpp)         FastWTAMatcher
 //   SemiGlobalLabMatcher (semigloballabmatcher.hpp)  SemiGlobalLabMatcher
+//   misc::create32FGray (misc.cpp:18-32)        create32FGray
+//   RectificationCV, calibrated path            Rectifier (maps once, remap per frame)
+//     (rectificationcv.cpp:114-117, 298-310)
+//   MedianFilterCPU (5x5 Gaussian, medianfiltercpu.cpp:15)  MedianFilterCPU
+//   MedianFilterDev (7x7 median, medianfilter.cu:37-57)     MedianFilterDev
+//   Dilate (dilate.cpp:11-22)                   Dilate
+//   DirectReprojector / CVReprojector           DirectReprojector / CVReprojector
+//     (directreprojector.hpp, cvreprojector.cpp:45-60)
+//   PLYMeshExporter::exportMesh (plymeshexporter.cpp)  PLYMeshExporter
 //
 // The reference's stages pull their inputs from pipes and run on worker
 // threads (workunitprocess.cpp); that runtime is not part of this path, so
@@ -299,6 +308,163 @@ public:
 private:
     MatchingCost& m_cost;
     Optimizer& m_opt;
+};
+
+// ---- stages either side of the matcher -----------------------------------
+// A device raster: an 8-bit color frame, a grey image or a disparity map.
+// pitchBytes 0 means dense rows.
+struct Raster {
+    void* devMem = nullptr;
+    int width = 0, height = 0, pitchBytes = 0;
+    int dtype = TDV_F32;  // TDV_U8, TDV_U16 or TDV_F32
+    int channels = 1;     // 1 or 3
+    tdv_raster abi() const {
+        const int elem = dtype == TDV_U8 ? 1 : dtype == TDV_U16 ? 2 : 4;
+        tdv_raster r;
+        r.ptr = devMem;
+        r.width = width;
+        r.height = height;
+        r.pitch_bytes = pitchBytes > 0 ? pitchBytes : width * channels * elem;
+        r.dtype = dtype;
+        r.channels = channels;
+        return r;
+    }
+};
+
+// 8-bit 3-channel frame -> [0,1] grey intensities (width x height floats).
+inline void create32FGray(Context& ctx, const Raster& color, float* gray, tdv_stream s = nullptr) {
+    tdv_raster c = color.abi();
+    check(ctx.get(), tdv_to_gray(ctx.get(), &c, gray, s));
+}
+
+// One camera of RectificationCV's calibrated path: the undistort-rectify maps
+// are computed once on the device into caller-owned buffers (width x height
+// floats each), then every frame is remapped through them.
+class Rectifier {
+public:
+    Rectifier(Context& ctx, float* mapx, float* mapy) : m_ctx(ctx), m_mapx(mapx), m_mapy(mapy) {}
+    // K, R, P row-major 3x3 (P's first three columns); dist (k1, k2, p1, p2,
+    // k3, k4, k5, k6), zeros for unused terms
+    void camera(const double K[9], const double dist[8], const double R[9], const double P[9], int width,
+                int height, tdv_stream s = nullptr) {
+        check(m_ctx.get(), tdv_rectify_maps(m_ctx.get(), K, dist, R, P, width, height, m_mapx, m_mapy, s));
+        m_width = width;
+        m_height = height;
+    }
+    // dst must be width x height (the maps' size), same dtype and channels as src
+    void update(const Raster& src, Raster& dst, tdv_stream s = nullptr) const {
+        if (dst.width != m_width || dst.height != m_height)
+            throw CUException(TDV_ERR_INVALID_ARG, "Rectifier: destination size differs from the maps'");
+        tdv_raster a = src.abi(), b = dst.abi();
+        check(m_ctx.get(), tdv_remap(m_ctx.get(), &a, m_mapx, m_mapy, &b, s));
+    }
+    const float* mapx() const { return m_mapx; }
+    const float* mapy() const { return m_mapy; }
+
+private:
+    Context& m_ctx;
+    float *m_mapx, *m_mapy;
+    int m_width = -1, m_height = -1;
+};
+
+// Pre-filters, FloatImage -> FloatImage (out: width x height floats).
+class PreFilter {
+public:
+    PreFilter(Context& ctx, tdv_filter_kind kind) : m_ctx(ctx), m_kind(kind) {}
+    void update(const FloatImage& in, float* out, tdv_stream s = nullptr) {
+        tdv_image im = in.abi();
+        check(m_ctx.get(), tdv_prefilter(m_ctx.get(), &im, m_kind, out, s));
+    }
+    // 8-bit input, filtered intensities multiplied by `scale`
+    void update(const ByteImage& in, float scale, float* out, tdv_stream s = nullptr) {
+        tdv_image im = in.abi();
+        im.scale = scale;
+        check(m_ctx.get(), tdv_prefilter(m_ctx.get(), &im, m_kind, out, s));
+    }
+
+private:
+    Context& m_ctx;
+    tdv_filter_kind m_kind;
+};
+
+class MedianFilterCPU : public PreFilter {
+public:
+    explicit MedianFilterCPU(Context& ctx) : PreFilter(ctx, TDV_FILTER_GAUSS5) {}
+};
+
+class MedianFilterDev : public PreFilter {
+public:
+    explicit MedianFilterDev(Context& ctx) : PreFilter(ctx, TDV_FILTER_MEDIAN7) {}
+};
+
+// Post-filters of a disparity map (F32 or U16, one channel); in and out have
+// the same size and dtype and do not overlap.
+class PostFilter {
+public:
+    PostFilter(Context& ctx, tdv_post_kind kind) : m_ctx(ctx), m_kind(kind) {}
+    void update(const Raster& in, Raster& out, tdv_stream s = nullptr) {
+        tdv_raster a = in.abi(), b = out.abi();
+        check(m_ctx.get(), tdv_postfilter(m_ctx.get(), &a, m_kind, &b, s));
+    }
+
+private:
+    Context& m_ctx;
+    tdv_post_kind m_kind;
+};
+
+class Dilate : public PostFilter {
+public:
+    explicit Dilate(Context& ctx) : PostFilter(ctx, TDV_POST_OPEN7) {}
+};
+
+// Disparity map -> grid mesh: one vertex (3 floats) per pixel and, when a
+// color frame is given, one color (3 floats in [0,1]) per pixel, as
+// GLReprojection::updateMesh fills its mesh (device buffers).
+class Reprojector {
+public:
+    virtual ~Reprojector() {}
+    void reproject(Context& ctx, const Raster& disp, const Raster* color, float* vertices, float* colors,
+                   tdv_stream s = nullptr) const {
+        tdv_raster d = disp.abi(), c;
+        if (color) c = color->abi();
+        tdv_reproject_params p = m_params;
+        check(ctx.get(), tdv_reproject(ctx.get(), &d, color ? &c : nullptr, &p, vertices, colors, s));
+    }
+
+protected:
+    tdv_reproject_params m_params{};
+};
+
+class DirectReprojector : public Reprojector {
+public:
+    explicit DirectReprojector(float zscale = 1.0f) {
+        m_params.mode = TDV_REPROJECT_DIRECT;
+        m_params.zscale = zscale;
+    }
+};
+
+class CVReprojector : public Reprojector {
+public:
+    CVReprojector() { m_params.mode = TDV_REPROJECT_Q; }
+    void qmatrix(const float mtx[16]) {
+        for (int i = 0; i < 16; i++) m_params.q[i] = mtx[i];
+    }
+    const float* qmatrix() const { return m_params.q; }
+};
+
+// Writes a grid mesh (HOST vertices and optional colors, as Reprojector lays
+// them out) to the reference's ASCII PLY.
+class PLYMeshExporter {
+public:
+    explicit PLYMeshExporter(const std::string& name) : m_filename(name) {}
+    void exportMesh(const float* vertices, const float* colors, int width, int height) const {
+        check(nullptr, tdv_write_ply(m_filename.c_str(), vertices, colors, width, height));
+    }
+    void filename(const std::string& fname) { m_filename = fname; }
+    const std::string& filename() const { return m_filename; }
+
+private:
+    std::string m_filename;
 };
 
 }  // namespace tdv_b200

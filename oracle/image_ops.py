@@ -226,3 +226,35 @@ def ply_text(vertices, colors=None):
             a, b = row * W + col, (row + 1) * W + col
             lines.append(f"4 {a} {b} {b + 1} {a + 1} ")
     return "\n".join(lines) + "\n"
+
+
+def reconstruction(left, right, cams, D, q=None, zscale=1.0, cost="ssd", optimizer="wta", median_filter=True,
+                   dilate=True):
+    """The reference's reconstruction chain on one pair of 8-bit 3-channel
+    frames (tdvision/reconstruction.cpp:9-55): grey conversion and remap of
+    both frames and of the left color frame (rectificationcv.cpp:258-310), the
+    DevStereoMatcher (5x5 Gaussian, cost, optimizer; devstereomatcher.cpp:13-48,
+    commonstereomatcherfactory.cpp:40-80) giving d/D, the opening (dilate.cpp),
+    then the reprojection with the rectified left colors.  ``cams`` holds
+    (K, dist, R, P) of each camera.  Returns (rectified left color, d/D map,
+    vertices, colors)."""
+    import oracle as orc
+    H, W = left.shape[:2]
+    maps = [rectify_maps(K, dist, R, P, W, H) for (K, dist, R, P) in cams]
+    gl = remap(to_gray(left), *maps[0])
+    gr = remap(to_gray(right), *maps[1])
+    cl = remap(left, *maps[0])
+    if median_filter:
+        gl, gr = gauss5(gl), gauss5(gr)
+    C = {"ssd": orc.ssd_cost, "ncc": orc.ncc_cost, "bt": orc.bt_cost}[cost](gl, gr, D)
+    if optimizer == "wta":
+        _, dn = orc.wta(C)
+    elif optimizer == "dp":
+        _, dn = orc.dp(C)
+    else:
+        _, dn, _ = orc.sgm(C, gl, 30.0 / 255.0, 150.0 / 255.0, p2_mode=orc.P2_ADJUST, table=orc.TABLE_REF,
+                           semantics=orc.SEM_REF_GPU, want_S=False)
+    if dilate:
+        dn = open7(dn)
+    v, c = reproject(dn, cl, "q" if q is not None else "direct", zscale, q)
+    return cl, dn, v, c

@@ -8,6 +8,13 @@
 //       BirchfieldCostDev -> SemiGlobalCPU / SemiGlobalDev -> maps, the
 //       fused SemiGlobalLabMatcher, FastWTAMatcher and DynamicProgDev on the
 //       pair; writes out_prefix.{lab,sgm_ref_cpu,sgm_ref_gpu,fastwta,dp}.u16
+//   stages_demo reconstruct W H D left.rgb right.rgb cams.f64 out_prefix
+//       the reference's reconstruction chain from 8-bit 3-channel frames:
+//       create32FGray -> Rectifier (both cameras, and the left color frame)
+//       -> MedianFilterCPU -> SSDDev + WTADev (d/D map) -> Dilate ->
+//       CVReprojector -> PLYMeshExporter.  cams.f64 holds K, dist (8), R, P
+//       (3x3) of the left then the right camera, then Q (4x4).  Writes
+//       out_prefix.{disp,verts,cols}.f32 and out_prefix.ply
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -68,6 +75,23 @@ static int validate() {
         Disparity out;
         out.disp = d;
         f.update(l, r, out);
+    }, ctx);
+    bad += expect_throw("rectifier size", TDV_ERR_INVALID_ARG, [](Context& c) {
+        static float mx[64], my[64];
+        Rectifier r(c, mx, my);  // no camera yet: any destination size is wrong
+        static unsigned char px[64];
+        Raster src{px, 8, 8, 0, TDV_U8, 1}, dst{px, 8, 8, 0, TDV_U8, 1};
+        r.update(src, dst);
+    }, ctx);
+    bad += expect_throw("dilate dtype", TDV_ERR_INVALID_ARG, [](Context& c) {
+        Dilate d(c);
+        static unsigned char a[64], b[64];
+        Raster in{a, 8, 8, 0, TDV_U8, 1}, out{b, 8, 8, 0, TDV_U8, 1};
+        d.update(in, out);
+    }, ctx);
+    bad += expect_throw("ply path", TDV_ERR_INVALID_ARG, [](Context&) {
+        PLYMeshExporter e("");
+        e.exportMesh(nullptr, nullptr, 2, 2);
     }, ctx);
     std::printf(bad ? "validate: FAILED\n" : "validate: ok\n");
     return bad ? 1 : 0;
@@ -159,10 +183,91 @@ static int run(int W, int H, int D, const char* lp, const char* rp, const std::s
     return 0;
 }
 
+template <typename T>
+static void write_dev(const std::string& path, const T* dev, size_t n) {
+    std::vector<T> h(n);
+    cudaMemcpy(h.data(), dev, n * sizeof(T), cudaMemcpyDeviceToHost);
+    FILE* f = std::fopen(path.c_str(), "wb");
+    std::fwrite(h.data(), sizeof(T), n, f);
+    std::fclose(f);
+}
+
+static int reconstruct(int W, int H, int D, const char* lp, const char* rp, const char* cp,
+                       const std::string& out) {
+    const size_t n = (size_t)W * H;
+    std::vector<unsigned char> lh = read_file(lp, 3 * n), rh = read_file(rp, 3 * n);
+    std::vector<unsigned char> cb = read_file(cp, sizeof(double) * (2 * 35 + 16));
+    const double* cams = (const double*)cb.data();
+    unsigned char *lc = dev_alloc<unsigned char>(3 * n), *rc = dev_alloc<unsigned char>(3 * n);
+    unsigned char* lrect = dev_alloc<unsigned char>(3 * n);
+    cudaMemcpy(lc, lh.data(), 3 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(rc, rh.data(), 3 * n, cudaMemcpyHostToDevice);
+    float *gray = dev_alloc<float>(n), *grect[2] = {dev_alloc<float>(n), dev_alloc<float>(n)};
+    float *filt[2] = {dev_alloc<float>(n), dev_alloc<float>(n)};
+    float *maps[4] = {dev_alloc<float>(n), dev_alloc<float>(n), dev_alloc<float>(n), dev_alloc<float>(n)};
+    float *vol = dev_alloc<float>(n * D), *disp = dev_alloc<float>(n), *opened = dev_alloc<float>(n);
+    float *verts = dev_alloc<float>(3 * n), *cols = dev_alloc<float>(3 * n);
+
+    Context ctx(0);
+    Rectifier rect[2] = {Rectifier(ctx, maps[0], maps[1]), Rectifier(ctx, maps[2], maps[3])};
+    unsigned char* frames[2] = {lc, rc};
+    for (int c = 0; c < 2; c++) {
+        const double* k = cams + 35 * c;
+        rect[c].camera(k, k + 9, k + 17, k + 26, W, H);
+        Raster color{frames[c], W, H, 0, TDV_U8, 3};
+        create32FGray(ctx, color, gray);
+        Raster g{gray, W, H, 0, TDV_F32, 1}, gr{grect[c], W, H, 0, TDV_F32, 1};
+        rect[c].update(g, gr);
+        MedianFilterCPU gauss(ctx);
+        gauss.update(FloatImage{grect[c], W, H}, filt[c]);
+    }
+    Raster lcol{lc, W, H, 0, TDV_U8, 3}, lrc{lrect, W, H, 0, TDV_U8, 3};
+    rect[0].update(lcol, lrc);
+
+    SSDDev ssd(ctx, D);
+    WTADev wta(ctx);
+    StereoMatcher matcher(ssd, wta);
+    DSIMem dsi;
+    dsi.devMem = vol;
+    dsi.width = W;
+    dsi.height = H;
+    dsi.depth = D;
+    dsi.layout = TDV_LAYOUT_HWD;
+    Disparity o;
+    o.dispNorm = disp;
+    matcher.update(FloatImage{filt[0], W, H}, FloatImage{filt[1], W, H}, dsi, o);
+
+    Dilate dilate(ctx);
+    Raster din{disp, W, H, 0, TDV_F32, 1}, dout{opened, W, H, 0, TDV_F32, 1};
+    dilate.update(din, dout);
+
+    CVReprojector repr;
+    float q[16];
+    for (int i = 0; i < 16; i++) q[i] = (float)cams[70 + i];
+    repr.qmatrix(q);
+    repr.reproject(ctx, dout, &lrc, verts, cols);
+    ctx.deviceStatus();
+
+    write_dev(out + ".disp.f32", opened, n);
+    write_dev(out + ".verts.f32", verts, 3 * n);
+    write_dev(out + ".cols.f32", cols, 3 * n);
+    std::vector<float> hv(3 * n), hc(3 * n);
+    cudaMemcpy(hv.data(), verts, 3 * n * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(hc.data(), cols, 3 * n * 4, cudaMemcpyDeviceToHost);
+    PLYMeshExporter(out + ".ply").exportMesh(hv.data(), hc.data(), W, H);
+    std::printf("reconstruct: ok\n");
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc >= 2 && std::strcmp(argv[1], "validate") == 0) return validate();
     if (argc == 8 && std::strcmp(argv[1], "run") == 0)
         return run(std::atoi(argv[2]), std::atoi(argv[3]), std::atoi(argv[4]), argv[5], argv[6], argv[7]);
-    std::fprintf(stderr, "usage: stages_demo validate | run W H D left.u8 right.u8 out_prefix\n");
+    if (argc == 9 && std::strcmp(argv[1], "reconstruct") == 0)
+        return reconstruct(std::atoi(argv[2]), std::atoi(argv[3]), std::atoi(argv[4]), argv[5], argv[6], argv[7],
+                           argv[8]);
+    std::fprintf(stderr,
+                 "usage: stages_demo validate | run W H D left.u8 right.u8 out_prefix |"
+                 " reconstruct W H D left.rgb right.rgb cams.f64 out_prefix\n");
     return 2;
 }

@@ -3,7 +3,8 @@ LibThunderVision's stage plugins (tdvision/matchingcost.hpp:48-49,
 tdvision/optimizer.hpp:46) -- compiled with g++ against libtdvb200.so.
 
 CPU: the header compiles and bad arguments throw CUException with the ABI's
-status before any CUDA call.  GPU: the stage chains give the oracle's maps on
+status before any CUDA call (the matcher stages, the rectifier, the dilation
+and the PLY exporter).  GPU: the stage chains give the oracle's maps on
 the same pair (REF_CPU / REF_GPU SGM with the reference's table, P2 adjusted
 by the intensity step, BT cost in [0,1] intensities; DP; FastWTA; the fused
 Lab-style matcher).
@@ -22,12 +23,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CUDA = "/usr/local/cuda"
 
 
-@pytest.fixture(scope="module")
-def demo(tmp_path_factory):
+def build_demo(out):
+    """Compiles tests/cpp/stages_demo.cpp against libtdvb200.so into `out`."""
     L.build()
     if shutil.which("g++") is None:
         pytest.skip("g++ not available")
-    out = str(tmp_path_factory.mktemp("cpp") / "stages_demo")
     libdir = os.path.dirname(L.LIB_PATH)
     cmd = ["g++", "-std=c++17", "-O1", "-I" + os.path.join(ROOT, "include"), "-I" + CUDA + "/include",
            os.path.join(ROOT, "tests", "cpp", "stages_demo.cpp"), "-L" + libdir, "-ltdvb200",
@@ -35,6 +35,11 @@ def demo(tmp_path_factory):
            "-o", out]
     subprocess.run(cmd, check=True)
     return out
+
+
+@pytest.fixture(scope="module")
+def demo(tmp_path_factory):
+    return build_demo(str(tmp_path_factory.mktemp("cpp") / "stages_demo"))
 
 
 def test_stage_classes_validate_before_cuda(demo):

@@ -149,3 +149,32 @@ def test_image_stage_arguments_are_validated():
         assert lib.tdv_rectify_maps(h, z, d8, z, z, 4, 4, 1 << 21, 1 << 22, None) == L.TDV_ERR_INVALID_ARG
     finally:
         lib.tdv_ctx_destroy(h)
+
+
+def test_reconstruction_chain_with_identity_rectification(orc):
+    # K = P, R = I, no distortion: the maps are the pixel grid and the remap
+    # the identity, so the chain is gauss5 -> SSD -> WTA -> opening -> direct
+    rng = np.random.default_rng(3)
+    H, W, D = 12, 20, 4
+    lc = rng.integers(0, 256, (H, W, 3), dtype=np.uint8)
+    rc = np.roll(lc, -2, axis=1)
+    K = np.array([[50.0, 0, 9.5], [0, 50.0, 6.0], [0, 0, 1]])
+    cam = (K, [0.0] * 5, np.eye(3), K)
+    mx, my = io.rectify_maps(*cam, W, H)
+    assert np.array_equal(mx, np.broadcast_to(np.arange(W, dtype=np.float32), (H, W)))
+    cl, dn, v, c = io.reconstruction(lc, rc, (cam, cam), D, zscale=2.0)
+    assert np.array_equal(cl, lc)
+    _, dref = orc.wta(orc.ssd_cost(io.gauss5(io.to_gray(lc)), io.gauss5(io.to_gray(rc)), D))
+    assert np.array_equal(dn, io.open7(dref))
+    assert np.array_equal(v[..., 2], dn * np.float32(2.0))
+    assert np.all(dn[:, 6:] == np.float32(2 / D))  # the 2-pixel shift, away from the left border
+
+
+def test_reconstruction_arguments():
+    from thundervision_b200 import reconstruction as rc
+    with pytest.raises(ValueError):
+        rc.StereoMatcher(None, cost="census")
+    with pytest.raises(ValueError):
+        rc.StereoMatcher(None, optimizer="graphcut")
+    with pytest.raises(ValueError):
+        rc.Camera(np.eye(3), [0.0] * 9, np.eye(3), np.eye(3))

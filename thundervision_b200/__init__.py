@@ -2,8 +2,11 @@
 -> SGM / DP aggregation -> WTA, behind the C ABI in include/tdv_stereo.h.
 
 The compute runs only in libtdvb200.so (hand-written CUDA); this package is
-its Python front end.  ``Context`` wraps one tdv_ctx; ``stages`` mirrors the
-reference's MatchingCost / Optimizer plugin classes.
+its Python front end.  ``Context`` wraps one tdv_ctx (``api``); ``Batch``
+runs many pairs per launch; ``video`` streams frames through graph replays;
+``soft`` is the differentiable SGM; ``reconstruction`` chains the stages
+either side of the matcher as the reference's Reconstruction does.  The C++
+stage classes mirroring the reference's plugins are in include/tdv_stages.hpp.
 """
 from ._lib import TdvError, build, lib  # noqa: F401
 
