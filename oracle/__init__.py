@@ -32,9 +32,9 @@ _i32p = ctypes.POINTER(ctypes.c_int32)
 
 
 def build(force=False):
-    """Compile liborc.so with the recipe in oracle/Makefile."""
-    if force or not os.path.exists(_LIB):
-        subprocess.check_call(["make", "-s", "-C", _HERE])
+    """Compile liborc.so with the recipe in oracle/Makefile (make rebuilds it
+    when tdv_oracle.cpp is newer)."""
+    subprocess.check_call(["make", "-s", "-C", _HERE] + (["-B"] if force else []))
 
 
 def lib():
@@ -87,6 +87,17 @@ def ncc_cost(L, R, D, radius=1, layout=LAYOUT_HWD):
     H, W = L.shape
     out = _vol(W, H, D, layout)
     lib().orc_ncc_cost(_p(L, _f32p), _p(R, _f32p), W, H, D, radius, layout, _p(out, _f32p))
+    return out
+
+
+def cost_pair(L, R, D, kind, radius=0, layout=LAYOUT_HWD):
+    """BT / SSD / NCC (kind 0 / 1 / 2) for images of different sizes: the
+    DSI is the smaller size, each image's taps clamp to its own edges."""
+    L, R = _img(L), _img(R)
+    W, H = min(L.shape[1], R.shape[1]), min(L.shape[0], R.shape[0])
+    out = _vol(W, H, D, layout)
+    lib().orc_cost_pair(_p(L, _f32p), L.shape[1], L.shape[0], _p(R, _f32p), R.shape[1], R.shape[0], D, kind,
+                        radius, layout, _p(out, _f32p))
     return out
 
 

@@ -61,15 +61,23 @@ inline float fmx(float a, float b) { return std::fmax(a, b); }
 // std::min / std::max: (b < a) ? b : a.
 inline float smin(float a, float b) { return (b < a) ? b : a; }
 
+// An image with its own size: taps clamp to each image's own edges (the DSI
+// takes the smaller size, tdvision/matchingcost.cpp:20-24).
+struct Img {
+    const float* p;
+    int W, H;
+    float at(int x, int y) const { return tex(p, W, H, x, y); }
+};
+
 // tdvision/birchfieldcost.cu:14-39 (costAtDisp), one tap (v == x).
-float bt_at(const float* L, const float* R, int W, int H, int x, int y, int disp) {
+float bt_at(const Img& L, const Img& R, int x, int y, int disp) {
     float sum = 0.0f;
-    const float lI = tex(L, W, H, x, y);
-    const float rI = tex(R, W, H, x - disp, y);
-    const float laI = 0.5f * (lI + tex(L, W, H, x - 1, y));
-    const float lbI = 0.5f * (lI + tex(L, W, H, x + 1, y));
-    const float raI = 0.5f * (rI + tex(R, W, H, x - disp - 1, y));
-    const float rbI = 0.5f * (rI + tex(R, W, H, x - disp + 1, y));
+    const float lI = L.at(x, y);
+    const float rI = R.at(x - disp, y);
+    const float laI = 0.5f * (lI + L.at(x - 1, y));
+    const float lbI = 0.5f * (lI + L.at(x + 1, y));
+    const float raI = 0.5f * (rI + R.at(x - disp - 1, y));
+    const float rbI = 0.5f * (rI + R.at(x - disp + 1, y));
     const float lImi = fmn(laI, fmn(lbI, lI));
     const float lIma = fmx(laI, fmx(lbI, lI));
     const float rImi = fmn(raI, fmn(rbI, rI));
@@ -80,12 +88,12 @@ float bt_at(const float* L, const float* R, int W, int H, int x, int y, int disp
 }
 
 // tdvision/ssd.cu:15-29 (ssdAtDisp): rows then columns in [-r, r].
-float ssd_at(const float* L, const float* R, int W, int H, int x, int y, int disp, int r) {
+float ssd_at(const Img& L, const Img& R, int x, int y, int disp, int r) {
     float sum = 0.0f;
     for (int row = -r; row <= r; row++)
         for (int col = -r; col <= r; col++) {
-            const float lI = tex(L, W, H, x + col, y + row);
-            const float rI = tex(R, W, H, x + col - disp, y + row);
+            const float lI = L.at(x + col, y + row);
+            const float rI = R.at(x + col - disp, y + row);
             const float df = lI - rI;
             const float sq = df * df;
             sum = sum + sq;
@@ -94,12 +102,12 @@ float ssd_at(const float* L, const float* R, int W, int H, int x, int y, int dis
 }
 
 // tdvision/crosscorrelation.cu:11-28 (ccAtDisp): un-centred NCC.
-float ncc_at(const float* L, const float* R, int W, int H, int x, int y, int disp, int r) {
+float ncc_at(const Img& L, const Img& R, int x, int y, int disp, int r) {
     float dom = 0.0f, ls = 0.0f, rs = 0.0f;
     for (int row = -r; row <= r; row++)
         for (int col = -r; col <= r; col++) {
-            const float lv = tex(L, W, H, x + col, y + row);
-            const float rv = tex(R, W, H, x + col - disp, y + row);
+            const float lv = L.at(x + col, y + row);
+            const float rv = R.at(x + col - disp, y + row);
             const float lr = lv * rv;
             const float ll = lv * lv;
             const float rr = rv * rv;
@@ -246,7 +254,7 @@ bool family_enabled(int dx, int dy, int paths) {
 
 extern "C" {
 
-int orc_version() { return 3; }
+int orc_version() { return 4; }
 
 // Grey u8 -> float intensity: v * scale (scale = 1 for the integer domain,
 // 1/255 for the reference domain of misc.cpp:31-32).
@@ -261,7 +269,7 @@ void orc_bt_cost(const float* L, const float* R, int W, int H, int D, int layout
     for (int y = 0; y < H; y++)
         for (int x = 0; x < W; x++)
             for (int d = 0; d < D; d++)
-                out[g.off(x, y, d)] = (x - d >= 0) ? bt_at(L, R, W, H, x, y, d) : kInf;
+                out[g.off(x, y, d)] = (x - d >= 0) ? bt_at(Img{L, W, H}, Img{R, W, H}, x, y, d) : kInf;
 }
 
 // tdvision/ssd.cu:32-50 (ssdKern): INF where x-d<0; window radius r (3 = 7x7).
@@ -271,7 +279,7 @@ void orc_ssd_cost(const float* L, const float* R, int W, int H, int D, int r, in
     for (int y = 0; y < H; y++)
         for (int x = 0; x < W; x++)
             for (int d = 0; d < D; d++)
-                out[g.off(x, y, d)] = (x - d >= 0) ? ssd_at(L, R, W, H, x, y, d, r) : kInf;
+                out[g.off(x, y, d)] = (x - d >= 0) ? ssd_at(Img{L, W, H}, Img{R, W, H}, x, y, d, r) : kInf;
 }
 
 // tdvision/crosscorrelation.cu:30-49 (ccorrelationKern): nDisps = min(D, x+1),
@@ -282,7 +290,27 @@ void orc_ncc_cost(const float* L, const float* R, int W, int H, int D, int r, in
     for (int y = 0; y < H; y++)
         for (int x = 0; x < W; x++)
             for (int d = 0; d < D; d++)
-                out[g.off(x, y, d)] = (d < x + 1) ? ncc_at(L, R, W, H, x, y, d, r) : kInf;
+                out[g.off(x, y, d)] = (d < x + 1) ? ncc_at(Img{L, W, H}, Img{R, W, H}, x, y, d, r) : kInf;
+}
+
+// Any of the three costs for a pair of different sizes: the DSI is the
+// smaller width x height, each image's taps clamp to its own edges.
+// kind: 0 BT, 1 SSD, 2 NCC (tdv_cost_kind).
+void orc_cost_pair(const float* L, int LW, int LH, const float* R, int RW, int RH, int D, int kind, int r,
+                   int layout, float* out) {
+    const int W = std::min(LW, RW), H = std::min(LH, RH);
+    Geo g{W, H, D, layout};
+    const Img li{L, LW, LH}, ri{R, RW, RH};
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++)
+            for (int d = 0; d < D; d++) {
+                float v = kInf;
+                if (x - d >= 0)
+                    v = kind == 0 ? bt_at(li, ri, x, y, d) : kind == 1 ? ssd_at(li, ri, x, y, d, r)
+                                                                       : ncc_at(li, ri, x, y, d, r);
+                out[g.off(x, y, d)] = v;
+            }
 }
 
 int orc_path_count(int W, int H) { return W + H + 2 * (W + H - 1); }
@@ -469,7 +497,7 @@ void orc_fastwta(const float* L, const float* R, int W, int H, int D, int r,
             int bd = 0;
             const int nd = std::min(D, x + 1);
             for (int d = 0; d < nd; d++) {
-                const float v = ssd_at(L, R, W, H, x, y, d, r);
+                const float v = ssd_at(Img{L, W, H}, Img{R, W, H}, x, y, d, r);
                 if (v < best) { best = v; bd = d; }
             }
             if (disp_norm) disp_norm[(size_t)W * y + x] = float(bd) / float(D);

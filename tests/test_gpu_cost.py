@@ -1,0 +1,64 @@
+"""The matching-cost DSI kernels (tdv_cost: BT, SSD, NCC) against the oracle,
+bit for bit (NaN where the oracle has NaN, +INF where x - d < 0), over the
+shapes that exercise the banded kernels' edges: tiles cut by the image,
+disparity ranges below, at and above a warp, both DSI layouts, u8 images with
+the 1/255 scale and float images with padded rows, and left / right images of
+different sizes (each clamps to its own edges).  Radius 5 takes the per-cell
+kernel and is checked the same way."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+KINDS = [("bt", 0), ("ssd", 1), ("ssd", 2), ("ssd", 3), ("ssd", 4), ("ssd", 5),
+         ("ncc", 1), ("ncc", 2), ("ncc", 4), ("ncc", 5)]
+KIND_ID = {"bt": 0, "ssd": 1, "ncc": 2}
+SHAPES = [((1, 1), (1, 1)), ((5, 7), (5, 7)), ((9, 70), (12, 75)), ((37, 130), (35, 129))]
+
+
+def padded(a, extra=3):
+    H, W = a.shape
+    t = torch.zeros((H, W + extra), dtype=torch.from_numpy(a[:1]).dtype, device="cuda")
+    t[:, :W] = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    return t[:, :W]
+
+
+@pytest.mark.parametrize("kind,radius", KINDS)
+@pytest.mark.parametrize("D", [1, 3, 8, 16, 17, 33, 64, 100])
+def test_cost_bit_exact(ctx, orc, kind, radius, D):
+    rng = np.random.default_rng(D * 100 + radius * 10 + KIND_ID[kind])
+    for i, ((lh, lw), (rh, rw)) in enumerate(SHAPES):
+        L8 = rng.integers(0, 256, (lh, lw), dtype=np.uint8)
+        R8 = rng.integers(0, 256, (rh, rw), dtype=np.uint8)
+        if i == 2:
+            L8[:, :5] = 0  # all-zero NCC windows: NaN
+            R8[:, :9] = 0
+        for layout in ("hwd", "ref"):
+            lay = orc.LAYOUT_HWD if layout == "hwd" else orc.LAYOUT_REF_WHD
+            if (i + (layout == "ref")) % 2 == 0:
+                s = np.float32(1.0) / np.float32(255.0)
+                C = ctx.cost(torch.from_numpy(L8).cuda(), torch.from_numpy(R8).cuda(), D, kind=kind, radius=radius,
+                             layout=layout, scale=float(s))
+                Lf, Rf = orc.u8_to_f32(L8, s), orc.u8_to_f32(R8, s)
+            else:
+                Lf = rng.random((lh, lw), dtype=np.float32)
+                Rf = rng.random((rh, rw), dtype=np.float32)
+                C = ctx.cost(padded(Lf), padded(Rf), D, kind=kind, radius=radius, layout=layout)
+            ref = orc.cost_pair(Lf, Rf, D, KIND_ID[kind], radius, lay)
+            torch.cuda.synchronize()
+            got = C.cpu().numpy()
+            assert got.shape == ref.shape
+            assert np.array_equal(got, ref, equal_nan=True), f"{kind} r={radius} D={D} shape={i} {layout}"
+
+
+@pytest.mark.parametrize("kind,radius", [("bt", 0), ("ssd", 3), ("ncc", 4)])
+def test_cost_large_d(ctx, orc, kind, radius):
+    # D = 256 over a frame wider than four tiles: every band column offset
+    rng = np.random.default_rng(3)
+    L8 = rng.integers(0, 256, (21, 300), dtype=np.uint8)
+    R8 = rng.integers(0, 256, (21, 300), dtype=np.uint8)
+    C = ctx.cost(torch.from_numpy(L8).cuda(), torch.from_numpy(R8).cuda(), 256, kind=kind, radius=radius)
+    ref = orc.cost_pair(orc.u8_to_f32(L8), orc.u8_to_f32(R8), 256, KIND_ID[kind], radius)
+    torch.cuda.synchronize()
+    assert np.array_equal(C.cpu().numpy(), ref, equal_nan=True)

@@ -292,3 +292,21 @@ def test_soft_sgm_gradcheck_fp64(orc):
     assert d1 == pytest.approx((f(C, 1.3 + eps) - f(C, 1.3 - eps)) / (2 * eps), rel=1e-5, abs=1e-8)
     assert d2 == pytest.approx((f(C, p2=4.1 + eps) - f(C, p2=4.1 - eps)) / (2 * eps), rel=1e-5,
                                abs=1e-8)
+
+
+def test_cost_pair_equals_the_equal_size_costs(orc):
+    # the different-size entry point reduces to the three cost functions
+    rng = np.random.default_rng(12)
+    L = rng.random((9, 23), dtype=np.float32)
+    R = rng.random((9, 23), dtype=np.float32)
+    for layout in (orc.LAYOUT_HWD, orc.LAYOUT_REF_WHD):
+        assert np.array_equal(orc.cost_pair(L, R, 6, 0, 0, layout), orc.bt_cost(L, R, 6, layout))
+        assert np.array_equal(orc.cost_pair(L, R, 6, 1, 2, layout), orc.ssd_cost(L, R, 6, 2, layout))
+        assert np.array_equal(orc.cost_pair(L, R, 6, 2, 1, layout), orc.ncc_cost(L, R, 6, 1, layout), equal_nan=True)
+    # a wider right image: the DSI is the left's width and the right taps
+    # read past it instead of clamping
+    R2 = np.concatenate([R, rng.random((9, 4), dtype=np.float32)], axis=1)
+    a = orc.cost_pair(L, R2, 6, 1, 2)
+    assert a.shape == (9, 23, 6)
+    assert not np.array_equal(a, orc.ssd_cost(L, R, 6, 2))
+    assert np.array_equal(a[:, :20], orc.ssd_cost(L, R, 6, 2)[:, :20])

@@ -1,0 +1,284 @@
+// Matching-cost DSI writers, banded: Birchfield-Tomasi (tdvision/birchfieldcost.cu:14-59),
+// window SSD (ssd.cu:15-50) and un-centred NCC (crosscorrelation.cu:11-49).
+//
+// One CTA owns a tile of kTX x kTY pixels and all D disparities of them.
+//   * Staging: the rows the tile's windows touch are read once, clamped to
+//     each image's own edges and multiplied by its scale exactly as the
+//     per-cell reference fetch does, into shared memory: raw bands for SSD /
+//     NCC; for BT the per-pixel left terms (I, min, max of I and its two
+//     half-sums) and the per-column right terms, which depend on x - d only.
+//     NCC also stages the window sums of l^2 (per pixel) and r^2 (per column
+//     x - d), summed in the reference's tap order.
+//   * Compute: warp lanes are disparities (32 per warp, or 8 / 16 with two
+//     or four pixel groups per warp when D is small) and each thread walks
+//     P consecutive pixels, so the right-band reads of a warp are 32
+//     consecutive words (no bank conflict) and the left-band reads are
+//     broadcasts.  Across the P pixels of a thread the tap values of one
+//     window row depend only on the column, so each squared difference
+//     (SSD) or product (NCC) is formed once per column and then accumulated
+//     into every pixel whose window holds it -- in each pixel's own row-major
+//     tap order, so every cell is rounded exactly as the reference's loop
+//     rounds it.
+//   * Stores: a warp writes the D-contiguous run of one pixel, a full
+//     128-byte line per instruction in either DSI layout.
+// Cells with x - d < 0 are +INF (the reference's range rule).
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include <cstdint>
+
+#include "tdv_internal.hpp"
+
+namespace tdv {
+
+namespace {
+
+constexpr int kTX = 64;           // tile width (pixels)
+constexpr int kTY = 4;            // tile height (rows)
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxBandBytes = 100 * 1024;
+
+__device__ __forceinline__ float fetch(const ImgArg& im, int x, int y) {
+    x = min(max(x, 0), im.W - 1);
+    y = min(max(y, 0), im.H - 1);
+    const size_t o = (size_t)y * im.pitch + x;
+    if (im.u8) return __fmul_rn((float)((const uint8_t*)im.ptr)[o], im.scale);
+    return __fmul_rn(((const float*)im.ptr)[o], im.scale);
+}
+
+struct Geom {
+    int D, Dw, G;      // disparities; lanes per pixel group (8, 16 or 32); groups per warp
+    int rbw;           // right-band width: columns x0-(D-1)-r .. x0+kTX-1+r
+    int lbw;           // left-band width: columns x0-r .. x0+kTX-1+r
+};
+
+// Shared-memory layout (floats) of one tile.
+template <int KIND, int R>
+struct Band {
+    static constexpr int kRows = kTY + 2 * R;
+    __host__ __device__ static int rband(const Geom& g) { return KIND == TDV_COST_BT ? 3 * kTX * kTY : kRows * g.lbw; }
+    // NCC window sums: LS per tile pixel, RS per (row, column x - d)
+    __host__ __device__ static int ls(const Geom& g) { return rband(g) + kRows * g.rbw; }
+    __host__ __device__ static int rs(const Geom& g) { return ls(g) + kTX * kTY; }
+    __host__ __device__ static int floats(const Geom& g) {
+        if (KIND == TDV_COST_BT) return 3 * kTX * kTY + 3 * kTY * (kTX + g.D - 1);
+        if (KIND == TDV_COST_SSD) return kRows * g.lbw + kRows * g.rbw;
+        return kRows * g.lbw + kRows * g.rbw + kTX * kTY + kTY * (kTX + g.D - 1);
+    }
+};
+
+// BT terms of one sample: I, min and max of {I, (I + I[-1]) / 2, (I + I[+1]) / 2}.
+__device__ __forceinline__ void bt_terms(const ImgArg& im, int x, int y, float& I, float& mi, float& ma) {
+    I = fetch(im, x, y);
+    const float a = __fmul_rn(0.5f, __fadd_rn(I, fetch(im, x - 1, y)));
+    const float b = __fmul_rn(0.5f, __fadd_rn(I, fetch(im, x + 1, y)));
+    mi = fminf(a, fminf(b, I));
+    ma = fmaxf(a, fmaxf(b, I));
+}
+
+template <int KIND, int R>
+__device__ void stage(const ImgArg& L, const ImgArg& Rim, const Geom& g, int x0, int y0, float* sm) {
+    using B = Band<KIND, R>;
+    const int tid = threadIdx.x;
+    if (KIND == TDV_COST_BT) {
+        float* lt = sm;                  // [3][kTY][kTX]
+        float* rt = sm + B::rband(g);    // [3][kTY][kTX + D - 1]
+        for (int i = tid; i < kTX * kTY; i += kThreads) {
+            const int row = i / kTX, col = i - row * kTX;
+            float I, mi, ma;
+            bt_terms(L, x0 + col, y0 + row, I, mi, ma);
+            lt[i] = I;
+            lt[kTX * kTY + i] = mi;
+            lt[2 * kTX * kTY + i] = ma;
+        }
+        const int rw = kTX + g.D - 1, n = rw * kTY;
+        for (int i = tid; i < n; i += kThreads) {
+            const int row = i / rw, col = i - row * rw;
+            float I, mi, ma;
+            bt_terms(Rim, x0 - (g.D - 1) + col, y0 + row, I, mi, ma);
+            rt[i] = I;
+            rt[n + i] = mi;
+            rt[2 * n + i] = ma;
+        }
+        return;
+    }
+    float* lb = sm;                       // [kRows][lbw], column x0 - R at index 0
+    float* rb = sm + B::rband(g);         // [kRows][rbw], column x0 - (D-1) - R at index 0
+    for (int i = tid; i < B::kRows * g.lbw; i += kThreads) {
+        const int row = i / g.lbw, col = i - row * g.lbw;
+        lb[i] = fetch(L, x0 - R + col, y0 - R + row);
+    }
+    for (int i = tid; i < B::kRows * g.rbw; i += kThreads) {
+        const int row = i / g.rbw, col = i - row * g.rbw;
+        rb[i] = fetch(Rim, x0 - (g.D - 1) - R + col, y0 - R + row);
+    }
+    if (KIND != TDV_COST_NCC) return;
+    __syncthreads();
+    // window sums of squares in the reference's tap order (rows, then columns)
+    float* ls = sm + B::ls(g);
+    float* rs = sm + B::rs(g);
+    for (int i = tid; i < kTX * kTY; i += kThreads) {
+        const int row = i / kTX, col = i - row * kTX;
+        float s = 0.0f;
+        for (int a = 0; a <= 2 * R; a++)
+            for (int b = 0; b <= 2 * R; b++) {
+                const float v = lb[(row + a) * g.lbw + col + b];
+                s = __fadd_rn(s, __fmul_rn(v, v));
+            }
+        ls[i] = s;
+    }
+    const int rw = kTX + g.D - 1;
+    for (int i = tid; i < rw * kTY; i += kThreads) {
+        const int row = i / rw, col = i - row * rw;
+        float s = 0.0f;
+        for (int a = 0; a <= 2 * R; a++)
+            for (int b = 0; b <= 2 * R; b++) {
+                const float v = rb[(row + a) * g.rbw + col + b];
+                s = __fadd_rn(s, __fmul_rn(v, v));
+            }
+        rs[i] = s;
+    }
+}
+
+template <int KIND, int R, int P>
+__global__ void __launch_bounds__(kThreads) cost_band_kernel(ImgArg L, ImgArg Rim, VolArg out, Geom g,
+                                                             int tiles_x) {
+    extern __shared__ float sm[];
+    using B = Band<KIND, R>;
+    const int x0 = (blockIdx.x % tiles_x) * kTX, y0 = (blockIdx.x / tiles_x) * kTY;
+    stage<KIND, R>(L, Rim, g, x0, y0, sm);
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int D = g.D, W = out.W, H = out.H;
+    const int sub = lane / g.Dw, dl = lane - sub * g.Dw;
+    const int span = P * g.G;                   // pixels of one work item
+    const int groups = kTX / span;
+    const int chunks = (D + g.Dw - 1) / g.Dw;
+    const int items = kTY * groups * chunks;
+    float* const outp = (float*)out.ptr;
+
+    for (int it = warp; it < items; it += kWarps) {
+        const int chunk = it % chunks;
+        const int rest = it / chunks;
+        const int grp = rest % groups, row = rest / groups;
+        const int y = y0 + row;
+        const int xs = x0 + grp * span + sub * P;   // first pixel of this thread
+        const int d = chunk * g.Dw + dl;
+        const bool dok = d < D;
+        const int de = dok ? d : D - 1;             // lanes past D read in-band columns, store nothing
+        float v[P];
+        if (KIND == TDV_COST_BT) {
+            const float* lt = sm;
+            const float* rt = sm + B::rband(g);
+            const int n = (kTX + D - 1) * kTY;
+#pragma unroll
+            for (int p = 0; p < P; p++) {
+                const int li = row * kTX + (xs + p - x0);
+                const float lI = lt[li], lImi = lt[kTX * kTY + li], lIma = lt[2 * kTX * kTY + li];
+                const int ri = row * (kTX + D - 1) + (xs + p - de) - (x0 - (D - 1));
+                const float rI = rt[ri], rImi = rt[n + ri], rIma = rt[2 * n + ri];
+                const float a = fmaxf(0.0f, fmaxf(__fsub_rn(lI, rIma), __fsub_rn(rImi, lI)));
+                const float b = fmaxf(0.0f, fmaxf(__fsub_rn(rI, lIma), __fsub_rn(lImi, rI)));
+                v[p] = __fadd_rn(0.0f, fminf(a, b));
+            }
+        } else {
+            constexpr int NJ = P + 2 * R;
+            float acc[P];
+#pragma unroll
+            for (int p = 0; p < P; p++) acc[p] = 0.0f;
+            const float* lb = sm + (size_t)row * g.lbw + (xs - x0);
+            const float* rb = sm + B::rband(g) + (size_t)row * g.rbw + (xs - de) - (x0 - (D - 1));
+#pragma unroll 1
+            for (int a = 0; a <= 2 * R; a++) {
+                float t[NJ];
+#pragma unroll
+                for (int j = 0; j < NJ; j++) {
+                    const float lv = lb[a * g.lbw + j], rv = rb[a * g.rbw + j];
+                    if (KIND == TDV_COST_SSD) {
+                        const float df = __fsub_rn(lv, rv);
+                        t[j] = __fmul_rn(df, df);
+                    } else {
+                        t[j] = __fmul_rn(lv, rv);
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b <= 2 * R; b++)
+#pragma unroll
+                    for (int p = 0; p < P; p++) acc[p] = __fadd_rn(acc[p], t[p + b]);
+            }
+            if (KIND == TDV_COST_SSD) {
+#pragma unroll
+                for (int p = 0; p < P; p++) v[p] = acc[p];
+            } else {
+                const float* ls = sm + B::ls(g) + row * kTX + (xs - x0);
+                const float* rs = sm + B::rs(g) + row * (kTX + D - 1) + (xs - de) - (x0 - (D - 1));
+#pragma unroll
+                for (int p = 0; p < P; p++)
+                    v[p] = __fsub_rn(1.0f, __fdiv_rn(acc[p], __fsqrt_rn(__fmul_rn(ls[p], rs[p]))));
+            }
+        }
+        if (!dok || y >= H) continue;
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            const int x = xs + p;
+            if (x < W) outp[x * out.sx + y * out.sy + d] = (x - d < 0) ? CUDART_INF_F : v[p];
+        }
+    }
+}
+
+template <int KIND, int R, int P>
+cudaError_t launch_one(const ImgArg& L, const ImgArg& Rim, const VolArg& out, const Geom& g, cudaStream_t st) {
+    const int bytes = Band<KIND, R>::floats(g) * 4;
+    auto k = cost_band_kernel<KIND, R, P>;
+    // opt in once to the largest band this launcher accepts
+    static const cudaError_t opt_in =
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxBandBytes);
+    if (opt_in != cudaSuccess) return opt_in;
+    const int tiles_x = (out.W + kTX - 1) / kTX, tiles_y = (out.H + kTY - 1) / kTY;
+    k<<<tiles_x * tiles_y, kThreads, bytes, st>>>(L, Rim, out, g, tiles_x);
+    return cudaGetLastError();
+}
+
+template <int KIND>
+cudaError_t dispatch_r(int r, const ImgArg& L, const ImgArg& Rim, const VolArg& out, const Geom& g,
+                       cudaStream_t st) {
+    switch (r) {
+        case 1: return launch_one<KIND, 1, 16>(L, Rim, out, g, st);
+        case 2: return launch_one<KIND, 2, 16>(L, Rim, out, g, st);
+        case 3: return launch_one<KIND, 3, 16>(L, Rim, out, g, st);
+        default: return launch_one<KIND, 4, 16>(L, Rim, out, g, st);
+    }
+}
+
+long long band_floats(int kind, int r, int D) {
+    const long long lbw = kTX + 2 * r, rbw = kTX + D - 1 + 2 * r;
+    if (kind == TDV_COST_BT) return 3LL * kTX * kTY + 3LL * kTY * (kTX + D - 1);
+    long long f = (long long)(kTY + 2 * r) * (lbw + rbw);
+    if (kind == TDV_COST_NCC) f += (long long)kTX * kTY + (long long)kTY * (kTX + D - 1);
+    return f;
+}
+
+}  // namespace
+
+bool cost_banded_supported(int kind, int radius, int D) {
+    if (kind != TDV_COST_BT && (radius < 1 || radius > 4)) return false;
+    return band_floats(kind, kind == TDV_COST_BT ? 0 : radius, D) * 4 <= kMaxBandBytes;
+}
+
+cudaError_t launch_cost_banded(const ImgArg& L, const ImgArg& R, int kind, int radius, const VolArg& out,
+                               cudaStream_t st) {
+    Geom g;
+    g.D = out.D;
+    g.Dw = out.D >= 32 ? 32 : out.D > 8 ? 16 : 8;
+    g.G = 32 / g.Dw;
+    const int r = kind == TDV_COST_BT ? 0 : radius;
+    g.lbw = kTX + 2 * r;
+    g.rbw = kTX + out.D - 1 + 2 * r;
+    if (kind == TDV_COST_BT) return launch_one<TDV_COST_BT, 0, 8>(L, R, out, g, st);
+    if (kind == TDV_COST_SSD) return dispatch_r<TDV_COST_SSD>(radius, L, R, out, g, st);
+    return dispatch_r<TDV_COST_NCC>(radius, L, R, out, g, st);
+}
+
+}  // namespace tdv

@@ -394,6 +394,13 @@ int grid_for(size_t n, int block) {
 
 cudaError_t launch_cost(const ImgArg& L, const ImgArg& R, int kind, int radius, const VolArg& out,
                         cudaStream_t st, Timer* tm) {
+    if (cost_banded_supported(kind, radius, out.D)) {
+        const cudaError_t e = launch_cost_banded(L, R, kind, radius, out, st);
+        if (tm) tm->mark("cost");
+        return e;
+    }
+    // windows wider than 9x9, or bands past the shared-memory budget: one
+    // thread per cell in memory order
     const size_t n = (size_t)out.W * out.H * out.D;
     const int xmajor = out.sx > out.sy ? 1 : 0;
     cost_kernel<<<grid_for(n, 256), 256, 0, st>>>(L, R, kind, radius, out, xmajor);

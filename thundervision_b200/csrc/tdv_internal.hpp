@@ -161,6 +161,10 @@ ImgArg make_img(const tdv_image& im);
 
 cudaError_t launch_cost(const ImgArg& L, const ImgArg& R, int kind, int radius, const VolArg& out,
                         cudaStream_t st, Timer* tm);
+// banded cost kernels (kernels_cost.cu): BT, and SSD / NCC with radius 1..4
+bool cost_banded_supported(int kind, int radius, int D);
+cudaError_t launch_cost_banded(const ImgArg& L, const ImgArg& R, int kind, int radius, const VolArg& out,
+                               cudaStream_t st);
 
 struct SgmArgs {
     VolArg C, S;
