@@ -126,11 +126,16 @@ tdv_status ensure_schedule(tdv_ctx* ctx, int W, int H, int table, int paths, cud
     tdv::PassSchedule fresh;
     if (!tdv::build_schedule(W, H, table, paths, fresh))
         return fail(ctx, TDV_ERR_BAD_WORK, "path table for %dx%d has a walk outside the image", W, H);
-    TDV_TRY(ensure(ctx, ctx->sched_buf, fresh.walks.size() * sizeof(tdv::Walk)));
+    const size_t wbytes = (fresh.walks.size() * sizeof(tdv::Walk) + 255) & ~(size_t)255;
+    TDV_TRY(ensure(ctx, ctx->sched_buf, wbytes + (fresh.deferred.size() + 1) * sizeof(int32_t)));
     sc = std::move(fresh);
     sc.d_walks = (tdv::Walk*)ctx->sched_buf.ptr;
+    sc.d_deferred = (int32_t*)((char*)ctx->sched_buf.ptr + wbytes);
     TDV_CUDA(cudaMemcpyAsync(sc.d_walks, sc.walks.data(), sc.walks.size() * sizeof(tdv::Walk),
                              cudaMemcpyHostToDevice, st));
+    if (!sc.deferred.empty())
+        TDV_CUDA(cudaMemcpyAsync(sc.d_deferred, sc.deferred.data(), sc.deferred.size() * sizeof(int32_t),
+                                 cudaMemcpyHostToDevice, st));
     // the host vector is the copy source: keep it until the copy has run
     TDV_CUDA(cudaStreamSynchronize(st));
     return TDV_OK;
@@ -150,7 +155,10 @@ tdv_status run_sgm(tdv_ctx* ctx, const tdv_volume* cost, const tdv_image* guide,
         Sv = tdv::make_vol(tmp);
     }
     TDV_TRY(ensure_schedule(ctx, W, H, p->table, p->paths, st));
+    if (ctx->sched.defer_rows > 0)
+        TDV_TRY(ensure(ctx, ctx->defer, (size_t)ctx->sched.defer_rows * D * sizeof(float)));
     tdv::SgmArgs a;
+    a.defer = ctx->sched.defer_rows > 0 ? (float*)ctx->defer.ptr : nullptr;
     a.C = C;
     a.S = Sv;
     a.has_guide = guide ? 1 : 0;
@@ -343,7 +351,7 @@ void tdv_ctx_destroy(tdv_ctx* ctx) {
     if (!ctx) return;
     const bool any = ctx->agg.ptr || ctx->cost.ptr || ctx->planes.ptr || ctx->codes.ptr ||
                      ctx->misc.ptr || ctx->sched_buf.ptr || ctx->err.ptr || ctx->soft.ptr ||
-                     ctx->agg2.ptr || ctx->side;
+                     ctx->agg2.ptr || ctx->defer.ptr || ctx->side;
     if (any) {
         DeviceScope ds(ctx->device);
         cudaDeviceSynchronize();
@@ -359,6 +367,7 @@ void tdv_ctx_destroy(tdv_ctx* ctx) {
         release_buf(ctx, ctx->sched_buf);
         release_buf(ctx, ctx->err);
         release_buf(ctx, ctx->soft);
+        release_buf(ctx, ctx->defer);
     }
     if (!ctx->timer.ev.empty()) {
         DeviceScope ds(ctx->device);
@@ -372,7 +381,7 @@ tdv_status tdv_ctx_set_allocator(tdv_ctx* ctx, tdv_alloc_fn alloc, tdv_free_fn r
     if ((alloc == nullptr) != (release == nullptr))
         return fail(ctx, TDV_ERR_INVALID_ARG, "allocator and release must be set together");
     if (ctx->agg.ptr || ctx->cost.ptr || ctx->planes.ptr || ctx->codes.ptr || ctx->misc.ptr ||
-        ctx->sched_buf.ptr)
+        ctx->sched_buf.ptr || ctx->defer.ptr)
         return fail(ctx, TDV_ERR_INVALID_ARG, "allocator must be set before any scratch exists");
     ctx->alloc = alloc;
     ctx->release = release;

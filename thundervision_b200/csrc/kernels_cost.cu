@@ -50,8 +50,10 @@ __device__ __forceinline__ float fetch(const ImgArg& im, int x, int y) {
 struct Geom {
     int D, Dw, G;      // disparities; lanes per pixel group (8, 16 or 32); groups per warp
     int rbw;           // right-band width: columns x0-(D-1)-r .. x0+kTX-1+r
-    int lbw;           // left-band width: columns x0-r .. x0+kTX-1+r
+    int lbw;           // left-band width: columns x0-r .. x0+kTX-1+r, padded to 4 floats
 };
+
+__host__ __device__ constexpr int left_band_width(int r) { return kTX + ((2 * r + 3) & ~3); }
 
 // Shared-memory layout (floats) of one tile.
 template <int KIND, int R>
@@ -144,7 +146,7 @@ __device__ void stage(const ImgArg& L, const ImgArg& Rim, const Geom& g, int x0,
 template <int KIND, int R, int P>
 __global__ void __launch_bounds__(kThreads) cost_band_kernel(ImgArg L, ImgArg Rim, VolArg out, Geom g,
                                                              int tiles_x) {
-    extern __shared__ float sm[];
+    extern __shared__ __align__(16) float sm[];
     using B = Band<KIND, R>;
     const int x0 = (blockIdx.x % tiles_x) * kTX, y0 = (blockIdx.x / tiles_x) * kTY;
     stage<KIND, R>(L, Rim, g, x0, y0, sm);
@@ -159,6 +161,44 @@ __global__ void __launch_bounds__(kThreads) cost_band_kernel(ImgArg L, ImgArg Ri
     const int items = kTY * groups * chunks;
     float* const outp = (float*)out.ptr;
 
+    if (KIND == TDV_COST_BT) {
+        // BT: a work item is P pixels of one row over every disparity chunk,
+        // so each pixel's left terms are read from shared memory once
+        const float* lt = sm;
+        const float* rt = sm + B::rband(g);
+        const int n = (kTX + D - 1) * kTY;
+        for (int it = warp; it < kTY * groups; it += kWarps) {
+            const int grp = it % groups, row = it / groups;
+            const int y = y0 + row;
+            const int xs = x0 + grp * span + sub * P;
+            float lI[P], lImi[P], lIma[P];
+#pragma unroll
+            for (int p = 0; p < P; p++) {
+                const int li = row * kTX + (xs + p - x0);
+                lI[p] = lt[li];
+                lImi[p] = lt[kTX * kTY + li];
+                lIma[p] = lt[2 * kTX * kTY + li];
+            }
+            for (int chunk = 0; chunk < chunks; chunk++) {
+                const int d = chunk * g.Dw + dl;
+                const bool dok = d < D;
+                const int de = dok ? d : D - 1;
+                const int r0 = row * (kTX + D - 1) + (xs - de) - (x0 - (D - 1));
+                float* const op = outp + y * out.sy + d;
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    const float rI = rt[r0 + p], rImi = rt[n + r0 + p], rIma = rt[2 * n + r0 + p];
+                    const float a = fmaxf(0.0f, fmaxf(__fsub_rn(lI[p], rIma), __fsub_rn(rImi, lI[p])));
+                    const float b = fmaxf(0.0f, fmaxf(__fsub_rn(rI, lIma[p]), __fsub_rn(lImi[p], rI)));
+                    const float v = __fadd_rn(0.0f, fminf(a, b));
+                    const int x = xs + p;
+                    if (dok && y < H && x < W) op[x * out.sx] = (x - d < 0) ? CUDART_INF_F : v;
+                }
+            }
+        }
+        return;
+    }
+
     for (int it = warp; it < items; it += kWarps) {
         const int chunk = it % chunks;
         const int rest = it / chunks;
@@ -169,33 +209,33 @@ __global__ void __launch_bounds__(kThreads) cost_band_kernel(ImgArg L, ImgArg Ri
         const bool dok = d < D;
         const int de = dok ? d : D - 1;             // lanes past D read in-band columns, store nothing
         float v[P];
-        if (KIND == TDV_COST_BT) {
-            const float* lt = sm;
-            const float* rt = sm + B::rband(g);
-            const int n = (kTX + D - 1) * kTY;
-#pragma unroll
-            for (int p = 0; p < P; p++) {
-                const int li = row * kTX + (xs + p - x0);
-                const float lI = lt[li], lImi = lt[kTX * kTY + li], lIma = lt[2 * kTX * kTY + li];
-                const int ri = row * (kTX + D - 1) + (xs + p - de) - (x0 - (D - 1));
-                const float rI = rt[ri], rImi = rt[n + ri], rIma = rt[2 * n + ri];
-                const float a = fmaxf(0.0f, fmaxf(__fsub_rn(lI, rIma), __fsub_rn(rImi, lI)));
-                const float b = fmaxf(0.0f, fmaxf(__fsub_rn(rI, lIma), __fsub_rn(lImi, rI)));
-                v[p] = __fadd_rn(0.0f, fminf(a, b));
-            }
-        } else {
+        {
             constexpr int NJ = P + 2 * R;
             float acc[P];
 #pragma unroll
             for (int p = 0; p < P; p++) acc[p] = 0.0f;
             const float* lb = sm + (size_t)row * g.lbw + (xs - x0);
             const float* rb = sm + B::rband(g) + (size_t)row * g.rbw + (xs - de) - (x0 - (D - 1));
+            constexpr int NJ4 = (NJ + 3) & ~3;
 #pragma unroll 1
             for (int a = 0; a <= 2 * R; a++) {
+                // the left window is the same for every lane: 128-bit
+                // broadcast reads (the row start is a multiple of 16 floats
+                // into a row padded to 4)
+                float lw[NJ4];
+                const float4* l4 = reinterpret_cast<const float4*>(lb + a * g.lbw);
+#pragma unroll
+                for (int q = 0; q < NJ4 / 4; q++) {
+                    const float4 f = l4[q];
+                    lw[4 * q] = f.x;
+                    lw[4 * q + 1] = f.y;
+                    lw[4 * q + 2] = f.z;
+                    lw[4 * q + 3] = f.w;
+                }
                 float t[NJ];
 #pragma unroll
                 for (int j = 0; j < NJ; j++) {
-                    const float lv = lb[a * g.lbw + j], rv = rb[a * g.rbw + j];
+                    const float lv = lw[j], rv = rb[a * g.rbw + j];
                     if (KIND == TDV_COST_SSD) {
                         const float df = __fsub_rn(lv, rv);
                         t[j] = __fmul_rn(df, df);
@@ -253,7 +293,7 @@ cudaError_t dispatch_r(int r, const ImgArg& L, const ImgArg& Rim, const VolArg& 
 }
 
 long long band_floats(int kind, int r, int D) {
-    const long long lbw = kTX + 2 * r, rbw = kTX + D - 1 + 2 * r;
+    const long long lbw = left_band_width(r), rbw = kTX + D - 1 + 2 * r;
     if (kind == TDV_COST_BT) return 3LL * kTX * kTY + 3LL * kTY * (kTX + D - 1);
     long long f = (long long)(kTY + 2 * r) * (lbw + rbw);
     if (kind == TDV_COST_NCC) f += (long long)kTX * kTY + (long long)kTY * (kTX + D - 1);
@@ -274,7 +314,7 @@ cudaError_t launch_cost_banded(const ImgArg& L, const ImgArg& R, int kind, int r
     g.Dw = out.D >= 32 ? 32 : out.D > 8 ? 16 : 8;
     g.G = 32 / g.Dw;
     const int r = kind == TDV_COST_BT ? 0 : radius;
-    g.lbw = kTX + 2 * r;
+    g.lbw = left_band_width(r);
     g.rbw = kTX + out.D - 1 + 2 * r;
     if (kind == TDV_COST_BT) return launch_one<TDV_COST_BT, 0, 8>(L, R, out, g, st);
     if (kind == TDV_COST_SSD) return dispatch_r<TDV_COST_SSD>(radius, L, R, out, g, st);

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "tdv_internal.hpp"
@@ -100,7 +101,11 @@ __device__ __forceinline__ float fdeord(uint32_t o) {
 
 __device__ __forceinline__ float smin(float a, float b) { return (b < a) ? b : a; }
 
-// One warp per walk; lane l holds disparities [l*NPL, l*NPL+NPL).
+// One warp per walk; lane l holds disparities l, l+32, ..., l+32*(NPL-1), so
+// every load and store of a step moves whole 128-byte lines.  Neighbours
+// d-1 and d+1 come from one rotation shuffle each: lane l-1 (or lane 31 of
+// the previous group for lane 0) and lane l+1 (lane 0 of the next group for
+// lane 31).
 template <int NPL>
 __global__ void __launch_bounds__(128) sgm_pass_kernel(SgmArgs a, const Walk* __restrict__ walks,
                                                        int nwalks, int dx, int dy, int first) {
@@ -109,34 +114,34 @@ __global__ void __launch_bounds__(128) sgm_pass_kernel(SgmArgs a, const Walk* __
     if (w >= nwalks) return;
     const Walk wk = walks[w];
     const int D = a.C.D;
-    const int d0 = lane * NPL;
     const bool refcpu = a.sem == TDV_SEM_REF_CPU;
     const bool refgpu = a.sem == TDV_SEM_REF_GPU;
     const int mlim = refcpu ? D - 1 : D;  // REF_CPU scans {sentinel, L(0..D-2)}
     const float* C = (const float*)a.C.ptr;
     float* S = (float*)a.S.ptr;
+    const int src_up = (lane + 31) & 31, src_dn = (lane + 1) & 31;
 
     int x = wk.sx, y = wk.sy;
-    float L[NPL], c[NPL];
+    float L[NPL];
     {
         const float* cp = C + x * a.C.sx + y * a.C.sy;
         float* sp = S + x * a.S.sx + y * a.S.sy;
         uint32_t mo = 0xFFFFFFFFu;
 #pragma unroll
         for (int j = 0; j < NPL; j++) {
-            const int d = d0 + j;
-            c[j] = d < D ? cp[d] : CUDART_INF_F;
-            if (d < mlim) mo = min(mo, ford(c[j]));
+            const int d = lane + 32 * j;
+            const float c = d < D ? cp[d] : CUDART_INF_F;
+            if (d < mlim) mo = min(mo, ford(c));
             if (d < D) {
                 if (refcpu || first) {
-                    sp[d] = c[j];
+                    sp[d] = c;
+                } else if (wk.mult == 1) {
+                    sp[d] = __fadd_rn(sp[d], c);
                 } else {
-                    float acc = sp[d];
-                    for (int k = 0; k < wk.mult; k++) acc = __fadd_rn(acc, c[j]);
-                    sp[d] = acc;
+                    a.defer[(size_t)wk.defer * D + d] = c;  // added mult times by sgm_deferred_kernel
                 }
             }
-            L[j] = (refgpu && d < D) ? __fadd_rn(c[j], a.p1) : c[j];
+            L[j] = (refgpu && d < D) ? __fadd_rn(c, a.p1) : c;
         }
         // minimum over d with fminf semantics starting from +INF: NaN ignored,
         // no candidate -> +INF
@@ -144,58 +149,111 @@ __global__ void __launch_bounds__(128) sgm_pass_kernel(SgmArgs a, const Walk* __
         float m = mo == 0xFFFFFFFFu ? CUDART_INF_F : fdeord(mo);
         float lastI = a.has_guide ? img_at(a.guide, x, y) : 0.0f;
 
-        for (int t = 1; t < wk.len; t++) {
-            x += dx;
-            y += dy;
-            const float* cq = C + x * a.C.sx + y * a.C.sy;
-            float* sq = S + x * a.S.sx + y * a.S.sy;
+        // Steps 1..len-1.  The loads of step t (C, S unless this is the
+        // first pass, the guide intensity) are issued K steps ahead into a
+        // register ring, so a walk keeps K steps of loads in flight instead
+        // of waiting on each step's own; cells are distinct along a walk and
+        // across the walks of a pass, so a prefetched S is never stale.
+        constexpr int K = NPL <= 2 ? 8 : 4;
+        float cr[K][NPL], sr[K][NPL], ir[K];
+        const int len = wk.len;
+        auto issue = [&](int t, float (&cs)[NPL], float (&ss)[NPL], float& is) {
+            const int xx = wk.sx + t * dx, yy = wk.sy + t * dy;
+            const float* cq = C + xx * a.C.sx + yy * a.C.sy;
+            const float* sq = S + xx * a.S.sx + yy * a.S.sy;
 #pragma unroll
             for (int j = 0; j < NPL; j++) {
-                const int d = d0 + j;
-                c[j] = d < D ? cq[d] : CUDART_INF_F;
+                const int d = lane + 32 * j;
+                cs[j] = d < D ? cq[d] : CUDART_INF_F;
+                ss[j] = (!first && d < D) ? sq[d] : 0.0f;
             }
-            float p2a = a.p2;
-            if (a.p2_adjust) {
-                const float I = img_at(a.guide, x, y);
-                p2a = __fdiv_rn(a.p2, fabsf(__fsub_rn(I, lastI)));
-                lastI = I;
-            }
-            const float mp2 = __fadd_rn(m, p2a);
-            float up = __shfl_up_sync(0xFFFFFFFFu, L[NPL - 1], 1);
-            float dn = __shfl_down_sync(0xFFFFFFFFu, L[0], 1);
-            if (lane == 0) up = CUDART_INF_F;
-            if (lane == 31) dn = CUDART_INF_F;
-            float Ln[NPL];
-            uint32_t mn_o = 0xFFFFFFFFu;
+            is = a.p2_adjust ? img_at(a.guide, xx, yy) : 0.0f;
+        };
 #pragma unroll
-            for (int j = 0; j < NPL; j++) {
-                const int d = d0 + j;
-                const float lm = j > 0 ? L[j - 1] : up;
-                const float lp = j < NPL - 1 ? L[j + 1] : dn;
-                const float b = __fadd_rn(lm, a.p1);
-                const float e = __fadd_rn(lp, a.p1);
-                float mn;
-                if (refcpu) mn = smin(L[j], smin(b, smin(e, mp2)));
-                else mn = fminf(L[j], fminf(b, fminf(e, mp2)));
-                float v = __fsub_rn(__fadd_rn(c[j], mn), m);
-                if (d >= D) v = CUDART_INF_F;
-                Ln[j] = v;
-                if (d < mlim) mn_o = min(mn_o, ford(v));
-                if (d < D) {
-                    if (first) {
-                        sq[d] = v;
-                    } else {
-                        float acc = sq[d];
-                        for (int k = 0; k < wk.mult; k++) acc = __fadd_rn(acc, v);
-                        sq[d] = acc;
+        for (int k = 0; k < K; k++)
+            if (1 + k < len) issue(1 + k, cr[k], sr[k], ir[k]);
+
+        for (int t0 = 1; t0 < len; t0 += K) {
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const int t = t0 + k;
+                if (t >= len) break;
+                x = wk.sx + t * dx;
+                y = wk.sy + t * dy;
+                float* sq = S + x * a.S.sx + y * a.S.sy;
+                float p2a = a.p2;
+                if (a.p2_adjust) {
+                    const float I = ir[k];
+                    p2a = __fdiv_rn(a.p2, fabsf(__fsub_rn(I, lastI)));
+                    lastI = I;
+                }
+                const float mp2 = __fadd_rn(m, p2a);
+                float ru[NPL], rd[NPL];
+#pragma unroll
+                for (int j = 0; j < NPL; j++) {
+                    ru[j] = __shfl_sync(0xFFFFFFFFu, L[j], src_up);
+                    rd[j] = __shfl_sync(0xFFFFFFFFu, L[j], src_dn);
+                }
+                float Ln[NPL];
+                uint32_t mn_o = 0xFFFFFFFFu;
+#pragma unroll
+                for (int j = 0; j < NPL; j++) {
+                    const int d = lane + 32 * j;
+                    const float lm = lane > 0 ? ru[j] : (j > 0 ? ru[j - 1] : CUDART_INF_F);
+                    const float lp = lane < 31 ? rd[j] : (j < NPL - 1 ? rd[j + 1] : CUDART_INF_F);
+                    const float b = __fadd_rn(lm, a.p1);
+                    const float e = __fadd_rn(lp, a.p1);
+                    float mn;
+                    if (refcpu) mn = smin(L[j], smin(b, smin(e, mp2)));
+                    else mn = fminf(L[j], fminf(b, fminf(e, mp2)));
+                    float v = __fsub_rn(__fadd_rn(cr[k][j], mn), m);
+                    if (d >= D) v = CUDART_INF_F;
+                    Ln[j] = v;
+                    if (d < mlim) mn_o = min(mn_o, ford(v));
+                    if (d < D) {
+                        if (first) {
+                            sq[d] = v;
+                        } else if (wk.mult == 1) {
+                            sq[d] = __fadd_rn(sr[k][j], v);
+                        } else {
+                            a.defer[((size_t)wk.defer + t) * D + d] = v;
+                        }
                     }
                 }
-            }
 #pragma unroll
-            for (int j = 0; j < NPL; j++) L[j] = Ln[j];
-            mn_o = __reduce_min_sync(0xFFFFFFFFu, mn_o);
-            m = mn_o == 0xFFFFFFFFu ? CUDART_INF_F : fdeord(mn_o);
+                for (int j = 0; j < NPL; j++) L[j] = Ln[j];
+                mn_o = __reduce_min_sync(0xFFFFFFFFu, mn_o);
+                m = mn_o == 0xFFFFFFFFu ? CUDART_INF_F : fdeord(mn_o);
+                if (t + K < len) issue(t + K, cr[k], sr[k], ir[k]);
+            }
         }
+    }
+}
+
+// The walks a pass repeats (the reference's table issues some walks up to
+// W - H + 1 times in a row): each repeat adds the same path cost to the cell
+// once more, each add rounded.  The pass kernel leaves those costs in the
+// deferred buffer; here one thread per cell adds its cost mult times, so the
+// repeats run in parallel over the walk's cells instead of in series along
+// it.  The walks of a pass touch disjoint cells, so every cell still sees
+// its updates in the reference's order.  The start cell of REF_CPU walks is
+// assigned, not accumulated, by the pass kernel itself.
+__global__ void sgm_deferred_kernel(SgmArgs a, const Walk* __restrict__ walks, const int32_t* __restrict__ idx,
+                                    int dx, int dy, int skip_start) {
+    const Walk wk = walks[idx[blockIdx.y]];
+    const int D = a.S.D;
+    const long long n = (long long)wk.len * D;
+    float* S = (float*)a.S.ptr;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int t = (int)(i / D), d = (int)(i - (long long)t * D);
+        if (t == 0 && skip_start) continue;
+        const int x = wk.sx + t * dx, y = wk.sy + t * dy;
+        float* sp = S + x * a.S.sx + y * a.S.sy + d;
+        const float v = a.defer[((size_t)wk.defer + t) * D + d];
+        float acc = *sp;
+        for (int q = 0; q < wk.mult; q++) acc = __fadd_rn(acc, v);
+        *sp = acc;
     }
 }
 
@@ -211,6 +269,15 @@ cudaError_t run_passes(const SgmArgs& a, const PassSchedule& sch, cudaStream_t s
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         if (tm) tm->mark("sgm_pass");
+        if (p > 0 && ps.dcount > 0) {
+            const long long cells = (long long)ps.dmaxlen * a.S.D;
+            const dim3 grid((unsigned)std::min<long long>((cells + 255) / 256, 4096), (unsigned)ps.dcount);
+            sgm_deferred_kernel<<<grid, 256, 0, st>>>(a, sch.d_walks, sch.d_deferred + ps.dfirst, ps.dx, ps.dy,
+                                                       a.sem == TDV_SEM_REF_CPU ? 1 : 0);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+            if (tm) tm->mark("sgm_repeats");
+        }
     }
     return cudaSuccess;
 }

@@ -104,7 +104,7 @@ bool build_schedule(int W, int H, int table, int paths, PassSchedule& out) {
         int j = j0;
         while (j < (int)pb.size() && !(pb[j].dx == dx && pb[j].dy == dy)) j++;
         if (j == (int)pb.size()) pb.push_back({dx, dy, {}});
-        pb[j].walks.push_back({sx, sy, len, 1});
+        pb[j].walks.push_back({sx, sy, len, 1, -1});
         x = sx;
         y = sy;
         for (int i = 0; i < len; i++, x += dx, y += dy) stamp[(size_t)y * W + x] = j;
@@ -115,12 +115,27 @@ bool build_schedule(int W, int H, int table, int paths, PassSchedule& out) {
         place(e.sx, e.sy, e.dx, e.dy, e.size);
         place(e.ex, e.ey, -e.dx, -e.dy, e.size);
     }
+    out.deferred.clear();
+    out.defer_rows = 0;
     for (auto& p : pb) {
         Pass ps;
         ps.dx = p.dx;
         ps.dy = p.dy;
         ps.first = out.walks.size();
         ps.count = p.walks.size();
+        ps.dfirst = out.deferred.size();
+        ps.dmaxlen = 0;
+        long long rows = 0;
+        for (size_t i = 0; i < p.walks.size(); i++) {
+            Walk& w = p.walks[i];
+            if (w.mult <= 1) continue;
+            w.defer = (int32_t)rows;
+            rows += w.len;
+            ps.dmaxlen = std::max(ps.dmaxlen, w.len);
+            out.deferred.push_back((int32_t)(ps.first + i));
+        }
+        ps.dcount = out.deferred.size() - ps.dfirst;
+        out.defer_rows = std::max(out.defer_rows, rows);
         out.walks.insert(out.walks.end(), p.walks.begin(), p.walks.end());
         out.passes.push_back(ps);
     }

@@ -19,9 +19,11 @@ constexpr int kMaxDispWide = 1024;
 
 // One walk of an aggregation pass: start cell, number of cells, and how many
 // identical walks the reference table issues back to back (REF tables repeat
-// some reverse diagonals).
+// some reverse diagonals).  A repeated walk (mult > 1) stores its per-cell
+// path costs in the deferred buffer, from row `defer` on (one row of D floats
+// per step), and a second kernel adds each of them mult times into S.
 struct Walk {
-    int32_t sx, sy, len, mult;
+    int32_t sx, sy, len, mult, defer;
 };
 
 // An ordered aggregation pass: all walks share one direction and touch
@@ -29,14 +31,19 @@ struct Walk {
 // reference's per-cell order of updates.
 struct Pass {
     int dx, dy;
-    size_t first, count;  // range in the device walk array
+    size_t first, count;    // range in the device walk array
+    size_t dfirst, dcount;  // its repeated walks: range in the deferred index array
+    int dmaxlen;            // longest repeated walk of the pass
 };
 
 struct PassSchedule {
     int W = 0, H = 0, table = -1, paths = 0;
     std::vector<Pass> passes;
-    std::vector<Walk> walks;  // host copy
-    Walk* d_walks = nullptr;  // device copy (ctx scratch)
+    std::vector<Walk> walks;         // host copy
+    std::vector<int32_t> deferred;   // indices (into walks) of repeated walks, pass by pass
+    long long defer_rows = 0;        // deferred-buffer rows one pass needs at most
+    Walk* d_walks = nullptr;         // device copies (ctx scratch)
+    int32_t* d_deferred = nullptr;
 };
 
 // Optional per-kernel timing.  Every kernel of one ABI call is bracketed by
@@ -120,6 +127,7 @@ struct tdv_ctx {
     Buf misc;     // small per-call scratch
     Buf err;      // one device int: error status written by kernels
     Buf soft;     // soft-SGM: dS volume / inference-mode S and statistics
+    Buf defer;    // general SGM: path costs of repeated walks, one pass at a time
     std::vector<long long> ckpt_off_host;
 
     tdv::PassSchedule sched;
@@ -172,6 +180,7 @@ struct SgmArgs {
     int has_guide;
     float p1, p2;
     int p2_adjust, sem;
+    float* defer;  // path costs of the repeated walks of one pass (PassSchedule::defer_rows x D)
 };
 cudaError_t launch_sgm_passes(const SgmArgs& a, const PassSchedule& sch, cudaStream_t st, Timer* tm);
 cudaError_t launch_wta(const VolArg& V, uint16_t* disp, float* disp_norm, cudaStream_t st, Timer* tm);
