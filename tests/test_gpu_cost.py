@@ -62,3 +62,31 @@ def test_cost_large_d(ctx, orc, kind, radius):
     ref = orc.cost_pair(orc.u8_to_f32(L8), orc.u8_to_f32(R8), 256, KIND_ID[kind], radius)
     torch.cuda.synchronize()
     assert np.array_equal(C.cpu().numpy(), ref, equal_nan=True)
+
+
+@pytest.mark.parametrize("radius", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("D", [1, 3, 16, 17, 33, 64, 100])
+def test_fast_wta_bit_exact(ctx, orc, radius, D):
+    # the fused SSD + argmin (lowest d on ties, NaN and +INF never win, d = 0
+    # when no cost is finite) against the oracle's scan, both outputs
+    rng = np.random.default_rng(1000 + D * 10 + radius)
+    for i, ((h, w), _) in enumerate(SHAPES):
+        if i % 2 == 0:
+            L8 = rng.integers(0, 256, (h, w), dtype=np.uint8)
+            R8 = np.roll(L8, 2, axis=1) if w > 4 else rng.integers(0, 256, (h, w), dtype=np.uint8)
+            s = np.float32(1.0) / np.float32(255.0)
+            out = ctx.fast_wta(torch.from_numpy(L8).cuda(), torch.from_numpy(R8).cuda(), D, radius=radius,
+                               scale=float(s), norm=True)
+            Lf, Rf = orc.u8_to_f32(L8, s), orc.u8_to_f32(R8, s)
+        else:
+            Lf = rng.random((h, w), dtype=np.float32)
+            Rf = rng.random((h, w), dtype=np.float32)
+            Lf[:, : w // 3] = Lf[:, :1]  # flat runs: ties
+            Rf[:, : w // 3] = Lf[:, :1]
+            if i == 3:
+                Lf[h // 2, w // 2] = np.nan  # windows over it give NaN costs
+            out = ctx.fast_wta(padded(Lf), padded(Rf), D, radius=radius, norm=True)
+        d_ref, dn_ref = orc.fastwta(Lf, Rf, D, radius=radius)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out["disp"].cpu().numpy(), d_ref, err_msg=f"shape {i}")
+        np.testing.assert_array_equal(out["disp_norm"].cpu().numpy(), dn_ref, err_msg=f"shape {i}")

@@ -268,6 +268,127 @@ __global__ void __launch_bounds__(kThreads) cost_band_kernel(ImgArg L, ImgArg Ri
     }
 }
 
+// Order-preserving key of a candidate cost for the argmin: finite values map
+// increasing; NaN, +INF and cells outside the range map to the largest key,
+// so they never win against a finite cost (the reference's `v < best` with
+// best starting at +INF).
+__device__ __forceinline__ uint32_t cost_key(float v) {
+    const uint32_t u = __float_as_uint(v);
+    if (!(fabsf(v) < CUDART_INF_F)) return 0xFFFFFFFFu;
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// FastWTA (tdvision/fastwta.cu:32-53): the window SSD of the banded kernel
+// with the argmin over d fused in, no DSI.  A lane keeps the best (key, d)
+// of its own disparities over the chunks (strict <, so its lowest d wins a
+// tie), then the lanes of a pixel group merge by (key, d) -- the lowest d
+// among the smallest costs, d = 0 when no cost is finite, as the reference's
+// scan gives.
+template <int R, int P>
+__global__ void __launch_bounds__(kThreads) fastwta_band_kernel(ImgArg L, ImgArg Rim, int W, int H, Geom g,
+                                                                int tiles_x, uint16_t* disp, float* disp_norm) {
+    extern __shared__ __align__(16) float sm[];
+    using B = Band<TDV_COST_SSD, R>;
+    const int x0 = (blockIdx.x % tiles_x) * kTX, y0 = (blockIdx.x / tiles_x) * kTY;
+    stage<TDV_COST_SSD, R>(L, Rim, g, x0, y0, sm);
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int D = g.D;
+    const int sub = lane / g.Dw, dl = lane - sub * g.Dw;
+    const int span = P * g.G;
+    const int groups = kTX / span;
+    const int chunks = (D + g.Dw - 1) / g.Dw;
+    constexpr int NJ = P + 2 * R;
+    constexpr int NJ4 = (NJ + 3) & ~3;
+
+    for (int it = warp; it < kTY * groups; it += kWarps) {
+        const int grp = it % groups, row = it / groups;
+        const int y = y0 + row;
+        const int xs = x0 + grp * span + sub * P;
+        uint32_t bk[P];
+        int bd[P];
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            bk[p] = 0xFFFFFFFFu;
+            bd[p] = dl;
+        }
+        for (int chunk = 0; chunk < chunks; chunk++) {
+            const int d = chunk * g.Dw + dl;
+            const bool dok = d < D;
+            const int de = dok ? d : D - 1;
+            float acc[P];
+#pragma unroll
+            for (int p = 0; p < P; p++) acc[p] = 0.0f;
+            const float* lb = sm + (size_t)row * g.lbw + (xs - x0);
+            const float* rb = sm + B::rband(g) + (size_t)row * g.rbw + (xs - de) - (x0 - (D - 1));
+#pragma unroll 1
+            for (int a = 0; a <= 2 * R; a++) {
+                float lw[NJ4];
+                const float4* l4 = reinterpret_cast<const float4*>(lb + a * g.lbw);
+#pragma unroll
+                for (int q = 0; q < NJ4 / 4; q++) {
+                    const float4 f = l4[q];
+                    lw[4 * q] = f.x;
+                    lw[4 * q + 1] = f.y;
+                    lw[4 * q + 2] = f.z;
+                    lw[4 * q + 3] = f.w;
+                }
+                float t[NJ];
+#pragma unroll
+                for (int j = 0; j < NJ; j++) {
+                    const float df = __fsub_rn(lw[j], rb[a * g.rbw + j]);
+                    t[j] = __fmul_rn(df, df);
+                }
+#pragma unroll
+                for (int b = 0; b <= 2 * R; b++)
+#pragma unroll
+                    for (int p = 0; p < P; p++) acc[p] = __fadd_rn(acc[p], t[p + b]);
+            }
+#pragma unroll
+            for (int p = 0; p < P; p++) {
+                const uint32_t key = cost_key(acc[p]);
+                if (dok && xs + p - d >= 0 && key < bk[p]) {
+                    bk[p] = key;
+                    bd[p] = d;
+                }
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            uint32_t k = bk[p];
+            int dd = bd[p];
+            for (int off = g.Dw >> 1; off > 0; off >>= 1) {
+                const uint32_t ok = __shfl_xor_sync(0xFFFFFFFFu, k, off);
+                const int od = __shfl_xor_sync(0xFFFFFFFFu, dd, off);
+                if (ok < k || (ok == k && od < dd)) {
+                    k = ok;
+                    dd = od;
+                }
+            }
+            const int x = xs + p;
+            if (dl == 0 && x < W && y < H) {
+                const size_t o = (size_t)y * W + x;
+                if (disp) disp[o] = (uint16_t)dd;
+                if (disp_norm) disp_norm[o] = __fdiv_rn((float)dd, (float)D);
+            }
+        }
+    }
+}
+
+template <int R>
+cudaError_t launch_fastwta_r(const ImgArg& L, const ImgArg& Rim, const Geom& g, uint16_t* disp, float* disp_norm,
+                             cudaStream_t st) {
+    const int bytes = Band<TDV_COST_SSD, R>::floats(g) * 4;
+    auto k = fastwta_band_kernel<R, 16>;
+    static const cudaError_t opt_in =
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxBandBytes);
+    if (opt_in != cudaSuccess) return opt_in;
+    const int tiles_x = (L.W + kTX - 1) / kTX, tiles_y = (L.H + kTY - 1) / kTY;
+    k<<<tiles_x * tiles_y, kThreads, bytes, st>>>(L, Rim, L.W, L.H, g, tiles_x, disp, disp_norm);
+    return cudaGetLastError();
+}
+
 template <int KIND, int R, int P>
 cudaError_t launch_one(const ImgArg& L, const ImgArg& Rim, const VolArg& out, const Geom& g, cudaStream_t st) {
     const int bytes = Band<KIND, R>::floats(g) * 4;
@@ -305,6 +426,22 @@ long long band_floats(int kind, int r, int D) {
 bool cost_banded_supported(int kind, int radius, int D) {
     if (kind != TDV_COST_BT && (radius < 1 || radius > 4)) return false;
     return band_floats(kind, kind == TDV_COST_BT ? 0 : radius, D) * 4 <= kMaxBandBytes;
+}
+
+cudaError_t launch_fast_wta_banded(const ImgArg& L, const ImgArg& R, int D, int radius, uint16_t* disp,
+                                  float* disp_norm, cudaStream_t st) {
+    Geom g;
+    g.D = D;
+    g.Dw = D >= 32 ? 32 : D > 8 ? 16 : 8;
+    g.G = 32 / g.Dw;
+    g.lbw = left_band_width(radius);
+    g.rbw = kTX + D - 1 + 2 * radius;
+    switch (radius) {
+        case 1: return launch_fastwta_r<1>(L, R, g, disp, disp_norm, st);
+        case 2: return launch_fastwta_r<2>(L, R, g, disp, disp_norm, st);
+        case 3: return launch_fastwta_r<3>(L, R, g, disp, disp_norm, st);
+        default: return launch_fastwta_r<4>(L, R, g, disp, disp_norm, st);
+    }
 }
 
 cudaError_t launch_cost_banded(const ImgArg& L, const ImgArg& R, int kind, int radius, const VolArg& out,

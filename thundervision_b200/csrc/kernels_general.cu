@@ -515,6 +515,12 @@ cudaError_t launch_dp(const VolArg& C, uint16_t* disp, float* disp_norm, void* c
 
 cudaError_t launch_fast_wta(const ImgArg& L, const ImgArg& R, int D, int radius, uint16_t* disp,
                             float* disp_norm, cudaStream_t st, Timer* tm) {
+    if (cost_banded_supported(TDV_COST_SSD, radius, D)) {
+        const cudaError_t e = launch_fast_wta_banded(L, R, D, radius, disp, disp_norm, st);
+        if (tm) tm->mark("fast_wta");
+        return e;
+    }
+    // radius 0 or beyond 4, or bands past the shared-memory budget
     dim3 blk(16, 16), grd((L.W + 15) / 16, (L.H + 15) / 16);
     fast_wta_kernel<<<grd, blk, 0, st>>>(L, R, D, radius, disp, disp_norm);
     if (tm) tm->mark("fast_wta");

@@ -173,6 +173,9 @@ cudaError_t launch_cost(const ImgArg& L, const ImgArg& R, int kind, int radius, 
 bool cost_banded_supported(int kind, int radius, int D);
 cudaError_t launch_cost_banded(const ImgArg& L, const ImgArg& R, int kind, int radius, const VolArg& out,
                                cudaStream_t st);
+// FastWTA on the banded SSD (radius 1..4, bands within the cost kernels' budget)
+cudaError_t launch_fast_wta_banded(const ImgArg& L, const ImgArg& R, int D, int radius, uint16_t* disp,
+                                  float* disp_norm, cudaStream_t st);
 
 struct SgmArgs {
     VolArg C, S;
