@@ -90,3 +90,22 @@ def test_fast_wta_bit_exact(ctx, orc, radius, D):
         torch.cuda.synchronize()
         np.testing.assert_array_equal(out["disp"].cpu().numpy(), d_ref, err_msg=f"shape {i}")
         np.testing.assert_array_equal(out["disp_norm"].cpu().numpy(), dn_ref, err_msg=f"shape {i}")
+
+
+@pytest.mark.parametrize("D", [1, 5, 31, 32, 33, 300, 600])
+@pytest.mark.parametrize("layout", ["hwd", "ref"])
+def test_dp_bit_exact(ctx, orc, D, layout):
+    # the DP scanline matcher over disparity ranges that fill one to
+    # nineteen lanes per warp slot, rows wider than one backtrack stage
+    rng = np.random.default_rng(7 * D + (layout == "ref"))
+    lay = orc.LAYOUT_HWD if layout == "hwd" else orc.LAYOUT_REF_WHD
+    for (h, w) in ((1, 1), (3, 45), (6, 131)):
+        L8 = rng.integers(0, 256, (h, w), dtype=np.uint8)
+        R8 = rng.integers(0, 256, (h, w), dtype=np.uint8)
+        C = orc.bt_cost(orc.u8_to_f32(L8), orc.u8_to_f32(R8), D, layout=lay)
+        C[rng.random(C.shape) < 0.01] = np.float32(np.nan)
+        d_ref, dn_ref = orc.dp(C, layout=lay)
+        out = ctx.dp(torch.from_numpy(C).cuda(), layout=layout, norm=True)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out["disp"].cpu().numpy(), d_ref, err_msg=f"{h}x{w}")
+        np.testing.assert_array_equal(out["disp_norm"].cpu().numpy(), dn_ref, err_msg=f"{h}x{w}")

@@ -357,58 +357,87 @@ __global__ void lr_kernel(VolArg S, uint16_t* dispL, float* disp_norm, uint16_t*
 
 // DP scanline, one warp per row (tdvision/dynamicprogcpu.cpp:13-62 recurrence,
 // tdvision/dynamicprog.cu:68-101 backtrack).  Choice codes (1 byte per cell,
-// -1/0/+1 stored as 0/1/2) go to scratch in [y][x][d] order.
+// -1/0/+1 stored as 0/1/2) go to scratch in [y][x][d] order.  Lane l holds
+// disparities l, l+32, ... (whole-line loads of C and stores of codes), the C
+// columns of the next 4 steps are in flight in a register ring, and the
+// backtrack stages the codes of CW columns at a time in shared memory with
+// the whole warp, so lane 0's dependent chain reads shared memory.
 template <int NPL>
 __global__ void __launch_bounds__(128) dp_kernel(VolArg C, uint8_t* codes, uint16_t* disp,
                                                  float* disp_norm) {
-    const int lane = threadIdx.x & 31;
+    constexpr int CW = NPL <= 8 ? 32 : 256 / NPL;  // backtrack columns per stage
+    __shared__ __align__(16) uint8_t stage_all[4][CW * 32 * NPL];
+    __shared__ int zs_all[4][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int y = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
     if (y >= C.H) return;
+    uint8_t* const stage = stage_all[wib];
+    int* const zs = zs_all[wib];
     const int D = C.D, W = C.W;
-    const int d0 = lane * NPL;
     const float* base = (const float*)C.ptr;
     uint8_t* crow = codes + (size_t)y * W * D;
+    const int src_up = (lane + 31) & 31, src_dn = (lane + 1) & 31;
     float A[NPL];
 #pragma unroll
     for (int j = 0; j < NPL; j++) {
-        const int d = d0 + j;
+        const int d = lane + 32 * j;
         A[j] = d < D ? base[y * C.sy + d] : CUDART_INF_F;
         if (d < D) crow[d] = 1;
     }
-    for (int x = 1; x < W; x++) {
+    constexpr int K = NPL >= 16 ? 2 : 4;
+    float cr[K][NPL];
+    auto issue = [&](int x, float (&cs)[NPL]) {
         const float* cp = base + x * C.sx + y * C.sy;
-        float up = __shfl_up_sync(0xFFFFFFFFu, A[NPL - 1], 1);
-        float dn = __shfl_down_sync(0xFFFFFFFFu, A[0], 1);
-        if (lane == 0) up = CUDART_INF_F;
-        if (lane == 31) dn = CUDART_INF_F;
-        float An[NPL];
 #pragma unroll
         for (int j = 0; j < NPL; j++) {
-            const int d = d0 + j;
-            const float c1 = j > 0 ? A[j - 1] : up;
-            const float c2 = A[j];
-            const float c3 = (j < NPL - 1 ? A[j + 1] : dn);
-            float m;
-            uint8_t code;
-            if (c1 < c2 && c1 < c3) { m = c1; code = 0; }
-            else if (c2 < c3) { m = c2; code = 1; }
-            else { m = c3; code = 2; }
-            if (d < D) {
-                An[j] = __fadd_rn(cp[d], m);
-                crow[(size_t)x * D + d] = code;
-            } else {
-                An[j] = CUDART_INF_F;
-            }
+            const int d = lane + 32 * j;
+            cs[j] = d < D ? cp[d] : 0.0f;
         }
+    };
 #pragma unroll
-        for (int j = 0; j < NPL; j++) A[j] = An[j];
+    for (int k = 0; k < K; k++)
+        if (1 + k < W) issue(1 + k, cr[k]);
+    for (int x0 = 1; x0 < W; x0 += K) {
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int x = x0 + k;
+            if (x >= W) break;
+            float ru[NPL], rd[NPL];
+#pragma unroll
+            for (int j = 0; j < NPL; j++) {
+                ru[j] = __shfl_sync(0xFFFFFFFFu, A[j], src_up);
+                rd[j] = __shfl_sync(0xFFFFFFFFu, A[j], src_dn);
+            }
+            float An[NPL];
+#pragma unroll
+            for (int j = 0; j < NPL; j++) {
+                const int d = lane + 32 * j;
+                const float c1 = lane > 0 ? ru[j] : (j > 0 ? ru[j - 1] : CUDART_INF_F);
+                const float c2 = A[j];
+                const float c3 = lane < 31 ? rd[j] : (j < NPL - 1 ? rd[j + 1] : CUDART_INF_F);
+                float m;
+                uint8_t code;
+                if (c1 < c2 && c1 < c3) { m = c1; code = 0; }
+                else if (c2 < c3) { m = c2; code = 1; }
+                else { m = c3; code = 2; }
+                if (d < D) {
+                    An[j] = __fadd_rn(cr[k][j], m);
+                    crow[(size_t)x * D + d] = code;
+                } else {
+                    An[j] = CUDART_INF_F;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NPL; j++) A[j] = An[j];
+            if (x + K < W) issue(x + K, cr[k]);
+        }
     }
     // argmin of the last column, strict '<' from d = 0
     uint32_t bo = 0xFFFFFFFFu;
     int bd = 0x7FFFFFFF;
 #pragma unroll
     for (int j = 0; j < NPL; j++) {
-        const int d = d0 + j;
+        const int d = lane + 32 * j;
         if (d < D) argmin_merge(bo, bd, ford(A[j]), d);
     }
 #pragma unroll
@@ -420,16 +449,38 @@ __global__ void __launch_bounds__(128) dp_kernel(VolArg C, uint8_t* codes, uint1
     // The reference seeds its minimum with d = 0 of the last column and only a
     // strictly smaller value replaces it, so a NaN there pins d = 0.
     const bool nan0 = __shfl_sync(0xFFFFFFFFu, A[0] != A[0] ? 1 : 0, 0) != 0;
+    int z = (bd == 0x7FFFFFFF || nan0) ? 0 : bd;
+    // the codes written above must be visible to the warp's staging loads
     __syncwarp();
-    if (lane == 0) {
-        int z = (bd == 0x7FFFFFFF || nan0) ? 0 : bd;
-        for (int x = W - 1; x >= 0; x--) {
-            const int nz = z + (int)crow[(size_t)x * D + z] - 1;
-            if (nz >= 0 && nz < D) z = nz;
-            const size_t o = (size_t)y * W + x;
-            if (disp) disp[o] = (uint16_t)z;
-            if (disp_norm) disp_norm[o] = __fdiv_rn((float)z, (float)D);
+    __threadfence_block();
+    for (int xe = W - 1; xe >= 0; xe -= CW) {
+        const int xs = max(0, xe - CW + 1);
+        const int n = (xe - xs + 1) * D;
+        const uint8_t* src = crow + (size_t)xs * D;
+        if ((D & 15) == 0 && ((uintptr_t)codes & 15) == 0) {  // 16-byte aligned rows
+            for (int i = lane; i < n / 16; i += 32)
+                reinterpret_cast<uint4*>(stage)[i] = reinterpret_cast<const uint4*>(src)[i];
+        } else {
+            for (int i = lane; i < n; i += 32) stage[i] = src[i];
         }
+        __syncwarp();
+        if (lane == 0) {
+            for (int x = xe; x >= xs; x--) {
+                const int nz = z + (int)stage[(x - xs) * D + z] - 1;
+                if (nz >= 0 && nz < D) z = nz;
+                zs[x - xs] = z;
+            }
+        }
+        __syncwarp();
+        z = __shfl_sync(0xFFFFFFFFu, z, 0);
+        if (lane <= xe - xs) {
+            const int x = xs + lane;
+            const size_t o = (size_t)y * W + x;
+            const int zz = zs[lane];
+            if (disp) disp[o] = (uint16_t)zz;
+            if (disp_norm) disp_norm[o] = __fdiv_rn((float)zz, (float)D);
+        }
+        __syncwarp();
     }
 }
 
