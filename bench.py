@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batch and soft-SGM measurements")
+    ap.add_argument("--profile-case", choices=["general"],
+                    help="run one launch of each general-path kernel on 1280x720, D=64 and exit "
+                         "(the case the general-path ncu summary is captured on)")
     return ap.parse_args()
 
 
@@ -756,8 +759,34 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def profile_case_general():
+    """One launch of each general-path kernel on a 1280x720 pair, D=64 (a
+    236 MB DSI, larger than L2): BT cost, SGM with the reference table and
+    REF_GPU semantics, DP, FastWTA, SSD 7x7 cost."""
+    import torch
+
+    from thundervision_b200 import api, synthetic
+    ctx = api.Context(0)
+    dev = torch.device("cuda", 0)
+    w, h, d = 1280, 720, 64
+    l, r, _, _ = synthetic.pair_sized(w, h, d, 3)
+    lf = torch.from_numpy(l).to(dev).float() * (1.0 / 255.0)
+    rf = torch.from_numpy(r).to(dev).float() * (1.0 / 255.0)
+    C = ctx.cost(lf, rf, d)
+    ctx.sgm(C, 30 / 255, 150 / 255, guide=lf, p2_mode="adjust", table="ref", semantics="ref_gpu")
+    ctx.dp(C)
+    ctx.fast_wta(lf, rf, d)
+    ctx.cost(lf, rf, d, kind="ssd", radius=3)
+    torch.cuda.synchronize()
+    ctx.close()
+    print(json.dumps({"profile_case": "general", "ok": True}))
+
+
 def main():
     args = parse()
+    if args.profile_case == "general":
+        profile_case_general()
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
