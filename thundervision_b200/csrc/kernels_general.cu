@@ -105,127 +105,134 @@ __device__ __forceinline__ float smin(float a, float b) { return (b < a) ? b : a
 // every load and store of a step moves whole 128-byte lines.  Neighbours
 // d-1 and d+1 come from one rotation shuffle each: lane l-1 (or lane 31 of
 // the previous group for lane 0) and lane l+1 (lane 0 of the next group for
-// lane 31).
-template <int NPL>
+// lane 31).  SEM and FIRST (the pass that writes S instead of adding to it)
+// are compile-time, so a step carries no branch on either.
+template <int NPL, int SEM, bool FIRST>
 __global__ void __launch_bounds__(128) sgm_pass_kernel(SgmArgs a, const Walk* __restrict__ walks,
-                                                       int nwalks, int dx, int dy, int first) {
+                                                       int nwalks, int dx, int dy) {
     const int lane = threadIdx.x & 31;
     const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
     if (w >= nwalks) return;
     const Walk wk = walks[w];
     const int D = a.C.D;
-    const bool refcpu = a.sem == TDV_SEM_REF_CPU;
-    const bool refgpu = a.sem == TDV_SEM_REF_GPU;
+    constexpr bool refcpu = SEM == TDV_SEM_REF_CPU;
+    constexpr bool refgpu = SEM == TDV_SEM_REF_GPU;
     const int mlim = refcpu ? D - 1 : D;  // REF_CPU scans {sentinel, L(0..D-2)}
-    const float* C = (const float*)a.C.ptr;
-    float* S = (float*)a.S.ptr;
     const int src_up = (lane + 31) & 31, src_dn = (lane + 1) & 31;
+    // the walk's cells: base + t * stride
+    const float* const cbase = (const float*)a.C.ptr + wk.sx * a.C.sx + wk.sy * a.C.sy;
+    float* const sbase = (float*)a.S.ptr + wk.sx * a.S.sx + wk.sy * a.S.sy;
+    const long long cstride = dx * a.C.sx + dy * a.C.sy, sstride = dx * a.S.sx + dy * a.S.sy;
 
-    int x = wk.sx, y = wk.sy;
     float L[NPL];
-    {
-        const float* cp = C + x * a.C.sx + y * a.C.sy;
-        float* sp = S + x * a.S.sx + y * a.S.sy;
-        uint32_t mo = 0xFFFFFFFFu;
+    uint32_t mo = 0xFFFFFFFFu;
+#pragma unroll
+    for (int j = 0; j < NPL; j++) {
+        const int d = lane + 32 * j;
+        const float c = d < D ? cbase[d] : CUDART_INF_F;
+        if (d < mlim) mo = min(mo, ford(c));
+        if (d < D) {
+            if (refcpu || FIRST) {
+                sbase[d] = c;
+            } else if (wk.mult == 1) {
+                sbase[d] = __fadd_rn(sbase[d], c);
+            } else {
+                a.defer[(size_t)wk.defer * D + d] = c;  // added mult times by sgm_deferred_kernel
+            }
+        }
+        L[j] = (refgpu && d < D) ? __fadd_rn(c, a.p1) : c;
+    }
+    // minimum over d with fminf semantics starting from +INF: NaN ignored,
+    // no candidate -> +INF
+    mo = __reduce_min_sync(0xFFFFFFFFu, mo);
+    float m = mo == 0xFFFFFFFFu ? CUDART_INF_F : fdeord(mo);
+    const int len = wk.len;
+
+    // P2 / |I(t) - I(t-1)| for 32 steps at a time, lane l holding step
+    // t0 + l: the guide values of the next block are loaded one block ahead,
+    // and a step takes its value with one shuffle.
+    const bool adj = a.p2_adjust;
+    auto guide_at = [&](int t) {
+        return t < len ? img_at(a.guide, wk.sx + t * dx, wk.sy + t * dy) : 0.0f;
+    };
+    float gcur = 0.0f, gprev = 0.0f, p2blk = a.p2;
+    if (adj) {
+        gcur = guide_at(1 + lane);
+        gprev = guide_at(lane);
+    }
+
+    // Steps 1..len-1.  The C and S loads of step t are issued K steps ahead
+    // into a register ring, so a walk keeps K steps of loads in flight;
+    // cells are distinct along a walk and across the walks of a pass, so a
+    // prefetched S is never stale.
+    constexpr int K = NPL <= 2 ? 8 : 4;
+    float cr[K][NPL], sr[K][NPL];
+    auto issue = [&](int t, float (&cs)[NPL], float (&ss)[NPL]) {
+        const float* cq = cbase + t * cstride;
+        const float* sq = sbase + t * sstride;
 #pragma unroll
         for (int j = 0; j < NPL; j++) {
             const int d = lane + 32 * j;
-            const float c = d < D ? cp[d] : CUDART_INF_F;
-            if (d < mlim) mo = min(mo, ford(c));
-            if (d < D) {
-                if (refcpu || first) {
-                    sp[d] = c;
-                } else if (wk.mult == 1) {
-                    sp[d] = __fadd_rn(sp[d], c);
-                } else {
-                    a.defer[(size_t)wk.defer * D + d] = c;  // added mult times by sgm_deferred_kernel
-                }
-            }
-            L[j] = (refgpu && d < D) ? __fadd_rn(c, a.p1) : c;
+            cs[j] = d < D ? cq[d] : CUDART_INF_F;
+            ss[j] = (!FIRST && d < D) ? sq[d] : 0.0f;
         }
-        // minimum over d with fminf semantics starting from +INF: NaN ignored,
-        // no candidate -> +INF
-        mo = __reduce_min_sync(0xFFFFFFFFu, mo);
-        float m = mo == 0xFFFFFFFFu ? CUDART_INF_F : fdeord(mo);
-        float lastI = a.has_guide ? img_at(a.guide, x, y) : 0.0f;
+    };
+#pragma unroll
+    for (int k = 0; k < K; k++)
+        if (1 + k < len) issue(1 + k, cr[k], sr[k]);
 
-        // Steps 1..len-1.  The loads of step t (C, S unless this is the
-        // first pass, the guide intensity) are issued K steps ahead into a
-        // register ring, so a walk keeps K steps of loads in flight instead
-        // of waiting on each step's own; cells are distinct along a walk and
-        // across the walks of a pass, so a prefetched S is never stale.
-        constexpr int K = NPL <= 2 ? 8 : 4;
-        float cr[K][NPL], sr[K][NPL], ir[K];
-        const int len = wk.len;
-        auto issue = [&](int t, float (&cs)[NPL], float (&ss)[NPL], float& is) {
-            const int xx = wk.sx + t * dx, yy = wk.sy + t * dy;
-            const float* cq = C + xx * a.C.sx + yy * a.C.sy;
-            const float* sq = S + xx * a.S.sx + yy * a.S.sy;
+    for (int t0 = 1; t0 < len; t0 += K) {
+        if (adj && ((t0 - 1) & 31) == 0) {
+            // a new block of 32 steps: its P2 values from the loaded guide
+            // intensities, then the loads for the block after it
+            p2blk = __fdiv_rn(a.p2, fabsf(__fsub_rn(gcur, gprev)));
+            gcur = guide_at(t0 + 32 + lane);
+            gprev = guide_at(t0 + 31 + lane);
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int t = t0 + k;
+            if (t >= len) break;
+            float* sq = sbase + t * sstride;
+            const float p2a = adj ? __shfl_sync(0xFFFFFFFFu, p2blk, (t - 1) & 31) : a.p2;
+            const float mp2 = __fadd_rn(m, p2a);
+            float ru[NPL], rd[NPL];
+#pragma unroll
+            for (int j = 0; j < NPL; j++) {
+                ru[j] = __shfl_sync(0xFFFFFFFFu, L[j], src_up);
+                rd[j] = __shfl_sync(0xFFFFFFFFu, L[j], src_dn);
+            }
+            float Ln[NPL];
+            uint32_t mn_o = 0xFFFFFFFFu;
 #pragma unroll
             for (int j = 0; j < NPL; j++) {
                 const int d = lane + 32 * j;
-                cs[j] = d < D ? cq[d] : CUDART_INF_F;
-                ss[j] = (!first && d < D) ? sq[d] : 0.0f;
-            }
-            is = a.p2_adjust ? img_at(a.guide, xx, yy) : 0.0f;
-        };
-#pragma unroll
-        for (int k = 0; k < K; k++)
-            if (1 + k < len) issue(1 + k, cr[k], sr[k], ir[k]);
-
-        for (int t0 = 1; t0 < len; t0 += K) {
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-                const int t = t0 + k;
-                if (t >= len) break;
-                x = wk.sx + t * dx;
-                y = wk.sy + t * dy;
-                float* sq = S + x * a.S.sx + y * a.S.sy;
-                float p2a = a.p2;
-                if (a.p2_adjust) {
-                    const float I = ir[k];
-                    p2a = __fdiv_rn(a.p2, fabsf(__fsub_rn(I, lastI)));
-                    lastI = I;
-                }
-                const float mp2 = __fadd_rn(m, p2a);
-                float ru[NPL], rd[NPL];
-#pragma unroll
-                for (int j = 0; j < NPL; j++) {
-                    ru[j] = __shfl_sync(0xFFFFFFFFu, L[j], src_up);
-                    rd[j] = __shfl_sync(0xFFFFFFFFu, L[j], src_dn);
-                }
-                float Ln[NPL];
-                uint32_t mn_o = 0xFFFFFFFFu;
-#pragma unroll
-                for (int j = 0; j < NPL; j++) {
-                    const int d = lane + 32 * j;
-                    const float lm = lane > 0 ? ru[j] : (j > 0 ? ru[j - 1] : CUDART_INF_F);
-                    const float lp = lane < 31 ? rd[j] : (j < NPL - 1 ? rd[j + 1] : CUDART_INF_F);
-                    const float b = __fadd_rn(lm, a.p1);
-                    const float e = __fadd_rn(lp, a.p1);
-                    float mn;
-                    if (refcpu) mn = smin(L[j], smin(b, smin(e, mp2)));
-                    else mn = fminf(L[j], fminf(b, fminf(e, mp2)));
-                    float v = __fsub_rn(__fadd_rn(cr[k][j], mn), m);
-                    if (d >= D) v = CUDART_INF_F;
-                    Ln[j] = v;
-                    if (d < mlim) mn_o = min(mn_o, ford(v));
-                    if (d < D) {
-                        if (first) {
-                            sq[d] = v;
-                        } else if (wk.mult == 1) {
-                            sq[d] = __fadd_rn(sr[k][j], v);
-                        } else {
-                            a.defer[((size_t)wk.defer + t) * D + d] = v;
-                        }
+                const float lm = lane > 0 ? ru[j] : (j > 0 ? ru[j - 1] : CUDART_INF_F);
+                const float lp = lane < 31 ? rd[j] : (j < NPL - 1 ? rd[j + 1] : CUDART_INF_F);
+                const float b = __fadd_rn(lm, a.p1);
+                const float e = __fadd_rn(lp, a.p1);
+                float mn;
+                if (refcpu) mn = smin(L[j], smin(b, smin(e, mp2)));
+                else mn = fminf(L[j], fminf(b, fminf(e, mp2)));
+                float v = __fsub_rn(__fadd_rn(cr[k][j], mn), m);
+                if (d >= D) v = CUDART_INF_F;
+                Ln[j] = v;
+                if (d < mlim) mn_o = min(mn_o, ford(v));
+                if (d < D) {
+                    if (FIRST) {
+                        sq[d] = v;
+                    } else if (wk.mult == 1) {
+                        sq[d] = __fadd_rn(sr[k][j], v);
+                    } else {
+                        a.defer[((size_t)wk.defer + t) * D + d] = v;
                     }
                 }
-#pragma unroll
-                for (int j = 0; j < NPL; j++) L[j] = Ln[j];
-                mn_o = __reduce_min_sync(0xFFFFFFFFu, mn_o);
-                m = mn_o == 0xFFFFFFFFu ? CUDART_INF_F : fdeord(mn_o);
-                if (t + K < len) issue(t + K, cr[k], sr[k], ir[k]);
             }
+#pragma unroll
+            for (int j = 0; j < NPL; j++) L[j] = Ln[j];
+            mn_o = __reduce_min_sync(0xFFFFFFFFu, mn_o);
+            m = mn_o == 0xFFFFFFFFu ? CUDART_INF_F : fdeord(mn_o);
+            if (t + K < len) issue(t + K, cr[k], sr[k]);
         }
     }
 }
@@ -264,8 +271,14 @@ cudaError_t run_passes(const SgmArgs& a, const PassSchedule& sch, cudaStream_t s
         const Pass& ps = sch.passes[p];
         const int nw = (int)ps.count;
         const int blocks = (nw + wpb - 1) / wpb;
-        sgm_pass_kernel<NPL><<<blocks, wpb * 32, 0, st>>>(a, sch.d_walks + ps.first, nw, ps.dx, ps.dy,
-                                                          p == 0 ? 1 : 0);
+        const bool first = p == 0;
+        auto kern = a.sem == TDV_SEM_REF_CPU ? (first ? sgm_pass_kernel<NPL, TDV_SEM_REF_CPU, true>
+                                                      : sgm_pass_kernel<NPL, TDV_SEM_REF_CPU, false>)
+                    : a.sem == TDV_SEM_REF_GPU ? (first ? sgm_pass_kernel<NPL, TDV_SEM_REF_GPU, true>
+                                                        : sgm_pass_kernel<NPL, TDV_SEM_REF_GPU, false>)
+                    : (first ? sgm_pass_kernel<NPL, TDV_SEM_STANDARD, true>
+                             : sgm_pass_kernel<NPL, TDV_SEM_STANDARD, false>);
+        kern<<<blocks, wpb * 32, 0, st>>>(a, sch.d_walks + ps.first, nw, ps.dx, ps.dy);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         if (tm) tm->mark("sgm_pass");
