@@ -109,3 +109,29 @@ def test_dp_bit_exact(ctx, orc, D, layout):
         torch.cuda.synchronize()
         np.testing.assert_array_equal(out["disp"].cpu().numpy(), d_ref, err_msg=f"{h}x{w}")
         np.testing.assert_array_equal(out["disp_norm"].cpu().numpy(), dn_ref, err_msg=f"{h}x{w}")
+
+
+@pytest.mark.parametrize("D", [1, 3, 4, 8, 33, 64, 100, 256])
+@pytest.mark.parametrize("layout", ["hwd", "ref"])
+def test_wta_and_lr_bit_exact(ctx, orc, D, layout):
+    # WTA (thread per pixel when D is a multiple of 4, warp per pixel
+    # otherwise) and the left-right check (right-view argmin tiled through
+    # shared memory) on volumes with ties, NaN and +INF cells, rows wider
+    # than one 256-pixel tile
+    rng = np.random.default_rng(11 * D + (layout == "ref"))
+    lay = orc.LAYOUT_HWD if layout == "hwd" else orc.LAYOUT_REF_WHD
+    for (h, w) in ((1, 1), (4, 37), (3, 600)):
+        shape = (h, w, D) if layout == "hwd" else (w, h, D)
+        V = (rng.integers(0, 8, shape) / np.float32(4.0)).astype(np.float32)  # many ties
+        V[rng.random(shape) < 0.02] = np.float32(np.nan)
+        V[rng.random(shape) < 0.02] = np.float32(np.inf)
+        d_ref, dn_ref = orc.wta(V, layout=lay)
+        out = ctx.wta(torch.from_numpy(V).cuda(), layout=layout, norm=True)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out["disp"].cpu().numpy(), d_ref, err_msg=f"wta {h}x{w}")
+        np.testing.assert_array_equal(out["disp_norm"].cpu().numpy(), dn_ref, err_msg=f"wta {h}x{w}")
+        dl, dr = orc.lr_check(V, d_ref, thr=1, layout=lay)
+        out = ctx.wta(torch.from_numpy(V).cuda(), layout=layout, lr=1, right=True)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out["disp"].cpu().numpy(), dl, err_msg=f"lr {h}x{w}")
+        np.testing.assert_array_equal(out["disp_right"].cpu().numpy(), dr, err_msg=f"lr right {h}x{w}")

@@ -329,6 +329,118 @@ __global__ void wta_kernel(VolArg V, uint16_t* disp, float* disp_norm) {
     }
 }
 
+// Winner-take-all, one thread per pixel, for D a multiple of 4 and a 16-byte
+// aligned volume: the pixel's D-run is read with 16-byte loads, eight in
+// flight per thread, and reduced in the thread in increasing d (strict '<',
+// so the lowest d wins a tie; NaN and +INF never win; no finite value ->
+// d = 0), the order wta_kernel's merge gives.  Threads take pixels in memory
+// order of the layout.
+__global__ void __launch_bounds__(256) wta_thread_kernel(VolArg V, uint16_t* disp, float* disp_norm,
+                                                         int xmajor) {
+    const size_t npix = (size_t)V.W * V.H;
+    const float* base = (const float*)V.ptr;
+    const int n4 = V.D >> 2;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < npix; q += (size_t)gridDim.x * blockDim.x) {
+        int x, y;
+        if (xmajor) {
+            x = (int)(q / V.H);
+            y = (int)(q - (size_t)x * V.H);
+        } else {
+            y = (int)(q / V.W);
+            x = (int)(q - (size_t)y * V.W);
+        }
+        const float4* vp = reinterpret_cast<const float4*>(base + x * V.sx + y * V.sy);
+        uint32_t bo = ford(CUDART_INF_F);
+        int bd = 0x7FFFFFFF;
+        for (int i0 = 0; i0 < n4; i0 += 8) {
+            float4 f[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                if (i0 + k < n4) f[k] = vp[i0 + k];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                if (i0 + k >= n4) break;
+                const int d = 4 * (i0 + k);
+                const float v4[4] = {f[k].x, f[k].y, f[k].z, f[k].w};
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+                    if (v4[e] < CUDART_INF_F) {
+                        const uint32_t o = ford(v4[e]);
+                        if (o < bo) {
+                            bo = o;
+                            bd = d + e;
+                        }
+                    }
+            }
+        }
+        const int d = bd == 0x7FFFFFFF ? 0 : bd;
+        const size_t o = (size_t)y * V.W + x;
+        if (disp) disp[o] = (uint16_t)d;
+        if (disp_norm) disp_norm[o] = __fdiv_rn((float)d, (float)V.D);
+    }
+}
+
+// Left-right check with the right-view argmin tiled through shared memory:
+// one block per row; for 256 right pixels at a time and 32 disparities at a
+// time the block stages S(x, y, d) for the 288 pixels those diagonals touch
+// (each pixel's 32-disparity run is one 128-byte line, one warp load), in a
+// 33-float row pitch so thread t reading S(xr0 + t + dd, dd) hits bank
+// (t + 2 dd) mod 32.  Each thread keeps its right pixel's best (cost, d) in
+// increasing d.  Then the row's left pixels are checked as in lr_kernel.
+constexpr int kLrTile = 256;
+__global__ void __launch_bounds__(256) lr_tiled_kernel(VolArg S, uint16_t* dispL, float* disp_norm,
+                                                       uint16_t* dispR, int thr) {
+    extern __shared__ float lsm[];
+    float* tile = lsm;                                              // [kLrTile + 32][33]
+    uint16_t* sdr = reinterpret_cast<uint16_t*>(lsm + (kLrTile + 32) * 33);  // [W]
+    const int y = blockIdx.x;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const float* base = (const float*)S.ptr;
+    const int W = S.W, D = S.D;
+    for (int xr0 = 0; xr0 < W; xr0 += kLrTile) {
+        uint32_t bo = ford(CUDART_INF_F);
+        int bd = 0x7FFFFFFF;
+        const int xr = xr0 + t;
+        for (int c = 0; c < D; c += 32) {
+            __syncthreads();
+            for (int i = warp; i < kLrTile + 32; i += 8) {
+                const int x = xr0 + c + i, d = c + lane;
+                tile[i * 33 + lane] = (x < W && d < D) ? base[x * S.sx + y * S.sy + d] : CUDART_INF_F;
+            }
+            __syncthreads();
+#pragma unroll 8
+            for (int dd = 0; dd < 32; dd++) {
+                const int d = c + dd;
+                if (d < D && xr + d < W) {
+                    const float v = tile[(t + dd) * 33 + dd];
+                    if (v < CUDART_INF_F) {
+                        const uint32_t o = ford(v);
+                        if (o < bo) {
+                            bo = o;
+                            bd = d;
+                        }
+                    }
+                }
+            }
+        }
+        if (xr < W) {
+            const uint16_t d = (uint16_t)(bd == 0x7FFFFFFF ? 0 : bd);
+            sdr[xr] = d;
+            if (dispR) dispR[(size_t)y * W + xr] = d;
+        }
+    }
+    __syncthreads();
+    for (int x = t; x < W; x += blockDim.x) {
+        const size_t o = (size_t)y * W + x;
+        const int dl = dispL[o];
+        const int xr = x - dl;
+        if (xr < 0 || abs(dl - (int)sdr[xr]) > thr) {
+            dispL[o] = 0xFFFF;
+            if (disp_norm) disp_norm[o] = -1.0f;
+        }
+    }
+}
+
 // Left-right check, one block per row.  dR(xr) = argmin_d S(xr+d, y, d) over
 // xr+d < W; a left pixel is rejected (0xFFFF, d/D = -1) when x-dL < 0 or
 // |dL - dR(x-dL)| > thr.
@@ -549,14 +661,21 @@ cudaError_t launch_sgm_passes(const SgmArgs& a, const PassSchedule& sch, cudaStr
 
 cudaError_t launch_wta(const VolArg& V, uint16_t* disp, float* disp_norm, cudaStream_t st, Timer* tm) {
     const size_t npix = (size_t)V.W * V.H;
-    wta_kernel<<<grid_for(npix * 32, 256), 256, 0, st>>>(V, disp, disp_norm);
+    if ((V.D & 3) == 0 && ((uintptr_t)V.ptr & 15) == 0)
+        wta_thread_kernel<<<grid_for(npix, 256), 256, 0, st>>>(V, disp, disp_norm, V.sx > V.sy ? 1 : 0);
+    else
+        wta_kernel<<<grid_for(npix * 32, 256), 256, 0, st>>>(V, disp, disp_norm);
     if (tm) tm->mark("wta");
     return cudaGetLastError();
 }
 
 cudaError_t launch_lr(const VolArg& S, uint16_t* dispL, float* disp_norm, uint16_t* dispR, int thr,
                       cudaStream_t st, Timer* tm) {
-    lr_kernel<<<S.H, 256, S.W * sizeof(uint16_t), st>>>(S, dispL, disp_norm, dispR, thr);
+    const size_t tiled = (size_t)(kLrTile + 32) * 33 * sizeof(float) + (size_t)S.W * sizeof(uint16_t);
+    if (tiled <= 48 * 1024)
+        lr_tiled_kernel<<<S.H, 256, tiled, st>>>(S, dispL, disp_norm, dispR, thr);
+    else
+        lr_kernel<<<S.H, 256, S.W * sizeof(uint16_t), st>>>(S, dispL, disp_norm, dispR, thr);
     if (tm) tm->mark("lr_check");
     return cudaGetLastError();
 }
