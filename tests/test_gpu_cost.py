@@ -135,3 +135,21 @@ def test_wta_and_lr_bit_exact(ctx, orc, D, layout):
         torch.cuda.synchronize()
         np.testing.assert_array_equal(out["disp"].cpu().numpy(), dl, err_msg=f"lr {h}x{w}")
         np.testing.assert_array_equal(out["disp_right"].cpu().numpy(), dr, err_msg=f"lr right {h}x{w}")
+
+
+@pytest.mark.parametrize("kind,radius,D", [("ssd", 4, 1000), ("ncc", 4, 1000), ("bt", 0, 1500)])
+def test_cost_bands_past_48kb(ctx, orc, kind, radius, D):
+    # disparity ranges whose bands need more than 48 KB of shared memory (the
+    # kernels raise their limit per device), on an image wider than one tile
+    rng = np.random.default_rng(D + radius)
+    L8 = rng.integers(0, 256, (9, 1100), dtype=np.uint8)
+    R8 = rng.integers(0, 256, (9, 1100), dtype=np.uint8)
+    C = ctx.cost(torch.from_numpy(L8).cuda(), torch.from_numpy(R8).cuda(), D, kind=kind, radius=radius)
+    ref = orc.cost_pair(orc.u8_to_f32(L8), orc.u8_to_f32(R8), D, KIND_ID[kind], radius)
+    torch.cuda.synchronize()
+    assert np.array_equal(C.cpu().numpy(), ref, equal_nan=True)
+    if kind == "ssd":
+        out = ctx.fast_wta(torch.from_numpy(L8).cuda(), torch.from_numpy(R8).cuda(), D, radius=radius)
+        d_ref, _ = orc.fastwta(orc.u8_to_f32(L8), orc.u8_to_f32(R8), D, radius=radius)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out["disp"].cpu().numpy(), d_ref)

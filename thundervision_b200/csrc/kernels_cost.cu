@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "tdv_internal.hpp"
@@ -268,6 +269,21 @@ __global__ void __launch_bounds__(kThreads) cost_band_kernel(ImgArg L, ImgArg Ri
     }
 }
 
+// Bands above 48 KB need the kernel's dynamic shared-memory limit raised, an
+// attribute of the function on each device: raised once per device (bit d of
+// `opted`; devices past 63 set it on every launch).
+template <typename Kern>
+cudaError_t opt_in_once(Kern k, std::atomic<unsigned long long>& opted) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (bit && (opted.load() & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxBandBytes);
+    if (e == cudaSuccess && bit) opted.fetch_or(bit);
+    return e;
+}
+
 // Order-preserving key of a candidate cost for the argmin: finite values map
 // increasing; NaN, +INF and cells outside the range map to the largest key,
 // so they never win against a finite cost (the reference's `v < best` with
@@ -381,9 +397,11 @@ cudaError_t launch_fastwta_r(const ImgArg& L, const ImgArg& Rim, const Geom& g, 
                              cudaStream_t st) {
     const int bytes = Band<TDV_COST_SSD, R>::floats(g) * 4;
     auto k = fastwta_band_kernel<R, 16>;
-    static const cudaError_t opt_in =
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxBandBytes);
-    if (opt_in != cudaSuccess) return opt_in;
+    static std::atomic<unsigned long long> opted{0};
+    if (bytes > 48 * 1024) {
+        const cudaError_t e = opt_in_once(k, opted);
+        if (e != cudaSuccess) return e;
+    }
     const int tiles_x = (L.W + kTX - 1) / kTX, tiles_y = (L.H + kTY - 1) / kTY;
     k<<<tiles_x * tiles_y, kThreads, bytes, st>>>(L, Rim, L.W, L.H, g, tiles_x, disp, disp_norm);
     return cudaGetLastError();
@@ -393,10 +411,11 @@ template <int KIND, int R, int P>
 cudaError_t launch_one(const ImgArg& L, const ImgArg& Rim, const VolArg& out, const Geom& g, cudaStream_t st) {
     const int bytes = Band<KIND, R>::floats(g) * 4;
     auto k = cost_band_kernel<KIND, R, P>;
-    // opt in once to the largest band this launcher accepts
-    static const cudaError_t opt_in =
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxBandBytes);
-    if (opt_in != cudaSuccess) return opt_in;
+    static std::atomic<unsigned long long> opted{0};
+    if (bytes > 48 * 1024) {
+        const cudaError_t e = opt_in_once(k, opted);
+        if (e != cudaSuccess) return e;
+    }
     const int tiles_x = (out.W + kTX - 1) / kTX, tiles_y = (out.H + kTY - 1) / kTY;
     k<<<tiles_x * tiles_y, kThreads, bytes, st>>>(L, Rim, out, g, tiles_x);
     return cudaGetLastError();
