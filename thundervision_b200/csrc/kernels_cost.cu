@@ -96,13 +96,13 @@ __device__ void stage(const ImgArg& L, const ImgArg& Rim, const Geom& g, int x0,
             lt[2 * kTX * kTY + i] = ma;
         }
         const int rw = kTX + g.D - 1, n = rw * kTY;
+        float2* rmm = reinterpret_cast<float2*>(rt + n);  // (min, max) pairs, 8-byte aligned
         for (int i = tid; i < n; i += kThreads) {
             const int row = i / rw, col = i - row * rw;
             float I, mi, ma;
             bt_terms(Rim, x0 - (g.D - 1) + col, y0 + row, I, mi, ma);
             rt[i] = I;
-            rt[n + i] = mi;
-            rt[2 * n + i] = ma;
+            rmm[i] = make_float2(mi, ma);
         }
         return;
     }
@@ -180,20 +180,33 @@ __global__ void __launch_bounds__(kThreads) cost_band_kernel(ImgArg L, ImgArg Ri
                 lImi[p] = lt[kTX * kTY + li];
                 lIma[p] = lt[2 * kTX * kTY + li];
             }
+            const float2* rmm = reinterpret_cast<const float2*>(rt + n);
+            const bool rows_in = y < H && xs + P <= W;
             for (int chunk = 0; chunk < chunks; chunk++) {
                 const int d = chunk * g.Dw + dl;
                 const bool dok = d < D;
                 const int de = dok ? d : D - 1;
                 const int r0 = row * (kTX + D - 1) + (xs - de) - (x0 - (D - 1));
-                float* const op = outp + y * out.sy + d;
+                float* const op = outp + y * out.sy + d + xs * out.sx;
+                float v[P];
 #pragma unroll
                 for (int p = 0; p < P; p++) {
-                    const float rI = rt[r0 + p], rImi = rt[n + r0 + p], rIma = rt[2 * n + r0 + p];
-                    const float a = fmaxf(0.0f, fmaxf(__fsub_rn(lI[p], rIma), __fsub_rn(rImi, lI[p])));
+                    const float rI = rt[r0 + p];
+                    const float2 mm = rmm[r0 + p];
+                    const float a = fmaxf(0.0f, fmaxf(__fsub_rn(lI[p], mm.y), __fsub_rn(mm.x, lI[p])));
                     const float b = fmaxf(0.0f, fmaxf(__fsub_rn(rI, lIma[p]), __fsub_rn(lImi[p], rI)));
-                    const float v = __fadd_rn(0.0f, fminf(a, b));
-                    const int x = xs + p;
-                    if (dok && y < H && x < W) op[x * out.sx] = (x - d < 0) ? CUDART_INF_F : v;
+                    v[p] = __fadd_rn(0.0f, fminf(a, b));
+                }
+                if (dok && rows_in && xs - d >= 0) {
+                    // all P cells in the image and in range: plain stores
+#pragma unroll
+                    for (int p = 0; p < P; p++) op[p * out.sx] = v[p];
+                } else if (dok && y < H) {
+#pragma unroll
+                    for (int p = 0; p < P; p++) {
+                        const int x = xs + p;
+                        if (x < W) op[p * out.sx] = (x - d < 0) ? CUDART_INF_F : v[p];
+                    }
                 }
             }
         }
