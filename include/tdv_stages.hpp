@@ -157,6 +157,18 @@ public:
         check(m_ctx.get(), tdv_cost(m_ctx.get(), &l, &r, &m_params, &v, s));
         dsi.leftOrigin = left;
     }
+    // DevStereoMatcher's default chain (devstereomatcher.cpp:22-29): both
+    // images pass `filter` (the 5x5 Gaussian fused into the cost kernel)
+    // before the cost; the filtered left image goes to `filteredLeft`
+    // (dsi.width x dsi.height floats) and becomes dsi.leftOrigin, the guide
+    // of an adjusted P2
+    void update(const FloatImage& left, const FloatImage& right, DSIMem& dsi, float* filteredLeft,
+                tdv_filter_kind filter = TDV_FILTER_GAUSS5, tdv_stream s = nullptr) {
+        tdv_image l = left.abi(), r = right.abi();
+        tdv_volume v = dsi.abi();
+        check(m_ctx.get(), tdv_cost_filtered(m_ctx.get(), &l, &r, &m_params, filter, &v, filteredLeft, s));
+        dsi.leftOrigin = FloatImage{filteredLeft, dsi.width, dsi.height};
+    }
 
 protected:
     Context& m_ctx;

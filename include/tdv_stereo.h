@@ -94,6 +94,22 @@ typedef struct {
 tdv_status tdv_cost(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right,
                     const tdv_cost_params* params, tdv_volume* out, tdv_stream stream);
 
+/* The cost of a pre-filtered pair, DevStereoMatcher's default chain
+ * (tdvision/devstereomatcher.cpp:13-48: MedianFilterCPU on both inputs, then
+ * the matching cost): `filter` (tdv_filter_kind, declared with tdv_prefilter)
+ * is applied to both images, value * scale, then the cost is taken over the
+ * filtered images exactly as tdv_cost takes it.  For TDV_FILTER_GAUSS5 with
+ * BT, or SSD / NCC of radius 1..4, the Gaussian runs inside the cost
+ * kernel's shared-memory staging and the filtered images are never stored;
+ * other cases filter into context scratch first.  Bit-identical to
+ * tdv_prefilter on both images followed by tdv_cost.  `left_filtered` (F32,
+ * the DSI's width x height, dense; NULL to skip) receives the filtered left
+ * image, the guide tdv_sgm's adjusted P2 reads (DSIMem::leftOrigin is the
+ * filtered left image, tdvision/matchingcost.cpp:30-33). */
+tdv_status tdv_cost_filtered(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right,
+                             const tdv_cost_params* params, int32_t filter, tdv_volume* out,
+                             float* left_filtered, tdv_stream stream);
+
 /* ---- semi-global aggregation ----------------------------------------- */
 typedef enum {
     TDV_SEM_STANDARD = 0, /* S += C at path starts, previous = C, full min over d */

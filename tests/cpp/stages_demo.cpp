@@ -7,7 +7,8 @@
 //   stages_demo run W H D left.u8 right.u8 out_prefix
 //       BirchfieldCostDev -> SemiGlobalCPU / SemiGlobalDev -> maps, the
 //       fused SemiGlobalLabMatcher, FastWTAMatcher and DynamicProgDev on the
-//       pair; writes out_prefix.{lab,sgm_ref_cpu,sgm_ref_gpu,fastwta,dp}.u16
+//       pair, and the Gaussian-filtered SemiGlobalDev chain; writes
+//       out_prefix.{lab,sgm_ref_cpu,sgm_ref_gpu,sgm_filtered,fastwta,dp}.u16
 //   stages_demo reconstruct W H D left.rgb right.rgb cams.f64 out_prefix
 //       the reference's reconstruction chain from 8-bit 3-channel frames:
 //       create32FGray -> Rectifier (both cameras, and the left color frame)
@@ -178,6 +179,13 @@ static int run(int W, int H, int D, const char* lp, const char* rp, const std::s
     ByteImage B8l{l8, W, H, W}, B8r{r8, W, H, W};
     lab.update(B8l, B8r, o);
     write_map(out + ".lab.u16", disp, n);
+
+    // DevStereoMatcher's default chain: Gaussian-filtered pair, SemiGlobalDev
+    // with the filtered left image as the P2 guide
+    float* filt = dev_alloc<float>(n);
+    bt.update(L, R, dsi, filt, TDV_FILTER_GAUSS5);
+    sgm_gpu.update(dsi, o);
+    write_map(out + ".sgm_filtered.u16", disp, n);
     ctx.deviceStatus();
     std::printf("run: ok\n");
     return 0;

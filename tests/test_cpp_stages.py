@@ -60,7 +60,7 @@ def test_stage_chains_match_oracle(demo, orc, tmp_path):
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     got = {k: np.fromfile(f"{prefix}.{k}.u16", dtype=np.uint16).reshape(H, W)
-           for k in ("sgm_ref_cpu", "sgm_ref_gpu", "dp", "fastwta", "lab")}
+           for k in ("sgm_ref_cpu", "sgm_ref_gpu", "sgm_filtered", "dp", "fastwta", "lab")}
 
     Lf = orc.u8_to_f32(Lh, 1.0 / 255.0)
     Rf = orc.u8_to_f32(Rh, 1.0 / 255.0)
@@ -69,6 +69,12 @@ def test_stage_chains_match_oracle(demo, orc, tmp_path):
         d_ref, _, _ = orc.sgm(C, Lf, 30.0 / 255.0, 150.0 / 255.0, p2_mode=orc.P2_ADJUST, table=orc.TABLE_REF,
                               semantics=sem, layout=orc.LAYOUT_REF_WHD, want_S=False)
         np.testing.assert_array_equal(got[key], d_ref, err_msg=key)
+    from oracle import image_ops as io
+    Gl, Gr = io.gauss5(Lf), io.gauss5(Rf)
+    Cg = orc.bt_cost(Gl, Gr, D, layout=orc.LAYOUT_REF_WHD)
+    d_ref, _, _ = orc.sgm(Cg, Gl, 30.0 / 255.0, 150.0 / 255.0, p2_mode=orc.P2_ADJUST, table=orc.TABLE_REF,
+                          semantics=orc.SEM_REF_GPU, layout=orc.LAYOUT_REF_WHD, want_S=False)
+    np.testing.assert_array_equal(got["sgm_filtered"], d_ref)
     d_ref, _ = orc.dp(C, layout=orc.LAYOUT_REF_WHD)
     np.testing.assert_array_equal(got["dp"], d_ref)
     d_ref, _ = orc.fastwta(Lf, Rf, D, radius=3)

@@ -153,3 +153,54 @@ def test_cost_bands_past_48kb(ctx, orc, kind, radius, D):
         d_ref, _ = orc.fastwta(orc.u8_to_f32(L8), orc.u8_to_f32(R8), D, radius=radius)
         torch.cuda.synchronize()
         np.testing.assert_array_equal(out["disp"].cpu().numpy(), d_ref)
+
+
+@pytest.mark.parametrize("kind,radius", [("bt", 0), ("ssd", 1), ("ssd", 3), ("ssd", 4), ("ssd", 5), ("ncc", 2),
+                                         ("ncc", 4)])
+@pytest.mark.parametrize("D", [1, 16, 33, 100])
+def test_cost_filtered_bit_exact(ctx, orc, kind, radius, D):
+    # the Gaussian fused into the cost kernel's staging (radius 5 takes the
+    # filter-then-cost path) against tdv_prefilter + tdv_cost on the GPU and
+    # against the oracle's gauss5 + cost; the filtered left image too
+    from oracle import image_ops as io
+    rng = np.random.default_rng(500 + D * 10 + radius + KIND_ID[kind])
+    for i, ((lh, lw), (rh, rw)) in enumerate(SHAPES):
+        L8 = rng.integers(0, 256, (lh, lw), dtype=np.uint8)
+        R8 = rng.integers(0, 256, (rh, rw), dtype=np.uint8)
+        layout = "hwd" if i % 2 == 0 else "ref"
+        lay = orc.LAYOUT_HWD if layout == "hwd" else orc.LAYOUT_REF_WHD
+        if i % 2 == 0:
+            s = float(np.float32(1.0) / np.float32(255.0))
+            Lt, Rt, Lh, Rh = torch.from_numpy(L8).cuda(), torch.from_numpy(R8).cuda(), L8, R8
+        else:
+            s = 1.0
+            Lh = rng.random((lh, lw), dtype=np.float32)
+            Rh = rng.random((rh, rw), dtype=np.float32)
+            Lt, Rt = padded(Lh), padded(Rh)
+        C, fl = ctx.cost_filtered(Lt, Rt, D, kind=kind, radius=radius, layout=layout, scale=s)
+        FL, FR = ctx.prefilter(Lt, "gauss5", scale=s), ctx.prefilter(Rt, "gauss5", scale=s)
+        C2 = ctx.cost(FL, FR, D, kind=kind, radius=radius, layout=layout)
+        ref = orc.cost_pair(io.gauss5(Lh, s), io.gauss5(Rh, s), D, KIND_ID[kind], radius, lay)
+        torch.cuda.synchronize()
+        H, W = min(lh, rh), min(lw, rw)
+        got = C.cpu().numpy()
+        assert np.array_equal(got, C2.cpu().numpy(), equal_nan=True), f"vs two-step, shape {i}"
+        assert np.array_equal(got, ref, equal_nan=True), f"vs oracle, shape {i}"
+        np.testing.assert_array_equal(fl.cpu().numpy(), FL.cpu().numpy()[:H, :W])
+
+
+def test_cost_filtered_median_and_validation(ctx, orc):
+    from oracle import image_ops as io
+    from thundervision_b200 import _lib as L
+    rng = np.random.default_rng(9)
+    L8 = rng.integers(0, 256, (20, 90), dtype=np.uint8)
+    R8 = rng.integers(0, 256, (20, 90), dtype=np.uint8)
+    s = float(np.float32(1.0) / np.float32(255.0))
+    C, fl = ctx.cost_filtered(torch.from_numpy(L8).cuda(), torch.from_numpy(R8).cuda(), 24, kind="ssd", radius=2,
+                              scale=s, prefilter="median7")
+    ref = orc.cost_pair(io.median7(L8, s), io.median7(R8, s), 24, 1, 2)
+    torch.cuda.synchronize()
+    assert np.array_equal(C.cpu().numpy(), ref)
+    np.testing.assert_array_equal(fl.cpu().numpy(), io.median7(L8, s))
+    with pytest.raises(L.TdvError):
+        ctx.check(L.lib().tdv_cost_filtered(ctx.handle, None, None, None, 0, None, None, None))

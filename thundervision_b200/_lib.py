@@ -24,7 +24,7 @@ P2_CONST, P2_ADJUST = 0, 1
 
 # every symbol include/tdv_stereo.h declares
 EXPORTS = [
-    "tdv_cost", "tdv_sgm", "tdv_wta", "tdv_dp_scanline", "tdv_fast_wta", "tdv_stereo_sgm",
+    "tdv_cost", "tdv_cost_filtered", "tdv_sgm", "tdv_wta", "tdv_dp_scanline", "tdv_fast_wta", "tdv_stereo_sgm",
     "tdv_ctx_create", "tdv_ctx_destroy", "tdv_ctx_set_allocator", "tdv_ctx_reserve",
     "tdv_last_error_string", "tdv_status_string", "tdv_version", "tdv_volume_bytes",
     "tdv_ctx_enable_timing", "tdv_ctx_timings", "tdv_ctx_timing_name", "tdv_ctx_device_status",
@@ -111,6 +111,8 @@ def _declare(lib):
     st = ctypes.c_int
     sig = {
         "tdv_cost": (st, [vp, P(tdv_image), P(tdv_image), P(tdv_cost_params), P(tdv_volume), vp]),
+        "tdv_cost_filtered": (st, [vp, P(tdv_image), P(tdv_image), P(tdv_cost_params), ctypes.c_int32,
+                                   P(tdv_volume), vp, vp]),
         "tdv_sgm": (st, [vp, P(tdv_volume), P(tdv_image), P(tdv_sgm_params), P(tdv_volume),
                          P(tdv_disparity), vp]),
         "tdv_wta": (st, [vp, P(tdv_volume), P(tdv_disparity), vp]),

@@ -163,6 +163,29 @@ class Context:
                                     ctypes.byref(vol), _stream()))
         return out
 
+    def cost_filtered(self, left, right, max_disp, kind="bt", radius=None, layout="hwd", scale=1.0,
+                      prefilter="gauss5", out=None, left_filtered=True):
+        """Cost DSI of the pre-filtered pair, DevStereoMatcher's default chain
+        (the 5x5 Gaussian fused into the cost kernel): bit-identical to
+        ``cost(prefilter(left), prefilter(right))``.  Returns (DSI, filtered
+        left image of the DSI's size, or None)."""
+        if radius is None:
+            radius = {"bt": 0, "ssd": 3, "ncc": 1}[kind]
+        f = {"gauss5": L.FILTER_GAUSS5, "median7": L.FILTER_MEDIAN7}[prefilter]
+        H = min(left.shape[0], right.shape[0])
+        W = min(left.shape[1], right.shape[1])
+        if out is None:
+            shape = (H, W, max_disp) if _LAYOUTS[layout] == L.LAYOUT_HWD else (W, H, max_disp)
+            out = torch.empty(shape, dtype=torch.float32, device=left.device)
+        fl = torch.empty((H, W), dtype=torch.float32, device=left.device) if left_filtered else None
+        li, ri = _image(left, scale), _image(right, scale)
+        vol = _volume(out, layout)
+        p = L.tdv_cost_params(_COSTS[kind], radius)
+        self.check(L.lib().tdv_cost_filtered(self.handle, ctypes.byref(li), ctypes.byref(ri), ctypes.byref(p), f,
+                                             ctypes.byref(vol), fl.data_ptr() if fl is not None else None,
+                                             _stream()))
+        return out, fl
+
     def sgm(self, cost, p1, p2, guide=None, guide_scale=1.0, p2_mode="const", paths=8,
             table="full", semantics="standard", layout="hwd", lr=None, norm=False, right=False,
             aggreg=None):

@@ -575,6 +575,50 @@ tdv_status tdv_cost(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right,
     return TDV_OK;
 }
 
+tdv_status tdv_cost_filtered(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right,
+                             const tdv_cost_params* params, int32_t filter, tdv_volume* out,
+                             float* left_filtered, tdv_stream stream) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    TDV_TRY(check_image(ctx, left, "left"));
+    TDV_TRY(check_image(ctx, right, "right"));
+    TDV_TRY(check_volume(ctx, out, "out"));
+    if (!params) return fail(ctx, TDV_ERR_INVALID_ARG, "null cost params");
+    if (params->kind < TDV_COST_BT || params->kind > TDV_COST_NCC)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "bad cost kind %d", params->kind);
+    if (params->kind != TDV_COST_BT && (params->radius < 0 || params->radius > 15))
+        return fail(ctx, TDV_ERR_INVALID_ARG, "window radius %d outside [0,15]", params->radius);
+    if (filter != TDV_FILTER_GAUSS5 && filter != TDV_FILTER_MEDIAN7)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "bad filter kind %d", filter);
+    const int W = std::min(left->width, right->width), H = std::min(left->height, right->height);
+    if (out->width != W || out->height != H)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "out volume %dx%d != min image size %dx%d", out->width,
+                    out->height, W, H);
+    TDV_DEVICE_SCOPE(ctx);
+    ctx->timer.begin(S(stream));
+    const tdv::ImgArg L = tdv::make_img(*left), R = tdv::make_img(*right);
+    const int radius = params->kind == TDV_COST_BT ? 0 : params->radius;
+    if (filter == TDV_FILTER_GAUSS5 && tdv::cost_banded_supported(params->kind, radius, out->depth, true)) {
+        TDV_CUDA(tdv::launch_cost_banded(L, R, params->kind, radius, tdv::make_vol(*out), true, left_filtered,
+                                         S(stream)));
+        ctx->timer.mark("cost_filtered");
+        return TDV_OK;
+    }
+    // filter into scratch, then the plain cost over the filtered images
+    const size_t nl = (size_t)left->width * left->height, nr = (size_t)right->width * right->height;
+    TDV_TRY(ensure(ctx, ctx->misc, (nl + nr) * sizeof(float)));
+    float* fl = (float*)ctx->misc.ptr;
+    float* fr = fl + nl;
+    TDV_CUDA(tdv::launch_prefilter(L, filter, fl, S(stream)));
+    TDV_CUDA(tdv::launch_prefilter(R, filter, fr, S(stream)));
+    tdv::ImgArg FL{fl, left->width, left->height, left->width, 0, 1.0f};
+    tdv::ImgArg FR{fr, right->width, right->height, right->width, 0, 1.0f};
+    TDV_CUDA(tdv::launch_cost(FL, FR, params->kind, params->radius, tdv::make_vol(*out), S(stream), &ctx->timer));
+    if (left_filtered)
+        TDV_CUDA(cudaMemcpy2DAsync(left_filtered, (size_t)W * sizeof(float), fl, (size_t)left->width * sizeof(float),
+                                   (size_t)W * sizeof(float), H, cudaMemcpyDeviceToDevice, S(stream)));
+    return TDV_OK;
+}
+
 tdv_status tdv_sgm(tdv_ctx* ctx, const tdv_volume* cost, const tdv_image* guide,
                    const tdv_sgm_params* params, tdv_volume* aggreg, tdv_disparity* out,
                    tdv_stream stream) {

@@ -28,6 +28,7 @@
 #include <atomic>
 #include <cstdint>
 
+#include "gauss5.cuh"
 #include "tdv_internal.hpp"
 
 namespace tdv {
@@ -69,6 +70,21 @@ struct Band {
         if (KIND == TDV_COST_SSD) return kRows * g.lbw + kRows * g.rbw;
         return kRows * g.lbw + kRows * g.rbw + kTX * kTY + kTY * (kTX + g.D - 1);
     }
+    // With the Gaussian fused: BT first builds filtered bands of the left
+    // (kTX + 2 columns) and right (kTX + D + 1 columns) rows; every kind needs
+    // the raw rows with a 2-pixel halo and their row pass as scratch.
+    __host__ __device__ static int fl_band(const Geom& g) { return floats(g); }
+    __host__ __device__ static int fr_band(const Geom& g) { return fl_band(g) + kTY * (kTX + 2); }
+    __host__ __device__ static int widest(const Geom& g) {
+        return KIND == TDV_COST_BT ? kTX + g.D + 1 : (g.lbw > g.rbw ? g.lbw : g.rbw);
+    }
+    __host__ __device__ static int scratch(const Geom& g) {
+        return KIND == TDV_COST_BT ? fr_band(g) + kTY * (kTX + g.D + 1) : floats(g);
+    }
+    __host__ __device__ static int floats_filtered(const Geom& g) {
+        const int rows = (KIND == TDV_COST_BT ? kTY : kRows) + 4, w = widest(g);
+        return scratch(g) + rows * (w + 4) + rows * w;
+    }
 };
 
 // BT terms of one sample: I, min and max of {I, (I + I[-1]) / 2, (I + I[+1]) / 2}.
@@ -80,8 +96,53 @@ __device__ __forceinline__ void bt_terms(const ImgArg& im, int x, int y, float& 
     ma = fmaxf(a, fmaxf(b, I));
 }
 
+// band[row * bw + col] = G(clamp(c0 + col), clamp(r0 + row)) for the 5x5
+// Gaussian G of the image with replicated borders (the pre-filter kernel's
+// values, bit for bit): the raw rows the clamped range needs, with a 2-pixel
+// halo, then the row pass, then the column pass, in that kernel's order.
+__device__ void gauss_band(const ImgArg& im, int c0, int ncols, int r0, int nrows, float* band, int bw,
+                           float* scratch) {
+    const int tid = threadIdx.x;
+    const int c_lo = min(max(c0, 0), im.W - 1), c_hi = min(max(c0 + ncols - 1, 0), im.W - 1);
+    const int r_lo = min(max(r0, 0), im.H - 1), r_hi = min(max(r0 + nrows - 1, 0), im.H - 1);
+    const int nc = c_hi - c_lo + 1, nr = r_hi - r_lo + 1;
+    float* raw = scratch;                   // [nr + 4][nc + 4]
+    float* rp = scratch + (nr + 4) * (nc + 4);  // [nr + 4][nc]
+    for (int i = tid; i < (nr + 4) * (nc + 4); i += kThreads) {
+        const int row = i / (nc + 4), col = i - row * (nc + 4);
+        raw[i] = fetch(im, c_lo - 2 + col, r_lo - 2 + row);
+    }
+    __syncthreads();
+    for (int i = tid; i < (nr + 4) * nc; i += kThreads) {
+        const int row = i / nc, col = i - row * nc;
+        const float* t = raw + row * (nc + 4) + col;
+        rp[i] = gauss5(t[0], t[1], t[2], t[3], t[4]);
+    }
+    __syncthreads();
+    for (int i = tid; i < nrows * ncols; i += kThreads) {
+        const int row = i / ncols, col = i - row * ncols;
+        const int cc = min(max(c0 + col, 0), im.W - 1) - c_lo, rr = min(max(r0 + row, 0), im.H - 1) - r_lo;
+        const float* t = rp + rr * nc + cc;
+        band[row * bw + col] = gauss5(t[0], t[nc], t[2 * nc], t[3 * nc], t[4 * nc]);
+    }
+    __syncthreads();
+}
+
+// BT terms from a band of (filtered) samples: b[0], b[1], b[2] are the
+// samples at x - 1, x, x + 1.
+__device__ __forceinline__ void bt_terms_band(const float* b, float& I, float& mi, float& ma) {
+    I = b[1];
+    const float a = __fmul_rn(0.5f, __fadd_rn(I, b[0]));
+    const float c = __fmul_rn(0.5f, __fadd_rn(I, b[2]));
+    mi = fminf(a, fminf(c, I));
+    ma = fmaxf(a, fmaxf(c, I));
+}
+
+template <int R>
+__device__ void ncc_sums(const Geom& g, float* sm);
+
 template <int KIND, int R>
-__device__ void stage(const ImgArg& L, const ImgArg& Rim, const Geom& g, int x0, int y0, float* sm) {
+__device__ void stage_plain(const ImgArg& L, const ImgArg& Rim, const Geom& g, int x0, int y0, float* sm) {
     using B = Band<KIND, R>;
     const int tid = threadIdx.x;
     if (KIND == TDV_COST_BT) {
@@ -118,7 +179,17 @@ __device__ void stage(const ImgArg& L, const ImgArg& Rim, const Geom& g, int x0,
     }
     if (KIND != TDV_COST_NCC) return;
     __syncthreads();
-    // window sums of squares in the reference's tap order (rows, then columns)
+    ncc_sums<R>(g, sm);
+}
+
+// NCC: window sums of squares in the reference's tap order (rows, then
+// columns), LS per tile pixel from the left band, RS per column x - d.
+template <int R>
+__device__ void ncc_sums(const Geom& g, float* sm) {
+    using B = Band<TDV_COST_NCC, R>;
+    const int tid = threadIdx.x;
+    const float* lb = sm;
+    const float* rb = sm + B::rband(g);
     float* ls = sm + B::ls(g);
     float* rs = sm + B::rs(g);
     for (int i = tid; i < kTX * kTY; i += kThreads) {
@@ -144,13 +215,67 @@ __device__ void stage(const ImgArg& L, const ImgArg& Rim, const Geom& g, int x0,
     }
 }
 
-template <int KIND, int R, int P>
+// Fills the tile's bands (and, when FILT, writes the filtered left samples of
+// the tile's own pixels to fl_out, W x H dense).
+template <int KIND, int R, bool FILT>
+__device__ void stage(const ImgArg& L, const ImgArg& Rim, const Geom& g, int x0, int y0, float* sm, int W, int H,
+                      float* fl_out) {
+    using B = Band<KIND, R>;
+    const int tid = threadIdx.x;
+    if (FILT && KIND == TDV_COST_BT) {
+        float* fl = sm + B::fl_band(g);     // [kTY][kTX + 2]: columns x0 - 1 .. x0 + kTX
+        float* fr = sm + B::fr_band(g);     // [kTY][kTX + D + 1]: columns x0 - D .. x0 + kTX
+        float* scr = sm + B::scratch(g);
+        gauss_band(L, x0 - 1, kTX + 2, y0, kTY, fl, kTX + 2, scr);
+        gauss_band(Rim, x0 - g.D, kTX + g.D + 1, y0, kTY, fr, kTX + g.D + 1, scr);
+        float* lt = sm;
+        float* rt = sm + B::rband(g);
+        for (int i = tid; i < kTX * kTY; i += kThreads) {
+            const int row = i / kTX, col = i - row * kTX;
+            float I, mi, ma;
+            bt_terms_band(fl + row * (kTX + 2) + col, I, mi, ma);
+            lt[i] = I;
+            lt[kTX * kTY + i] = mi;
+            lt[2 * kTX * kTY + i] = ma;
+            const int x = x0 + col, y = y0 + row;
+            if (fl_out && x < W && y < H) fl_out[(size_t)y * W + x] = I;
+        }
+        const int rw = kTX + g.D - 1, n = rw * kTY;
+        float2* rmm = reinterpret_cast<float2*>(rt + n);
+        for (int i = tid; i < n; i += kThreads) {
+            const int row = i / rw, col = i - row * rw;
+            float I, mi, ma;
+            bt_terms_band(fr + row * (kTX + g.D + 1) + col, I, mi, ma);
+            rt[i] = I;
+            rmm[i] = make_float2(mi, ma);
+        }
+        return;
+    }
+    if (FILT) {
+        float* lb = sm;
+        float* rb = sm + B::rband(g);
+        float* scr = sm + B::scratch(g);
+        gauss_band(L, x0 - R, g.lbw, y0 - R, B::kRows, lb, g.lbw, scr);
+        gauss_band(Rim, x0 - (g.D - 1) - R, g.rbw, y0 - R, B::kRows, rb, g.rbw, scr);
+        if (fl_out)
+            for (int i = tid; i < kTX * kTY; i += kThreads) {
+                const int row = i / kTX, col = i - row * kTX;
+                const int x = x0 + col, y = y0 + row;
+                if (x < W && y < H) fl_out[(size_t)y * W + x] = lb[(row + R) * g.lbw + col + R];
+            }
+        if (KIND == TDV_COST_NCC) ncc_sums<R>(g, sm);
+        return;
+    }
+    stage_plain<KIND, R>(L, Rim, g, x0, y0, sm);
+}
+
+template <int KIND, int R, int P, bool FILT>
 __global__ void __launch_bounds__(kThreads) cost_band_kernel(ImgArg L, ImgArg Rim, VolArg out, Geom g,
-                                                             int tiles_x) {
+                                                             int tiles_x, float* fl_out) {
     extern __shared__ __align__(16) float sm[];
     using B = Band<KIND, R>;
     const int x0 = (blockIdx.x % tiles_x) * kTX, y0 = (blockIdx.x / tiles_x) * kTY;
-    stage<KIND, R>(L, Rim, g, x0, y0, sm);
+    stage<KIND, R, FILT>(L, Rim, g, x0, y0, sm, out.W, out.H, fl_out);
     __syncthreads();
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -319,7 +444,7 @@ __global__ void __launch_bounds__(kThreads) fastwta_band_kernel(ImgArg L, ImgArg
     extern __shared__ __align__(16) float sm[];
     using B = Band<TDV_COST_SSD, R>;
     const int x0 = (blockIdx.x % tiles_x) * kTX, y0 = (blockIdx.x / tiles_x) * kTY;
-    stage<TDV_COST_SSD, R>(L, Rim, g, x0, y0, sm);
+    stage<TDV_COST_SSD, R, false>(L, Rim, g, x0, y0, sm, W, H, nullptr);
     __syncthreads();
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -420,44 +545,57 @@ cudaError_t launch_fastwta_r(const ImgArg& L, const ImgArg& Rim, const Geom& g, 
     return cudaGetLastError();
 }
 
-template <int KIND, int R, int P>
-cudaError_t launch_one(const ImgArg& L, const ImgArg& Rim, const VolArg& out, const Geom& g, cudaStream_t st) {
-    const int bytes = Band<KIND, R>::floats(g) * 4;
-    auto k = cost_band_kernel<KIND, R, P>;
+template <int KIND, int R, int P, bool FILT>
+cudaError_t launch_one(const ImgArg& L, const ImgArg& Rim, const VolArg& out, const Geom& g, float* fl_out,
+                       cudaStream_t st) {
+    const int bytes = (FILT ? Band<KIND, R>::floats_filtered(g) : Band<KIND, R>::floats(g)) * 4;
+    auto k = cost_band_kernel<KIND, R, P, FILT>;
     static std::atomic<unsigned long long> opted{0};
     if (bytes > 48 * 1024) {
         const cudaError_t e = opt_in_once(k, opted);
         if (e != cudaSuccess) return e;
     }
     const int tiles_x = (out.W + kTX - 1) / kTX, tiles_y = (out.H + kTY - 1) / kTY;
-    k<<<tiles_x * tiles_y, kThreads, bytes, st>>>(L, Rim, out, g, tiles_x);
+    k<<<tiles_x * tiles_y, kThreads, bytes, st>>>(L, Rim, out, g, tiles_x, fl_out);
     return cudaGetLastError();
 }
 
-template <int KIND>
-cudaError_t dispatch_r(int r, const ImgArg& L, const ImgArg& Rim, const VolArg& out, const Geom& g,
+template <int KIND, bool FILT>
+cudaError_t dispatch_r(int r, const ImgArg& L, const ImgArg& Rim, const VolArg& out, const Geom& g, float* fl_out,
                        cudaStream_t st) {
     switch (r) {
-        case 1: return launch_one<KIND, 1, 16>(L, Rim, out, g, st);
-        case 2: return launch_one<KIND, 2, 16>(L, Rim, out, g, st);
-        case 3: return launch_one<KIND, 3, 16>(L, Rim, out, g, st);
-        default: return launch_one<KIND, 4, 16>(L, Rim, out, g, st);
+        case 1: return launch_one<KIND, 1, 16, FILT>(L, Rim, out, g, fl_out, st);
+        case 2: return launch_one<KIND, 2, 16, FILT>(L, Rim, out, g, fl_out, st);
+        case 3: return launch_one<KIND, 3, 16, FILT>(L, Rim, out, g, fl_out, st);
+        default: return launch_one<KIND, 4, 16, FILT>(L, Rim, out, g, fl_out, st);
     }
 }
 
-long long band_floats(int kind, int r, int D) {
+long long band_floats(int kind, int r, int D, bool filt) {
     const long long lbw = left_band_width(r), rbw = kTX + D - 1 + 2 * r;
-    if (kind == TDV_COST_BT) return 3LL * kTX * kTY + 3LL * kTY * (kTX + D - 1);
-    long long f = (long long)(kTY + 2 * r) * (lbw + rbw);
+    long long f;
+    if (kind == TDV_COST_BT) {
+        f = 3LL * kTX * kTY + 3LL * kTY * (kTX + D - 1);
+        if (filt) {
+            const long long w = kTX + D + 1, rows = kTY + 4;
+            f += (long long)kTY * (kTX + 2) + (long long)kTY * w + rows * (w + 4) + rows * w;
+        }
+        return f;
+    }
+    f = (long long)(kTY + 2 * r) * (lbw + rbw);
     if (kind == TDV_COST_NCC) f += (long long)kTX * kTY + (long long)kTY * (kTX + D - 1);
+    if (filt) {
+        const long long w = lbw > rbw ? lbw : rbw, rows = kTY + 2 * r + 4;
+        f += rows * (w + 4) + rows * w;
+    }
     return f;
 }
 
 }  // namespace
 
-bool cost_banded_supported(int kind, int radius, int D) {
+bool cost_banded_supported(int kind, int radius, int D, bool prefiltered) {
     if (kind != TDV_COST_BT && (radius < 1 || radius > 4)) return false;
-    return band_floats(kind, kind == TDV_COST_BT ? 0 : radius, D) * 4 <= kMaxBandBytes;
+    return band_floats(kind, kind == TDV_COST_BT ? 0 : radius, D, prefiltered) * 4 <= kMaxBandBytes;
 }
 
 cudaError_t launch_fast_wta_banded(const ImgArg& L, const ImgArg& R, int D, int radius, uint16_t* disp,
@@ -477,7 +615,7 @@ cudaError_t launch_fast_wta_banded(const ImgArg& L, const ImgArg& R, int D, int 
 }
 
 cudaError_t launch_cost_banded(const ImgArg& L, const ImgArg& R, int kind, int radius, const VolArg& out,
-                               cudaStream_t st) {
+                               bool prefiltered, float* left_filtered, cudaStream_t st) {
     Geom g;
     g.D = out.D;
     g.Dw = out.D >= 32 ? 32 : out.D > 8 ? 16 : 8;
@@ -485,9 +623,14 @@ cudaError_t launch_cost_banded(const ImgArg& L, const ImgArg& R, int kind, int r
     const int r = kind == TDV_COST_BT ? 0 : radius;
     g.lbw = left_band_width(r);
     g.rbw = kTX + out.D - 1 + 2 * r;
-    if (kind == TDV_COST_BT) return launch_one<TDV_COST_BT, 0, 8>(L, R, out, g, st);
-    if (kind == TDV_COST_SSD) return dispatch_r<TDV_COST_SSD>(radius, L, R, out, g, st);
-    return dispatch_r<TDV_COST_NCC>(radius, L, R, out, g, st);
+    if (prefiltered) {
+        if (kind == TDV_COST_BT) return launch_one<TDV_COST_BT, 0, 8, true>(L, R, out, g, left_filtered, st);
+        if (kind == TDV_COST_SSD) return dispatch_r<TDV_COST_SSD, true>(radius, L, R, out, g, left_filtered, st);
+        return dispatch_r<TDV_COST_NCC, true>(radius, L, R, out, g, left_filtered, st);
+    }
+    if (kind == TDV_COST_BT) return launch_one<TDV_COST_BT, 0, 8, false>(L, R, out, g, nullptr, st);
+    if (kind == TDV_COST_SSD) return dispatch_r<TDV_COST_SSD, false>(radius, L, R, out, g, nullptr, st);
+    return dispatch_r<TDV_COST_NCC, false>(radius, L, R, out, g, nullptr, st);
 }
 
 }  // namespace tdv

@@ -638,7 +638,7 @@ int grid_for(size_t n, int block) {
 cudaError_t launch_cost(const ImgArg& L, const ImgArg& R, int kind, int radius, const VolArg& out,
                         cudaStream_t st, Timer* tm) {
     if (cost_banded_supported(kind, radius, out.D)) {
-        const cudaError_t e = launch_cost_banded(L, R, kind, radius, out, st);
+        const cudaError_t e = launch_cost_banded(L, R, kind, radius, out, false, nullptr, st);
         if (tm) tm->mark("cost");
         return e;
     }

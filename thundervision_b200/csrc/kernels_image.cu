@@ -14,6 +14,7 @@
 #include <cfloat>
 #include <cstdint>
 
+#include "gauss5.cuh"
 #include "tdv_internal.hpp"
 
 namespace tdv {
@@ -130,12 +131,6 @@ __device__ __forceinline__ float img_clamped(const ImgArg& im, int x, int y) {
     return __fmul_rn(((const float*)im.ptr)[o], im.scale);
 }
 
-// [1 4 6 4 1]/16 along one axis, symmetric form c*k2 + (a1+b1)*k1 + (a2+b2)*k0
-__device__ __forceinline__ float gauss5(float a2, float a1, float c, float b1, float b2) {
-    float s = __fmul_rn(c, 0.375f);
-    s = __fadd_rn(s, __fmul_rn(__fadd_rn(a1, b1), 0.25f));
-    return __fadd_rn(s, __fmul_rn(__fadd_rn(a2, b2), 0.0625f));
-}
 
 // 5x5 Gaussian, replicated borders: input tile (kTY+4) x (kTX+4), rows
 // filtered into (kTY+4) x kTX, then columns.

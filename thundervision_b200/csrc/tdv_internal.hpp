@@ -169,10 +169,13 @@ ImgArg make_img(const tdv_image& im);
 
 cudaError_t launch_cost(const ImgArg& L, const ImgArg& R, int kind, int radius, const VolArg& out,
                         cudaStream_t st, Timer* tm);
-// banded cost kernels (kernels_cost.cu): BT, and SSD / NCC with radius 1..4
-bool cost_banded_supported(int kind, int radius, int D);
+// banded cost kernels (kernels_cost.cu): BT, and SSD / NCC with radius 1..4;
+// `prefiltered` fuses the 5x5 Gaussian of both images into the band staging
+// and writes the filtered left image (DSI width x height) when left_filtered
+// is not null
+bool cost_banded_supported(int kind, int radius, int D, bool prefiltered = false);
 cudaError_t launch_cost_banded(const ImgArg& L, const ImgArg& R, int kind, int radius, const VolArg& out,
-                               cudaStream_t st);
+                               bool prefiltered, float* left_filtered, cudaStream_t st);
 // FastWTA on the banded SSD (radius 1..4, bands within the cost kernels' budget)
 cudaError_t launch_fast_wta_banded(const ImgArg& L, const ImgArg& R, int D, int radius, uint16_t* disp,
                                   float* disp_norm, cudaStream_t st);

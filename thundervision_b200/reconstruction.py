@@ -63,9 +63,12 @@ class StereoMatcher:
 
     def __call__(self, left, right):
         if self.median_filter:
-            left = self.ctx.prefilter(left, "gauss5")
-            right = self.ctx.prefilter(right, "gauss5")
-        C = self.ctx.cost(left, right, self.max_disp, kind=self.cost)
+            # the Gaussian runs inside the cost kernel; the filtered left
+            # image is kept as the SGM's P2 guide
+            C, left = self.ctx.cost_filtered(left, right, self.max_disp, kind=self.cost, prefilter="gauss5",
+                                             left_filtered=self.optimizer == "sgm")
+        else:
+            C = self.ctx.cost(left, right, self.max_disp, kind=self.cost)
         if self.optimizer == "wta":
             return self.ctx.wta(C, norm=True)["disp_norm"]
         if self.optimizer == "dp":
