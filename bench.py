@@ -352,6 +352,29 @@ def measure_plain(ctx, dev, reps=3):
         del dsi
     out["workload"] = ("tdv_cost (BT, REF_WHD, [0,1] floats) + tdv_sgm (REF table, REF_GPU semantics, "
                        "P2 adjusted, 8 paths) + WTA")
+    # every stage of the 640x480, D=64 configuration timed alone: the three
+    # costs at the configuration's windows (SSD 5x5, NCC 9x9) and the
+    # reference's (SSD 7x7, NCC 3x3), 8-path SGM with WTA + left-right check,
+    # DP, WTA + left-right check, and the 8-path fused SGM on u8 intensities
+    l, r, _, _ = synthetic.pair_sized(640, 480, 64, 1)
+    lf = torch.from_numpy(l).to(dev).float() * (1.0 / 255.0)
+    rf = torch.from_numpy(r).to(dev).float() * (1.0 / 255.0)
+    l8, r8 = torch.from_numpy(l).to(dev), torch.from_numpy(r).to(dev)
+    dsi = torch.empty((480, 640, 64), dtype=torch.float32, device=dev)
+    c1 = {"workload": "640x480, D=64, [0,1] float images, HWD DSI; device ms per call (mean of 10 after 2)"}
+    for name, kind, rad in (("cost_bt", "bt", 0), ("cost_ssd5x5", "ssd", 2), ("cost_ssd7x7", "ssd", 3),
+                            ("cost_ncc9x9", "ncc", 4), ("cost_ncc3x3", "ncc", 1)):
+        c1[name] = _event_ms(lambda: ctx.cost(lf, rf, 64, kind=kind, radius=rad, out=dsi), 10, 2, st)
+    ctx.cost(lf, rf, 64, out=dsi)
+    c1["sgm8_ref_gpu_wta_lr"] = _event_ms(
+        lambda: ctx.sgm(dsi, 30.0 / 255.0, 150.0 / 255.0, guide=lf, p2_mode="adjust", table="ref",
+                        semantics="ref_gpu", lr=1), 10, 2, st)
+    c1["sgm8_standard_wta_lr"] = _event_ms(lambda: ctx.sgm(dsi, 10.0 / 255.0, 120.0 / 255.0, lr=1), 10, 2, st)
+    c1["dp"] = _event_ms(lambda: ctx.dp(dsi), 10, 2, st)
+    c1["wta_lr"] = _event_ms(lambda: ctx.wta(dsi, lr=1), 10, 2, st)
+    c1["fused_bt_sgm8_wta_lr_u8"] = _event_ms(lambda: ctx.stereo_sgm(l8, r8, 64, 10, 120, paths=8, lr=1), 10, 2, st)
+    out["640x480_D64_stages"] = c1
+    del dsi
     return out
 
 
