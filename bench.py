@@ -11,8 +11,9 @@ Our arm (default): `value` is frames/s with the pair already in HBM, timed
 per step with CUDA events on the launch stream, L2 flushed (256 MiB write)
 between steps; `e2e` is the same frames run as a stream through the public
 video API (video.VideoLoop): every frame copied from pinned host memory and
-its disparity map copied back inside the timed region, with two buffer sets so
-that the copies of one frame overlap the kernels of the previous one;
+its disparity map copied back inside the timed region, with two buffer sets,
+each with its own context and compute stream, so that the copies of one frame
+and the kernels of the next overlap the kernels of the previous one;
 `e2e_sequential` runs copy-in, tdv_stereo_sgm and copy-out of each step in
 sequence on one stream.  Under torchrun every rank processes its own frames (weak scaling, no
 collective on the data path); the time is the max over ranks.
@@ -739,6 +740,7 @@ def run_ours(args):
         "e2e": {"value": stream_fps, "unit": UNIT, "h2d_bytes_per_step": 2 * W * H,
                 "d2h_bytes_per_step": 2 * W * H, "ms_per_step": stream_ms / args.steps,
                 "path": "video.VideoLoop: pinned host frames in, maps out to pinned host, two buffer sets, "
+                        "each with its own context and compute stream so consecutive frames overlap, "
                         "one CUDA graph replay of the tdv_stereo_sgm kernels per frame",
                 "last_map_equals_stereo_sgm": stream_ok, "clocks": clocks_stream},
         "e2e_sequential": {"value": e2e_fps, "unit": UNIT, "h2d_bytes_per_step": 2 * W * H,

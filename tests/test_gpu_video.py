@@ -1,8 +1,9 @@
 """Video loop (double-buffered frames from pinned host memory): every frame's
 disparity map, read back to the host, is bit-identical to a ``stereo_sgm``
 call on the same frame, for both engines (one persistent batch launch per
-frame; the per-frame fused kernels captured as a CUDA graph) and with graph
-replay on and off."""
+frame; the per-frame fused kernels captured as a CUDA graph), with graph
+replay on and off, and with consecutive frames on one context or overlapped
+on two (one per buffer set, each on its own stream)."""
 import numpy as np
 import pytest
 import torch
@@ -21,14 +22,14 @@ def _frames(W, H, D, n, seed=3):
     return out
 
 
-@pytest.mark.parametrize("engine", ["persistent", "launches"])
+@pytest.mark.parametrize("engine,overlap", [("persistent", False), ("launches", False), ("launches", True)])
 @pytest.mark.parametrize("graph", [True, False])
 @pytest.mark.parametrize("paths", [8, 4])
-def test_video_loop_matches_per_frame(ctx, engine, graph, paths):
+def test_video_loop_matches_per_frame(ctx, engine, overlap, graph, paths):
     W, H, D, lr = 240, 96, 64, 1
-    frames = _frames(W, H, D, 5)
+    frames = _frames(W, H, D, 7)
     loop = video.VideoLoop(ctx, W, H, D, 10, 120, paths=paths, lr=lr, graph=graph, autotune=False,
-                           engine=engine)
+                           engine=engine, overlap=overlap)
     out = [torch.empty((H, W), dtype=torch.uint16).pin_memory() for _ in frames]
     ms = loop.run(frames, out)
     assert ms > 0

@@ -92,14 +92,22 @@ class VideoLoop:
     persistent batch launch (tdv_batch_graph_launch, tiles autotuned once).
     ``paths`` 4 or 8; P1/P2 must be multiples of 1/2 (the integer-domain
     fused path).
+
+    ``overlap=True`` (launches engine): each buffer set has its own private
+    context (its own aggregation volumes) and its own compute stream, so
+    frame t+1's passes can run while frame t finishes: the last horizontal
+    pass, bound by its instruction stream, overlaps the next frame's
+    DRAM-bound passes.  Maps are the same as with one context.
     """
 
     def __init__(self, ctx, W, H, D, p1, p2, paths=8, lr=1, graph=True, autotune=True, device="cuda",
-                 engine="launches"):
+                 engine="launches", overlap=True):
         self.ctx, self.graph, self.engine = ctx, graph, engine
         self.bufs = [(torch.empty((H, W), dtype=torch.uint8, device=device),
                       torch.empty((H, W), dtype=torch.uint8, device=device)) for _ in range(2)]
         self.copy_stream = torch.cuda.Stream(device=device)
+        self.overlap = bool(overlap) and engine == "launches"
+        self.compute_streams = [torch.cuda.Stream(device=device) for _ in range(2)] if self.overlap else None
         self.tiles = None
         if engine == "persistent":
             self.batches = [api.Batch(ctx, [(l, r, D, lr)], p1, p2, paths=paths) for (l, r) in self.bufs]
@@ -115,8 +123,11 @@ class VideoLoop:
             # context keeps other callers from growing (reallocating) them
             self.batches = []
             idx = torch.device(device).index
-            ctx = self.ctx = self._own_ctx = api.Context(torch.cuda.current_device() if idx is None else idx)
-            ctx.reserve(W, H, D)
+            dev_index = torch.cuda.current_device() if idx is None else idx
+            self._ctxs = [api.Context(dev_index) for _ in range(2 if self.overlap else 1)]
+            for c in self._ctxs:
+                c.reserve(W, H, D)
+            self.ctx = self._own_ctx = self._ctxs[0]
             self.outputs = [torch.empty((H, W), dtype=torch.uint16, device=device) for _ in range(2)]
             prm = api.L.tdv_sgm_params(float(p1), float(p2), api.L.P2_CONST, paths, api.L.TABLE_FULL,
                                        api.L.SEM_STANDARD)
@@ -146,8 +157,9 @@ class VideoLoop:
     def _call(self, b):
         import ctypes
         li, ri, o = self._calls[b]
-        self.ctx.check(api.L.lib().tdv_stereo_sgm(self.ctx.handle, ctypes.byref(li), ctypes.byref(ri), self._D,
-                                                  ctypes.byref(self._prm), ctypes.byref(o), api._stream()))
+        ctx = self._ctxs[b % len(self._ctxs)]
+        ctx.check(api.L.lib().tdv_stereo_sgm(ctx.handle, ctypes.byref(li), ctypes.byref(ri), self._D,
+                                             ctypes.byref(self._prm), ctypes.byref(o), api._stream()))
 
     def close(self):
         for b in self.batches:
@@ -155,7 +167,8 @@ class VideoLoop:
         if self.engine == "launches":
             torch.cuda.synchronize()
             self._graphs = [None, None]
-            self._own_ctx.close()
+            for c in self._ctxs:
+                c.close()
 
     def _launch(self, b):
         if self.engine == "persistent":
@@ -189,21 +202,31 @@ class VideoLoop:
                 copied[b].record(cs)
 
         n = len(host_frames)
+        streams = self.compute_streams if self.overlap else [ks, ks]
+        if self.overlap:
+            for st in streams:
+                st.wait_stream(ks)
         upload(0)
         for t in range(n):
             b = t % 2
             if t + 1 < n:
                 upload(t + 1)
-            ks.wait_event(copied[b])
-            self._launch(b)
-            host_out[t].copy_(self.outputs[b], non_blocking=True)
-            done[b].record(ks)
+            st = streams[b]
+            st.wait_event(copied[b])
+            with torch.cuda.stream(st):
+                self._launch(b)
+                host_out[t].copy_(self.outputs[b], non_blocking=True)
+            done[b].record(st)
+        if self.overlap:
+            for st in streams:
+                ks.wait_stream(st)
         t1.record(ks)
         t1.synchronize()
         for b in self.batches:
             b.status()
         if self.engine == "launches":
-            self.ctx.device_status()
+            for c in self._ctxs:
+                c.device_status()
         return t0.elapsed_time(t1)
 
     def disparity(self, left, right):
