@@ -422,22 +422,22 @@ cudaError_t opt_in_once(Kern k, std::atomic<unsigned long long>& opted) {
     return e;
 }
 
-// Order-preserving key of a candidate cost for the argmin: finite values map
-// increasing; NaN, +INF and cells outside the range map to the largest key,
-// so they never win against a finite cost (the reference's `v < best` with
-// best starting at +INF).
-__device__ __forceinline__ uint32_t cost_key(float v) {
-    const uint32_t u = __float_as_uint(v);
-    if (!(fabsf(v) < CUDART_INF_F)) return 0xFFFFFFFFu;
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
+// Order-preserving key of a window SSD for the argmin.  An SSD is a sum of
+// squares from +0, so it is +0, positive, +INF or NaN: its bits order the
+// finite values, and clamping at the bits of +INF puts NaN and +INF on one
+// key above every finite cost (the reference's `v < best` with best starting
+// at +INF never takes either; when no cost is finite the lowest d, 0, wins
+// the tie).  Cells outside the range keep the initial key 0xFFFFFFFF.
+__device__ __forceinline__ uint32_t ssd_key(float v) { return min(__float_as_uint(v), 0x7F800000u); }
 
 // FastWTA (tdvision/fastwta.cu:32-53): the window SSD of the banded kernel
 // with the argmin over d fused in, no DSI.  A lane keeps the best (key, d)
 // of its own disparities over the chunks (strict <, so its lowest d wins a
 // tie), then the lanes of a pixel group merge by (key, d) -- the lowest d
 // among the smallest costs, d = 0 when no cost is finite, as the reference's
-// scan gives.
+// scan gives.  Eight pixels per thread (half the SSD kernel's sixteen) keep
+// the per-pixel best keys within a register budget that fits four blocks per
+// SM.
 template <int R, int P>
 __global__ void __launch_bounds__(kThreads) fastwta_band_kernel(ImgArg L, ImgArg Rim, int W, int H, Geom g,
                                                                 int tiles_x, uint16_t* disp, float* disp_norm) {
@@ -499,12 +499,23 @@ __global__ void __launch_bounds__(kThreads) fastwta_band_kernel(ImgArg L, ImgArg
 #pragma unroll
                     for (int p = 0; p < P; p++) acc[p] = __fadd_rn(acc[p], t[p + b]);
             }
+            if (dok && xs - d >= 0) {  // every cell of the chunk in range
 #pragma unroll
-            for (int p = 0; p < P; p++) {
-                const uint32_t key = cost_key(acc[p]);
-                if (dok && xs + p - d >= 0 && key < bk[p]) {
-                    bk[p] = key;
-                    bd[p] = d;
+                for (int p = 0; p < P; p++) {
+                    const uint32_t key = ssd_key(acc[p]);
+                    if (key < bk[p]) {
+                        bk[p] = key;
+                        bd[p] = d;
+                    }
+                }
+            } else if (dok) {
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    const uint32_t key = ssd_key(acc[p]);
+                    if (xs + p - d >= 0 && key < bk[p]) {
+                        bk[p] = key;
+                        bd[p] = d;
+                    }
                 }
             }
         }
@@ -512,12 +523,19 @@ __global__ void __launch_bounds__(kThreads) fastwta_band_kernel(ImgArg L, ImgArg
         for (int p = 0; p < P; p++) {
             uint32_t k = bk[p];
             int dd = bd[p];
-            for (int off = g.Dw >> 1; off > 0; off >>= 1) {
-                const uint32_t ok = __shfl_xor_sync(0xFFFFFFFFu, k, off);
-                const int od = __shfl_xor_sync(0xFFFFFFFFu, dd, off);
-                if (ok < k || (ok == k && od < dd)) {
-                    k = ok;
-                    dd = od;
+            if (g.Dw == 32) {
+                // the warp is one pixel group: the smallest key, then the
+                // lowest d among the lanes holding it
+                k = __reduce_min_sync(0xFFFFFFFFu, k);
+                dd = (int)__reduce_min_sync(0xFFFFFFFFu, bk[p] == k ? (unsigned)dd : 0x7FFFFFFFu);
+            } else {
+                for (int off = g.Dw >> 1; off > 0; off >>= 1) {
+                    const uint32_t ok = __shfl_xor_sync(0xFFFFFFFFu, k, off);
+                    const int od = __shfl_xor_sync(0xFFFFFFFFu, dd, off);
+                    if (ok < k || (ok == k && od < dd)) {
+                        k = ok;
+                        dd = od;
+                    }
                 }
             }
             const int x = xs + p;
@@ -534,7 +552,7 @@ template <int R>
 cudaError_t launch_fastwta_r(const ImgArg& L, const ImgArg& Rim, const Geom& g, uint16_t* disp, float* disp_norm,
                              cudaStream_t st) {
     const int bytes = Band<TDV_COST_SSD, R>::floats(g) * 4;
-    auto k = fastwta_band_kernel<R, 16>;
+    auto k = fastwta_band_kernel<R, 8>;
     static std::atomic<unsigned long long> opted{0};
     if (bytes > 48 * 1024) {
         const cudaError_t e = opt_in_once(k, opted);
