@@ -51,9 +51,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batch and soft-SGM measurements")
-    ap.add_argument("--profile-case", choices=["general"],
-                    help="run one launch of each general-path kernel on 1280x720, D=64 and exit "
-                         "(the case the general-path ncu summary is captured on)")
+    ap.add_argument("--profile-case", choices=["general", "cost1080"],
+                    help="general: one launch of each general-path kernel on 1280x720, D=64; cost1080: "
+                         "one BT cost DSI at 1920x1080, D=256 (HWD); then exit (the cases the ncu "
+                         "summaries are captured on)")
     return ap.parse_args()
 
 
@@ -807,10 +808,32 @@ def profile_case_general():
     print(json.dumps({"profile_case": "general", "ok": True}))
 
 
+def profile_case_cost1080():
+    """One BT cost DSI (HWD, 2.12 GB) of a 1920x1080 pair at D=256 after
+    one warm-up call."""
+    import torch
+
+    from thundervision_b200 import api, synthetic
+    ctx = api.Context(0)
+    dev = torch.device("cuda", 0)
+    l, r, _, _ = synthetic.pair_sized(W, H, D, 3)
+    lf = torch.from_numpy(l).to(dev).float() * (1.0 / 255.0)
+    rf = torch.from_numpy(r).to(dev).float() * (1.0 / 255.0)
+    out = torch.empty((H, W, D), dtype=torch.float32, device=dev)
+    for _ in range(2):
+        ctx.cost(lf, rf, D, out=out)
+    torch.cuda.synchronize()
+    ctx.close()
+    print(json.dumps({"profile_case": "cost1080", "ok": True}))
+
+
 def main():
     args = parse()
     if args.profile_case == "general":
         profile_case_general()
+        return
+    if args.profile_case == "cost1080":
+        profile_case_cost1080()
         return
     if args.impl == "reference":
         run_reference(args)
