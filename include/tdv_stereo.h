@@ -389,7 +389,15 @@ void tdv_ctx_destroy(tdv_ctx* ctx);
 /* Replaces the device allocator for scratch (default cudaMalloc/cudaFree). */
 tdv_status tdv_ctx_set_allocator(tdv_ctx* ctx, tdv_alloc_fn alloc, tdv_free_fn release,
                                  void* user);
-/* Pre-sizes scratch for pairs up to W x H x D so later calls do not allocate. */
+/* Pre-sizes the scratch of tdv_stereo_sgm (the fused path: planes, both
+ * 16-bit aggregation volumes, the row scratch) for pairs up to W x H x D, so
+ * later calls of it do not allocate.  The general path sizes its own scratch
+ * on first use, once per size: tdv_sgm without a caller aggregation volume
+ * (W x H x D floats, the path schedule, the deferred costs of repeated
+ * walks), tdv_dp_scanline (W x H x D choice bytes), the filter-then-cost
+ * case of tdv_cost_filtered (both filtered images).  A caller that must not
+ * allocate later makes one call of each kind first, or passes its own
+ * volumes. */
 tdv_status tdv_ctx_reserve(tdv_ctx* ctx, int32_t width, int32_t height, int32_t max_disp);
 const char* tdv_last_error_string(const tdv_ctx* ctx);
 /* Synchronises `stream` and returns the error status kernels of this
