@@ -178,3 +178,28 @@ def test_reconstruction_arguments():
         rc.StereoMatcher(None, optimizer="graphcut")
     with pytest.raises(ValueError):
         rc.Camera(np.eye(3), [0.0] * 9, np.eye(3), np.eye(3))
+
+
+def test_cost_filtered_arguments_are_validated():
+    from thundervision_b200 import _lib as L
+    lib = L.lib()
+    h = ctypes.c_void_p()
+    assert lib.tdv_ctx_create(0, ctypes.byref(h)) == L.TDV_OK
+    try:
+        img = L.tdv_image(1 << 20, 8, 4, 8, L.U8, 1.0)
+        vol = L.tdv_volume(1 << 21, 8, 4, 4, L.LAYOUT_HWD, L.F32)
+        prm = L.tdv_cost_params(L.COST_SSD, 2)
+        assert lib.tdv_cost_filtered(None, ctypes.byref(img), ctypes.byref(img), ctypes.byref(prm), L.FILTER_GAUSS5,
+                                     ctypes.byref(vol), None, None) == L.TDV_ERR_INVALID_ARG
+        assert lib.tdv_cost_filtered(h, ctypes.byref(img), ctypes.byref(img), ctypes.byref(prm), 7,
+                                     ctypes.byref(vol), None, None) == L.TDV_ERR_INVALID_ARG  # filter kind
+        bad = L.tdv_volume(1 << 21, 9, 4, 4, L.LAYOUT_HWD, L.F32)  # not the images' size
+        assert lib.tdv_cost_filtered(h, ctypes.byref(img), ctypes.byref(img), ctypes.byref(prm), L.FILTER_GAUSS5,
+                                     ctypes.byref(bad), None, None) == L.TDV_ERR_INVALID_ARG
+        wide = L.tdv_cost_params(L.COST_NCC, 16)  # radius past 15
+        assert lib.tdv_cost_filtered(h, ctypes.byref(img), ctypes.byref(img), ctypes.byref(wide), L.FILTER_GAUSS5,
+                                     ctypes.byref(vol), None, None) == L.TDV_ERR_INVALID_ARG
+        assert lib.tdv_cost_filtered(h, ctypes.byref(img), ctypes.byref(img), None, L.FILTER_GAUSS5,
+                                     ctypes.byref(vol), None, None) == L.TDV_ERR_INVALID_ARG
+    finally:
+        lib.tdv_ctx_destroy(h)
