@@ -478,6 +478,13 @@ def measure_reconstruction(ctx, dev, frames=20, warmup=3):
                     ts.append(e0.elapsed_time(e1))
             ms = sorted(ts)[len(ts) // 2]
             res[name] = {"ms_per_frame": ms, "fps": 1000.0 / ms}
+            # the same frames as a stream, consecutive frames overlapped on two
+            # contexts, each map read back to pinned host memory
+            outs = [torch.empty((H, W), dtype=torch.float32).pin_memory() for _ in range(frames)]
+            pairs = [(lc, rcol)] * frames
+            rec.stream(pairs[:4], outs[:4])
+            sms = rec.stream(pairs, outs) / frames
+            res[name + "_stream"] = {"ms_per_frame": sms, "fps": 1000.0 / sms}
         finally:
             rec.close()
     return res

@@ -108,3 +108,24 @@ def test_cpp_reconstruct_matches_oracle_chain(orc, tmp_path):
     np.testing.assert_array_equal(np.fromfile(prefix + ".cols.f32", np.float32).reshape(H, W, 3), c)
     with open(prefix + ".ply") as f:
         assert f.read() == io.ply_text(v, c)
+
+
+@pytest.mark.parametrize("optimizer", ["wta", "sgm"])
+def test_reconstruction_stream_overlapped(ctx, orc, optimizer):
+    # frames alternate between two contexts on two streams; every map read
+    # back equals the oracle chain's for its frame
+    from thundervision_b200 import reconstruction as rc
+    left, right, Q = cameras()
+    cost = "ssd" if optimizer == "wta" else "bt"
+    m = rc.StereoMatcher(ctx, max_disp=D, cost=cost, optimizer=optimizer)
+    rec = rc.Reconstruction(ctx, W, H, rc.Camera(*left), rc.Camera(*right), Q=Q, matcher=m)
+    try:
+        scenes = [scene(60 + t) for t in range(5)]
+        frames = [(torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()) for a, b in scenes]
+        out = [torch.empty((H, W), dtype=torch.float32).pin_memory() for _ in frames]
+        assert rec.stream(frames, out) > 0
+        for t, (a, b) in enumerate(scenes):
+            ref = io.reconstruction(a, b, (left, right), D, q=Q.ravel(), cost=cost, optimizer=optimizer)[1]
+            np.testing.assert_array_equal(out[t].numpy(), ref, err_msg=f"frame {t}")
+    finally:
+        rec.close()

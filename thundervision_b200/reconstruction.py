@@ -96,6 +96,8 @@ class Reconstruction:
 
     def __init__(self, ctx, width, height, left_cam, right_cam, Q=None, zscale=1.0, matcher=None,
                  dilate=True, graph=True):
+        self._args = (width, height, left_cam, right_cam, Q, zscale, dilate, graph)
+        self._twin = None
         self.ctx, self.W, self.H = ctx, int(width), int(height)
         self.matcher = matcher if matcher is not None else StereoMatcher(ctx)
         self.dilate, self.graph = bool(dilate), bool(graph)
@@ -167,8 +169,48 @@ class Reconstruction:
             raise RuntimeError("no frame reconstructed yet")
         api.write_ply(path, out["vertices"], out["colors"])
 
+    def stream(self, frames, out_disp):
+        """Runs a stream of frames and returns the device milliseconds from
+        the first copy in to the last map read back.  ``frames``: list of
+        (left, right) pinned host (H, W, 3) uint8 tensors; ``out_disp``: list
+        of pinned host (H, W) float32 tensors receiving each frame's d/D map.
+        Frames alternate between this object and a twin with its own context
+        (its own scratch), input buffers, graph and CUDA stream, so
+        consecutive frames overlap on the GPU, as the video loop runs them;
+        each frame's map is the one ``update`` gives for it."""
+        if self._twin is None:
+            W, H, L, R, Q, z, dil, graph = self._args
+            m = self.matcher
+            ctx2 = api.Context(self.ctx.device)
+            self._twin = Reconstruction(ctx2, W, H, L, R, Q=Q, zscale=z, dilate=dil, graph=graph,
+                                        matcher=StereoMatcher(ctx2, m.max_disp, m.cost, m.optimizer,
+                                                              m.median_filter))
+            self._twin_ctx = ctx2
+        lanes = [self, self._twin]
+        streams = [torch.cuda.Stream(self.dev), torch.cuda.Stream(self.dev)]
+        main = torch.cuda.current_stream(self.dev)
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(main)
+        for st in streams:
+            st.wait_stream(main)
+        for t, (left, right) in enumerate(frames):
+            k = t % 2
+            with torch.cuda.stream(streams[k]):
+                out = lanes[k].update(left, right)
+                out_disp[t].copy_(out["disp"], non_blocking=True)
+        for st in streams:
+            main.wait_stream(st)
+        t1.record(main)
+        t1.synchronize()
+        return t0.elapsed_time(t1)
+
     def close(self):
         self._g = None
         self._out = None
         self._in = None
         self.last = None
+        if self._twin is not None:
+            torch.cuda.synchronize()
+            self._twin.close()
+            self._twin_ctx.close()
+            self._twin = None
