@@ -338,71 +338,73 @@ __global__ void __launch_bounds__(kThreads) cost_band_kernel(ImgArg L, ImgArg Ri
         return;
     }
 
-    for (int it = warp; it < items; it += kWarps) {
-        const int chunk = it % chunks;
-        const int rest = it / chunks;
-        const int grp = rest % groups, row = rest / groups;
-        const int y = y0 + row;
-        const int xs = x0 + grp * span + sub * P;   // first pixel of this thread
-        const int d = chunk * g.Dw + dl;
-        const bool dok = d < D;
-        const int de = dok ? d : D - 1;             // lanes past D read in-band columns, store nothing
-        float v[P];
-        {
-            constexpr int NJ = P + 2 * R;
-            float acc[P];
-#pragma unroll
-            for (int p = 0; p < P; p++) acc[p] = 0.0f;
-            const float* lb = sm + (size_t)row * g.lbw + (xs - x0);
-            const float* rb = sm + B::rband(g) + (size_t)row * g.rbw + (xs - de) - (x0 - (D - 1));
-            constexpr int NJ4 = (NJ + 3) & ~3;
-#pragma unroll 1
-            for (int a = 0; a <= 2 * R; a++) {
-                // the left window is the same for every lane: 128-bit
-                // broadcast reads (the row start is a multiple of 16 floats
-                // into a row padded to 4)
-                float lw[NJ4];
-                const float4* l4 = reinterpret_cast<const float4*>(lb + a * g.lbw);
-#pragma unroll
-                for (int q = 0; q < NJ4 / 4; q++) {
-                    const float4 f = l4[q];
-                    lw[4 * q] = f.x;
-                    lw[4 * q + 1] = f.y;
-                    lw[4 * q + 2] = f.z;
-                    lw[4 * q + 3] = f.w;
-                }
-                float t[NJ];
-#pragma unroll
-                for (int j = 0; j < NJ; j++) {
-                    const float lv = lw[j], rv = rb[a * g.rbw + j];
-                    if (KIND == TDV_COST_SSD) {
-                        const float df = __fsub_rn(lv, rv);
-                        t[j] = __fmul_rn(df, df);
-                    } else {
-                        t[j] = __fmul_rn(lv, rv);
+    if constexpr (KIND != TDV_COST_BT) {
+        for (int it = warp; it < items; it += kWarps) {
+            const int chunk = it % chunks;
+            const int rest = it / chunks;
+            const int grp = rest % groups, row = rest / groups;
+            const int y = y0 + row;
+            const int xs = x0 + grp * span + sub * P;   // first pixel of this thread
+            const int d = chunk * g.Dw + dl;
+            const bool dok = d < D;
+            const int de = dok ? d : D - 1;             // lanes past D read in-band columns, store nothing
+            float v[P];
+            {
+                constexpr int NJ = P + 2 * R;
+                float acc[P];
+    #pragma unroll
+                for (int p = 0; p < P; p++) acc[p] = 0.0f;
+                const float* lb = sm + (size_t)row * g.lbw + (xs - x0);
+                const float* rb = sm + B::rband(g) + (size_t)row * g.rbw + (xs - de) - (x0 - (D - 1));
+                constexpr int NJ4 = (NJ + 3) & ~3;
+    #pragma unroll 1
+                for (int a = 0; a <= 2 * R; a++) {
+                    // the left window is the same for every lane: 128-bit
+                    // broadcast reads (the row start is a multiple of 16 floats
+                    // into a row padded to 4)
+                    float lw[NJ4];
+                    const float4* l4 = reinterpret_cast<const float4*>(lb + a * g.lbw);
+    #pragma unroll
+                    for (int q = 0; q < NJ4 / 4; q++) {
+                        const float4 f = l4[q];
+                        lw[4 * q] = f.x;
+                        lw[4 * q + 1] = f.y;
+                        lw[4 * q + 2] = f.z;
+                        lw[4 * q + 3] = f.w;
                     }
+                    float t[NJ];
+    #pragma unroll
+                    for (int j = 0; j < NJ; j++) {
+                        const float lv = lw[j], rv = rb[a * g.rbw + j];
+                        if (KIND == TDV_COST_SSD) {
+                            const float df = __fsub_rn(lv, rv);
+                            t[j] = __fmul_rn(df, df);
+                        } else {
+                            t[j] = __fmul_rn(lv, rv);
+                        }
+                    }
+    #pragma unroll
+                    for (int b = 0; b <= 2 * R; b++)
+    #pragma unroll
+                        for (int p = 0; p < P; p++) acc[p] = __fadd_rn(acc[p], t[p + b]);
                 }
-#pragma unroll
-                for (int b = 0; b <= 2 * R; b++)
-#pragma unroll
-                    for (int p = 0; p < P; p++) acc[p] = __fadd_rn(acc[p], t[p + b]);
+                if (KIND == TDV_COST_SSD) {
+    #pragma unroll
+                    for (int p = 0; p < P; p++) v[p] = acc[p];
+                } else {
+                    const float* ls = sm + B::ls(g) + row * kTX + (xs - x0);
+                    const float* rs = sm + B::rs(g) + row * (kTX + D - 1) + (xs - de) - (x0 - (D - 1));
+    #pragma unroll
+                    for (int p = 0; p < P; p++)
+                        v[p] = __fsub_rn(1.0f, __fdiv_rn(acc[p], __fsqrt_rn(__fmul_rn(ls[p], rs[p]))));
+                }
             }
-            if (KIND == TDV_COST_SSD) {
-#pragma unroll
-                for (int p = 0; p < P; p++) v[p] = acc[p];
-            } else {
-                const float* ls = sm + B::ls(g) + row * kTX + (xs - x0);
-                const float* rs = sm + B::rs(g) + row * (kTX + D - 1) + (xs - de) - (x0 - (D - 1));
-#pragma unroll
-                for (int p = 0; p < P; p++)
-                    v[p] = __fsub_rn(1.0f, __fdiv_rn(acc[p], __fsqrt_rn(__fmul_rn(ls[p], rs[p]))));
+            if (!dok || y >= H) continue;
+    #pragma unroll
+            for (int p = 0; p < P; p++) {
+                const int x = xs + p;
+                if (x < W) outp[x * out.sx + y * out.sy + d] = (x - d < 0) ? CUDART_INF_F : v[p];
             }
-        }
-        if (!dok || y >= H) continue;
-#pragma unroll
-        for (int p = 0; p < P; p++) {
-            const int x = xs + p;
-            if (x < W) outp[x * out.sx + y * out.sy + d] = (x - d < 0) ? CUDART_INF_F : v[p];
         }
     }
 }
