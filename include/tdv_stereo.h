@@ -8,8 +8,7 @@
  * LibThunderVision) reaches the same stages through free C++ functions with no
  * extern "C"; each declaration below names the reference function it replaces
  * (paths relative to the ThunderVision root; tdvision/ =
- * LibThunderVision/src/tdvision/).  INTEGRATION.md shows the reference-side
- * adapters.
+ * LibThunderVision/src/tdvision/).
  *
  * Conventions
  *   - Images are single-channel, row-major, device memory: u8 or f32, with a
@@ -168,11 +167,19 @@ tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* 
  * every allocation, a real-time frame loop that must not stall on an
  * allocation).  It has no counterpart in the reference.  All scratch comes
  * from one 64 MiB static __device__ array held by every GPU that loads this
- * library until the process exits; pairs whose scratch exceeds it (about
- * W*H*(34 + 128*ceil(D/64)) bytes) are rejected with TDV_ERR_UNSUPPORTED, as
- * are inputs outside the fused path.  The first call on a device resolves the
- * array's address there; make it before any stream capture.  Calls share the
- * array: calls whose GPU work overlaps race. */
+ * library until the process exits.  A pair needs the BT planes,
+ * 16*(W + 9*ceil(W/8)) bytes per row (about 34 B per pixel), plus the
+ * aggregation volume, 128 B per pixel for D <= 64, 256 B for D <= 128 and
+ * 512 B for D <= 256, each rounded up to 256 bytes, plus 256 bytes; pairs
+ * that do not fit, and inputs outside the fused path, are rejected with
+ * TDV_ERR_UNSUPPORTED, malformed arguments (non-finite penalties, values
+ * outside the enums, sizes that differ) with TDV_ERR_INVALID_ARG.  The first
+ * call on a device, and the first after a device reset or in another context
+ * there, resolves the array's address; make it before any stream capture (a
+ * capturing call cannot and returns TDV_ERR_INVALID_ARG).  Calls share the
+ * array: calls whose GPU work overlaps race.  If a bounded wait inside the
+ * kernels runs out, every pixel of the requested outputs is marked invalid
+ * (0xFFFF, -1.0f). */
 tdv_status tdv_stereo_sgm_static(const tdv_image* left, const tdv_image* right, int32_t max_disp,
                                  const tdv_sgm_params* params, tdv_disparity* out, tdv_stream stream);
 

@@ -256,7 +256,7 @@ def refit_penalties(ctx, frames, max_disp, p1, p2, steps=50, lr=0.05, tau=1.0, p
         opt.zero_grad()
         loss.backward()
         opt.step()
-        hist.append({"step": it, "loss": float(loss), "p1": float(pen[0]), "p2": float(pen[1])})
+        hist.append({"step": it, "loss": loss.item(), "p1": pen[0].item(), "p2": pen[1].item()})
         del cost, dh, loss
     p = theta.detach().exp().tolist()
     return p[0], p[1], hist
