@@ -12,6 +12,7 @@
 // one walk with a repeat count; a repeat that precedes its own forward walk,
 // as in portrait images, lands in an earlier pass).
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 #include <vector>
 
@@ -140,6 +141,171 @@ bool build_schedule(int W, int H, int table, int paths, PassSchedule& out) {
         out.passes.push_back(ps);
     }
     return ok;
+}
+
+// ------------------------------------------------------------ fused weights
+namespace {
+
+// fused direction index of a walk direction (V+ V- D1+ D1- D2+ D2- H+ H-)
+int fused_dir(int dx, int dy) {
+    if (dx == 0) return dy > 0 ? 0 : 1;
+    if (dy == 0) return dx > 0 ? 6 : 7;
+    if (dx == dy) return dx > 0 ? 2 : 3;
+    return dx < 0 ? 4 : 5;
+}
+const int kFdx[kFusedDirs] = {0, 0, 1, -1, -1, 1, 1, -1};
+const int kFdy[kFusedDirs] = {1, -1, 1, -1, 1, -1, 0, 0};
+
+}  // namespace
+
+bool build_fused_weights(int W, int H, int table, int paths, bool assign, FusedWeights& out, const char** why) {
+    auto bad = [&](const char* m) {
+        if (why) *why = m;
+        return false;
+    };
+    out = FusedWeights();
+    out.W = W;
+    out.H = H;
+    out.table = table;
+    out.paths = paths;
+    out.assign = assign ? 1 : 0;
+    if (W < 1 || H < 1) return bad("empty image");
+    const size_t npx = (size_t)W * H;
+    // n[dir][cell]: walks of the direction counted in the cell's final sum,
+    // replaying the table's sequential walk order (forward, then backward,
+    // per entry; tdvision/semiglobalcpu.cpp:210-222)
+    std::vector<uint16_t> n(kFusedDirs * npx, 0);
+    const auto tab = make_table(W, H, table == TDV_TABLE_REF);
+    auto inside = [&](int x, int y) { return x >= 0 && x < W && y >= 0 && y < H; };
+    bool ok = true;
+    auto walk = [&](int sx, int sy, int dx, int dy, int len) {
+        if (len < 1 || !inside(sx, sy) || !inside(sx + (len - 1) * dx, sy + (len - 1) * dy)) {
+            ok = false;
+            return;
+        }
+        const int k = fused_dir(dx, dy);
+        const size_t c0 = (size_t)sy * W + sx;
+        if (assign)  // the start cell's sum is replaced by this walk's first cost
+            for (int j = 0; j < kFusedDirs; j++) n[j * npx + c0] = 0;
+        int x = sx, y = sy;
+        for (int i = 0; i < len; i++, x += dx, y += dy) {
+            uint16_t& v = n[k * npx + (size_t)y * W + x];
+            if (v == 0xFFFF) {
+                ok = false;
+                return;
+            }
+            v++;
+        }
+    };
+    for (const auto& e : tab) {
+        if (paths == 4 && e.dx != 0 && e.dy != 0) continue;
+        walk(e.sx, e.sy, e.dx, e.dy, e.size);
+        walk(e.ex, e.ey, -e.dx, -e.dy, e.size);
+    }
+    if (!ok) return bad("a table walk leaves the image");
+
+    auto cls = [](int v) { return v == 0 ? 0 : (v == 1 ? 1 : 2); };
+    auto border = [&](int x, int y) { return y == 0 || y == H - 1 || x == 0 || x == W - 1; };
+    out.nl = W + H - 1;
+    out.nb = 2 * W + 2 * H;
+    out.lw_off = 0;
+    out.bw_off = (size_t)6 * out.nl;
+    out.corner_off = (out.bw_off + (size_t)kFusedDirs * out.nb + 15) & ~(size_t)15;
+    out.bytes = out.corner_off + (size_t)H * 16;
+    out.image.assign(out.bytes, 0);
+    unsigned char* lw = out.image.data() + out.lw_off;
+    unsigned char* bw = out.image.data() + out.bw_off;
+    int32_t* corner = (int32_t*)(out.image.data() + out.corner_off);
+    for (int y = 0; y < H; y++) {
+        corner[4 * y + 0] = -1;
+        corner[4 * y + 2] = -1;
+    }
+    int corner_line[2] = {INT32_MIN, INT32_MIN};
+
+    for (int k = 0; k < kFusedDirs; k++) {
+        const uint16_t* nk = n.data() + k * npx;
+        const bool active = paths == 8 || kFdx[k] == 0 || kFdy[k] == 0;
+        // border classes, checked against the line classes below
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++)
+                if (border(x, y)) bw[(size_t)k * out.nb + border_index(W, H, x, y)] = (unsigned char)cls(nk[(size_t)y * W + x]);
+        if (!active) continue;
+        // line classes: a line is the set of cells x - s*y = kp (vertical and
+        // diagonal) or a row (horizontal); its interior cells share one weight
+        const int dx = kFdx[k], dy = kFdy[k];
+        const int s = dx * dy;
+        const bool horiz = dy == 0;
+        const int nlines = horiz ? H : (s == 0 ? W : W + H - 1);
+        const int kmin = s > 0 ? -(H - 1) : 0;
+        for (int j = 0; j < nlines; j++) {
+            int interior = -1, any = 0;
+            bool mixed = false;
+            auto visit = [&](int x, int y) {
+                const int v = nk[(size_t)y * W + x];
+                any |= v;
+                if (border(x, y)) return;
+                if (interior < 0) interior = v;
+                else if (interior != v) mixed = true;
+            };
+            if (horiz) {
+                for (int x = 0; x < W; x++) visit(x, j);
+            } else {
+                const int kp = kmin + j;
+                for (int y = 0; y < H; y++) {
+                    const int x = kp + s * y;
+                    if (x >= 0 && x < W) visit(x, y);
+                }
+            }
+            if (mixed) return bad("cells inside one path line count it differently");
+            int c;
+            if (any == 0) c = 0;            // no walk of this direction: skip the line
+            else if (interior == 0) return bad("a walked line counts only at the border");
+            else c = interior < 0 ? 1 : cls(interior);
+            if (horiz) {
+                // rows 0 and H-1 are all border cells: their classes decide
+                if (interior >= 0 && c != 1) return bad("a horizontal line that does not count once");
+                continue;
+            }
+            lw[(size_t)k * out.nl + j] = (unsigned char)c;
+            if (c != 1) out.has_line = true;
+            if (c == 2) {
+                const int slot = k == 3 ? 0 : (k == 5 ? 1 : -1);
+                if (slot < 0) return bad("a repeated line outside the reverse diagonal directions");
+                if (corner_line[slot] != INT32_MIN && corner_line[slot] != j)
+                    return bad("two repeated lines in one direction");
+                corner_line[slot] = j;
+            }
+        }
+    }
+    // border cells, and cells counted more than once
+    for (int k = 0; k < kFusedDirs; k++) {
+        const uint16_t* nk = n.data() + k * npx;
+        const int dx = kFdx[k], dy = kFdy[k], s = dx * dy;
+        const int kmin = s > 0 ? -(H - 1) : 0;
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++) {
+                const int v = nk[(size_t)y * W + x];
+                const bool b = border(x, y);
+                int line_cls = 1;
+                if (dy != 0) line_cls = out.image[out.lw_off + (size_t)k * out.nl + (x - s * y - kmin)];
+                if (b && cls(v) != line_cls) {
+                    if (!assign) return bad("a border cell that counts unlike its line");
+                    out.has_border = true;
+                }
+                if (v >= 2) {
+                    const int slot = k == 3 ? 0 : (k == 5 ? 1 : -1);
+                    if (slot < 0 || line_cls != 2) return bad("a repeated cell off the repeated line");
+                    int e = corner[4 * y] < 0 ? 0 : 1;
+                    if (e == 1 && corner[4 * y + 2] >= 0) return bad("more than two repeated cells in a row");
+                    corner[4 * y + 2 * e] = x;
+                    corner[4 * y + 2 * e + 1] = ((v - 1) << 1) | slot;
+                    out.has_corner = true;
+                    out.max_wm1 = std::max(out.max_wm1, v - 1);
+                }
+            }
+    }
+    if (assign) out.has_border = true;  // the horizontal passes' ends always restart
+    return true;
 }
 
 }  // namespace tdv

@@ -104,6 +104,44 @@ struct Timer {
 // Returns false (and schedules nothing usable) if a walk leaves the image.
 bool build_schedule(int W, int H, int table, int paths, PassSchedule& out);
 
+// Walk weights of the fused path (paths.cpp).  The fused kernels walk every
+// path line of each of the 8 directions exactly once, from the image edge it
+// enters.  The reference's sequential loop over its table differs in ways
+// that only change how many times a direction's path cost L_k(p) counts in
+// S(p) = sum_k n_k(p) L_k(p): a stale table walks some reverse diagonals
+// never and one of them many times, and with start-assign semantics
+// (tdvision/semiglobalcpu.cpp:79-83) a walk starting at a border cell wipes
+// what earlier walks added there.  n_k(p) is found by replaying the table's
+// walk order on the host and stored compactly as weight classes:
+//   0 = the cell does not count L_k, 1 = it counts once, 2 = it counts
+//   n >= 2 times (only on the one "corner" line of the reverse diagonal
+//   directions whose table ends are stale).
+// Fused direction order: V+ V- D1+ D1- D2+ D2- H+ H- with (dx, dy) =
+// (0,1) (0,-1) (1,1) (-1,-1) (-1,1) (1,-1) (1,0) (-1,0); D1- and D2- are the
+// corner slots 0 and 1.
+constexpr int kFusedDirs = 8;
+struct FusedWeights {
+    int W = 0, H = 0, table = -1, paths = 0, assign = -1;
+    bool has_line = false;    // some vertical/diagonal line is not all-ones
+    bool has_border = false;  // border cells carry their own classes
+    bool has_corner = false;  // some cell counts a direction more than once
+    int max_wm1 = 0;          // largest n - 1 over the corner cells
+    int nl = 0, nb = 0;       // line slots per direction (W + H - 1), border cells (2W + 2H)
+    // device image: [6][nl] line classes of the vertical/diagonal passes,
+    // [8][nb] border classes, then per row two corner entries (int32 x or -1,
+    // int32 (n-1) << 1 | slot)
+    size_t lw_off = 0, bw_off = 0, corner_off = 0, bytes = 0;
+    std::vector<unsigned char> image;
+};
+// Border cell index: row 0 -> x, row H-1 -> W + x, column 0 -> 2W + y,
+// column W-1 -> 2W + H + y.
+__host__ __device__ inline int border_index(int W, int H, int x, int y) {
+    return y == 0 ? x : (y == H - 1 ? W + x : (x == 0 ? 2 * W + y : 2 * W + H + y));
+}
+// Returns false (with a reason) when the table's weights do not fit this
+// model; the caller then takes the general path.
+bool build_fused_weights(int W, int H, int table, int paths, bool assign, FusedWeights& out, const char** why);
+
 }  // namespace tdv
 
 struct tdv_ctx {
