@@ -31,10 +31,22 @@ _u16p = ctypes.POINTER(ctypes.c_uint16)
 _i32p = ctypes.POINTER(ctypes.c_int32)
 
 
+# where the reference tree lies on the machine that builds oracle/_ref
+REFERENCE_TREE = os.environ.get("TDV_REFERENCE_TREE", "/root/reference")
+
+
 def build(force=False):
     """Compile liborc.so with the recipe in oracle/Makefile (make rebuilds it
     when tdv_oracle.cpp is newer)."""
     subprocess.check_call(["make", "-s", "-C", _HERE] + (["-B"] if force else []))
+
+
+def build_ref():
+    """Compile the reference's own CPU aggregation (semiglobalcpu.cpp,
+    wtacpu.cpp, semiglobal.cu from the reference tree) into
+    _ref/libtdvref.so, the code the oracle is checked against
+    (tests/test_oracle_ref.py)."""
+    subprocess.check_call(["make", "-s", "-C", _HERE, "ref", "REF=" + REFERENCE_TREE])
 
 
 def lib():
