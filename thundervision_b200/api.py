@@ -311,6 +311,19 @@ class Context:
                                          _stream()))
         return verts, cols
 
+    def kernel_times(self, fn):
+        """Runs fn() with per-kernel timing on (tdv_ctx_enable_timing) and
+        returns [(kernel name, device ms)] of the last ABI call fn made."""
+        self.check(L.lib().tdv_ctx_enable_timing(self.handle, 1))
+        try:
+            fn()
+            torch.cuda.synchronize()
+            buf = (ctypes.c_float * 256)()
+            n = L.lib().tdv_ctx_timings(self.handle, buf, 256)
+            return [(L.lib().tdv_ctx_timing_name(self.handle, i).decode(), buf[i]) for i in range(n)]
+        finally:
+            L.lib().tdv_ctx_enable_timing(self.handle, 0)
+
     def stereo_sgm(self, left, right, max_disp, p1, p2, paths=8, p2_mode="const", table="full",
                    semantics="standard", scale=1.0, lr=None, norm=False, right_disp=False):
         """BT + SGM + WTA with the cost recomputed inside the aggregation."""

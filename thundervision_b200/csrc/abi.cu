@@ -280,6 +280,72 @@ tdv_status check_soft(tdv_ctx* ctx, const tdv_volume* cost, const tdv_soft_param
 
 bool is_half_multiple(float v) { return v >= 0.0f && v <= 4096.0f && std::floor(2.0f * v) == 2.0f * v; }
 
+// How an integer-domain call runs on the fused 16-bit path, if it can.
+struct FusedPlan {
+    bool ok = false;
+    int p1h = 0, p2h = 0, off_h = 0, excl = 0;
+    bool weighted = false, assign = false;
+};
+
+// The fused path holds every quantity of the integer domain (u8 images used
+// unscaled, constant P2, penalties multiples of 1/2) exactly in 16-bit
+// half-units: the STANDARD and the reference CPU recurrence, either table.
+// Ranges (half-units, see fused_body.cuh): with the reference CPU recurrence
+// path costs reach down to -OFF, OFF = 510 + max(P1h, P2h - P1h); the
+// sentinel is BIG = OFF + 511 + 2 P2h and an invalid cell's sum over 8 paths,
+// 8 (BIG + P2h + OFF), must fit 16 bits.
+FusedPlan plan_fused(const tdv_image* left, const tdv_image* right, int D, const tdv_sgm_params* p) {
+    FusedPlan f;
+    if (left->dtype != TDV_U8 || right->dtype != TDV_U8 || left->scale != 1.0f || right->scale != 1.0f) return f;
+    if (p->p2_mode != TDV_P2_CONST || !is_half_multiple(p->p1) || !is_half_multiple(p->p2)) return f;
+    if (p->semantics != TDV_SEM_STANDARD && p->semantics != TDV_SEM_REF_CPU) return f;
+    f.p1h = (int)(2.0f * p->p1);
+    f.p2h = (int)(2.0f * p->p2);
+    if (p->semantics == TDV_SEM_REF_CPU) {
+        if (D < 2) return f;  // its minimum over d < D-1 is then empty
+        f.excl = 1;
+        f.off_h = 510 + std::max(f.p1h, f.p2h - f.p1h);
+        f.assign = true;
+    }
+    const long big = (long)f.off_h + 511 + 2L * f.p2h;
+    if (8 * (big + f.p2h + f.off_h) > 65535) return f;
+    f.weighted = p->table == TDV_TABLE_REF || f.assign;
+    f.ok = true;
+    return f;
+}
+
+// Builds (or reuses) the walk weights of the reference table / recurrence for
+// a W x H pair and uploads them; false if this table's weights, or the
+// 32-bit range of its repeated-line sums, fall outside the fused kernels.
+bool fused_weights_ready(tdv_ctx* ctx, int W, int H, int D, const tdv_sgm_params* p, const FusedPlan& f,
+                         cudaStream_t st, tdv_status* err) {
+    *err = TDV_OK;
+    tdv::FusedWeights& fw = ctx->fweights;
+    if (fw.W != W || fw.H != H || fw.table != p->table || fw.paths != p->paths || fw.assign != (int)f.assign) {
+        const char* why = nullptr;
+        if (!tdv::build_fused_weights(W, H, p->table, p->paths, f.assign, fw, &why)) {
+            fw = tdv::FusedWeights();
+            return false;
+        }
+        if ((*err = ensure(ctx, ctx->fw_buf, fw.bytes)) != TDV_OK) return false;
+        if (cudaMemcpyAsync(ctx->fw_buf.ptr, fw.image.data(), fw.bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+            fw = tdv::FusedWeights();
+            *err = fail(ctx, TDV_ERR_CUDA, "uploading the fused walk weights failed");
+            return false;
+        }
+    }
+    // a repeated line's cells add (n-1) L in 32-bit keys of (sum << 8 | d):
+    // the sums must stay inside +-(2^23 - 1)
+    const long maxl = (long)f.off_h + 510 + f.p2h;
+    const long hi = 8 * (maxl + f.p2h) + (long)fw.max_wm1 * (maxl - f.off_h);
+    const long lo = (long)fw.max_wm1 * f.off_h;
+    if (hi >= (1L << 23) - 1 || lo >= (1L << 23) - 1) return false;
+    if (fw.has_corner &&
+        (*err = ensure(ctx, ctx->fside, (size_t)2 * H * tdv::fused_side_words(D) * sizeof(uint32_t))) != TDV_OK)
+        return false;
+    return true;
+}
+
 }  // namespace
 
 namespace tdv {
@@ -351,7 +417,7 @@ void tdv_ctx_destroy(tdv_ctx* ctx) {
     if (!ctx) return;
     const bool any = ctx->agg.ptr || ctx->cost.ptr || ctx->planes.ptr || ctx->codes.ptr ||
                      ctx->misc.ptr || ctx->sched_buf.ptr || ctx->err.ptr || ctx->soft.ptr ||
-                     ctx->agg2.ptr || ctx->defer.ptr || ctx->side;
+                     ctx->agg2.ptr || ctx->defer.ptr || ctx->side || ctx->fw_buf.ptr || ctx->fside.ptr;
     if (any) {
         DeviceScope ds(ctx->device);
         cudaDeviceSynchronize();
@@ -368,6 +434,8 @@ void tdv_ctx_destroy(tdv_ctx* ctx) {
         release_buf(ctx, ctx->err);
         release_buf(ctx, ctx->soft);
         release_buf(ctx, ctx->defer);
+        release_buf(ctx, ctx->fw_buf);
+        release_buf(ctx, ctx->fside);
     }
     if (!ctx->timer.ev.empty()) {
         DeviceScope ds(ctx->device);
@@ -717,12 +785,14 @@ tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* 
         return fail(ctx, TDV_ERR_INVALID_ARG, "left and right images differ in size");
     const int W = left->width, H = left->height;
     ctx->timer.begin(S(stream));
-    const bool fused = left->dtype == TDV_U8 && right->dtype == TDV_U8 && left->scale == 1.0f &&
-                       right->scale == 1.0f && params->semantics == TDV_SEM_STANDARD &&
-                       params->table == TDV_TABLE_FULL && params->p2_mode == TDV_P2_CONST &&
-                       is_half_multiple(params->p1) && is_half_multiple(params->p2) &&
-                       2.0f * params->p2 <= 2560.0f && W >= 1 && H >= 1;
+    const FusedPlan fp = plan_fused(left, right, D, params);
+    bool fused = fp.ok;
     TDV_DEVICE_SCOPE(ctx);
+    if (fused && fp.weighted) {
+        tdv_status werr;
+        fused = fused_weights_ready(ctx, W, H, D, params, fp, S(stream), &werr);
+        TDV_TRY(werr);
+    }
     if (fused) {
         TDV_TRY(reserve_fused(ctx, W, H, D));
         TDV_TRY(ensure_side(ctx));
@@ -732,8 +802,15 @@ tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* 
         a.W = W;
         a.H = H;
         a.D = D;
-        a.p1h = (int)(2.0f * params->p1);
-        a.p2h = (int)(2.0f * params->p2);
+        a.p1h = fp.p1h;
+        a.p2h = fp.p2h;
+        a.excl = fp.excl;
+        a.off_h = fp.off_h;
+        if (fp.weighted) {
+            a.fw = &ctx->fweights;
+            a.weights = (const unsigned char*)ctx->fw_buf.ptr;
+            a.side = (uint32_t*)ctx->fside.ptr;
+        }
         a.paths = params->paths;
         a.disp = out->disp;
         a.disp_norm = out->disp_norm;
@@ -744,7 +821,7 @@ tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* 
         TDV_TRY(ensure_err(ctx, S(stream)));
         a.err = (int*)ctx->err.ptr;
         a.agg2 = ctx->agg2.ptr;
-        a.side = ctx->side;
+        a.side_stream = ctx->side;
         a.fork = ctx->fork_ev;
         a.join = ctx->join_ev;
         TDV_CUDA(tdv::launch_fused(a, S(stream), &ctx->timer));

@@ -1,6 +1,7 @@
 // Fused Birchfield-Tomasi + SGM + WTA (+ left-right check) for integer-domain
 // inputs: u8 intensities used unscaled, P1/P2 multiples of 1/2, constant P2,
-// STANDARD recurrence over the FULL path table, D <= 256.
+// D <= 256; the STANDARD recurrence over the FULL path table, or the
+// reference's own CPU recurrence and path table (see "Reference semantics").
 //
 // Exactness.  In this domain every BT cost is a multiple of 1/2 in [0, 255]
 // and every path cost L = C + min(...) - m' lies in [0, 255 + P2], so all
@@ -38,6 +39,23 @@
 //   records TDV_ERR_TIMEOUT, waits (bounded) for its copies in flight and
 //   returns.
 //
+// Reference semantics.  tdvision/semiglobalcpu.cpp:56-126 differs from the
+// STANDARD recurrence in the minimum m' it subtracts, taken over d < D-1
+// only (:95-97), and its sequential walk loop (:210-222) over the stale path
+// table (tdvision/semiglobal.cu:163-166,197-205) with start-assign (:79-83)
+// changes only how many times each direction's path cost counts in a cell:
+// S(p) = sum_k n_k(p) L_k(p).  The kernels walk every line once and weigh
+// each cell's contribution by a class from build_fused_weights: 1 adds L, 0
+// adds nothing, 2 adds L and leaves the line's L in a side row, from which
+// the last pass adds (n-1) L more in 32-bit arithmetic.  Without the D-1
+// term m' can exceed a path cost, so L can go below zero (down to
+// -(255 + max(P1, P2-P1))): every direction adds its values with an offset
+// OFF = 2*(255 + max(P1, P2-P1)) half-units, folded into the recurrence's
+// subtraction of m', and a class-0 cell adds OFF alone, so every cell's S
+// carries 8*OFF and cells stay comparable in the left-right check.  The
+// sentinel becomes BIG = OFF + 511 + 2*P2h.  The last pass's keys are signed
+// (a corrected sum can be negative).
+//
 // This header holds the device code of those passes as __device__ bodies that
 // take their block index and shared-memory base explicitly, so that the
 // per-frame kernels (kernels_fused.cu, one launch per pass) and the
@@ -47,6 +65,7 @@
 
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <cstdint>
 #include <type_traits>
 
@@ -242,6 +261,13 @@ struct FK {
     uint16_t* disp_right;
     int lr_thr;
     int* err;
+    // reference semantics (all zero / null for the STANDARD recurrence over the FULL table)
+    uint32_t OFFOFF;          // per-direction offset, half-units in both halves
+    const uint8_t* lw;        // this pass's line classes (vertical/diagonal), null: all 1
+    const uint8_t* bw;        // this pass's border-cell classes, null: as the line
+    uint32_t* side;           // this pass's repeated-line rows (Dp2 words per row)
+    const int* corner;        // last pass: per row two (x or -1, (n-1) << 1 | slot) entries
+    const uint32_t* side_all; // last pass: the side rows of both slots, slot * H * Dp2
 };
 
 // ---------------------------------------------------------------- compute
@@ -300,21 +326,35 @@ __device__ __forceinline__ uint32_t mask_pair(uint32_t v, int d, int lim, uint32
     return v;
 }
 
-template <int PPL>
-__device__ __forceinline__ uint32_t warp_min_pairs(const uint32_t* L) {
-    uint32_t t = L[0];
+// Minimum over the warp's disparities; with EXCL the half that holds D-1 is
+// left out (exm[q]: 0xFFFF in that half of that lane's pair q, else 0).
+template <int PPL, bool EXCL>
+__device__ __forceinline__ uint32_t warp_min_pairs(const uint32_t* L, const uint32_t* exm) {
+    uint32_t t = EXCL ? (L[0] | exm[0]) : L[0];
     #pragma unroll
-    for (int q = 1; q < PPL; q++) t = vmin2(t, L[q]);
+    for (int q = 1; q < PPL; q++) t = vmin2(t, EXCL ? (L[q] | exm[q]) : L[q]);
     t = min(t & 0xFFFFu, t >> 16);
     return __reduce_min_sync(FULL, t);
+}
+// The exclusion mask of lane `lane` (pairs (base_d + 2q, base_d + 2q + 1)).
+template <int PPL>
+__device__ __forceinline__ void excl_mask(int base_d, int D, uint32_t* exm) {
+    #pragma unroll
+    for (int q = 0; q < PPL; q++) {
+        const int d = base_d + 2 * q;
+        exm[q] = d == D - 1 ? 0x0000FFFFu : (d + 1 == D - 1 ? 0xFFFF0000u : 0u);
+    }
 }
 
 // One step of the min-plus recurrence for this lane's pairs.
 template <int PPL>
 __device__ __forceinline__ void recur(const uint32_t* L, uint32_t m, const uint32_t* c, uint32_t* Ln,
                                       int lane, const FK& k) {
+    // L = C + tv - m' + OFF per half: the 32-bit sum is exact modulo 2^32 and
+    // each half's result lies in [0, 65535], so no half borrows from the other
     const uint32_t MM = m * 0x10001u;
     const uint32_t MP2 = MM + k.P2P2;
+    const uint32_t MMO = MM - k.OFFOFF;
     uint32_t up = __shfl_up_sync(FULL, L[PPL - 1], 1);
     uint32_t dn = __shfl_down_sync(FULL, L[0], 1);
     if (lane == 0) up = k.BIGBIG;
@@ -325,7 +365,7 @@ __device__ __forceinline__ void recur(const uint32_t* L, uint32_t m, const uint3
         const uint32_t lp = hi_lo(L[q], q < PPL - 1 ? L[q + 1] : dn);
         uint32_t tv = vmin2(lm, lp) + k.P1P1;
         tv = vmin2(vmin2(tv, L[q]), MP2);
-        Ln[q] = tv + c[q] - MM;
+        Ln[q] = tv + c[q] - MMO;
     }
 }
 
@@ -339,7 +379,7 @@ __device__ __forceinline__ void recur(const uint32_t* L, uint32_t m, const uint3
 // a line is one column, so each lane's right-plane offsets are the same on
 // every row and are computed once; the recurrence starts from L = 0, m = 0
 // (first step L = C, as in the horizontal passes).
-template <int PPL, int MODE, bool DIAG>
+template <int PPL, int MODE, bool DIAG, bool EXCL = false>
 __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, int nlines, int G, int blk,
                                         unsigned char* smem) {
     constexpr int SB = 128 * PPL;
@@ -435,9 +475,13 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
         const bool dmask = k.D < DSPAN;  // some lanes hold disparities >= D
         const unsigned char* lp_slot = slots + offL + warp * 16;
         const unsigned char* sv_slot = slots + warp * SB + lane * PPL * 4;
-        uint32_t L[PPL], m = 0;
+        uint32_t L[PPL], m = 0, exm[PPL];
 #pragma unroll
         for (int q = 0; q < PPL; q++) L[q] = 0;
+        if (EXCL) excl_mask<PPL>(base_d, k.D, exm);
+        // weight class of the line (reference table / recurrence): 0 no walk
+        // takes it, 1 counts once, 2 the repeated line (leaves side rows)
+        const int lcls = k.lw ? (int)k.lw[j0 + warp] : 1;
         // vertical (s = 0): column x = kp on every row, offsets computed once
         const int xs = kf + warp;
         const int lim_s = min(xs + 1, k.D);
@@ -476,6 +520,27 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
         auto row = [&](auto chk, int i, int boff) {
             constexpr bool CHECK = decltype(chk)::value;
             uint32_t c[PPL], Ln[PPL];
+            const int yc = CHECK ? y0 + dy * i : 0;
+            const int xc = CHECK ? xs + s * yc : 0;
+            if (DIAG && CHECK && (xc < 0 || xc >= k.W)) {  // uniform: one line per warp
+                sg += sstep;
+                return;
+            }
+            if (CHECK && lcls == 0) {
+                // no walk of this direction: every cell adds the offset alone
+                uint32_t sv[PPL];
+                if (MODE == 0) {
+#pragma unroll
+                    for (int q = 0; q < PPL; q++) sv[q] = k.OFFOFF;
+                } else {
+                    Vec<PPL>::lds((const uint32_t*)(sv_slot + boff), sv);
+#pragma unroll
+                    for (int q = 0; q < PPL; q++) sv[q] += k.OFFOFF;
+                }
+                Vec<PPL>::st(sg, sv);
+                sg += sstep;
+                return;
+            }
             if (!DIAG) {
                 const uint4 lp = *(const uint4*)(lp_slot + boff);
 #pragma unroll
@@ -487,10 +552,6 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
             } else {
                 const int y = y0 + dy * i;
                 const int x = xs + s * y;
-                if (CHECK && (x < 0 || x >= k.W)) {  // uniform: one line per warp
-                    sg += sstep;
-                    return;
-                }
                 const uint4 lp = *(const uint4*)(lp_slot + boff);
                 const int phase = (kf + s * y - DSPAN + 2) & 7;
                 if constexpr (PPL == 4) {
@@ -512,24 +573,40 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
                     for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
                 }
             }
-            recur<PPL>(L, m, c, Ln, lane, k);  // from L = 0, m = 0 the first step gives L = C
+            recur<PPL>(L, m, c, Ln, lane, k);  // from L = 0, m = 0 the first step gives L = C (+ OFF)
+            uint32_t add[PPL];
+#pragma unroll
+            for (int q = 0; q < PPL; q++) add[q] = Ln[q];
+            if (CHECK) {
+                // a border cell whose sum a later walk restarts counts the offset alone
+                if (k.bw && (yc == 0 || yc == k.H - 1 || xc == 0 || xc == k.W - 1) &&
+                    k.bw[border_index(k.W, k.H, xc, yc)] == 0) {
+#pragma unroll
+                    for (int q = 0; q < PPL; q++) add[q] = k.OFFOFF;
+                }
+                if (lcls == 2) Vec<PPL>::st(k.side + (size_t)yc * k.Dp2 + lane * PPL, Ln);
+            }
             if (MODE == 0) {
-                Vec<PPL>::st(sg, Ln);
+                Vec<PPL>::st(sg, add);
             } else {
                 uint32_t sv[PPL];
                 Vec<PPL>::lds((const uint32_t*)(sv_slot + boff), sv);
 #pragma unroll
-                for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
+                for (int q = 0; q < PPL; q++) sv[q] += add[q];
                 Vec<PPL>::st(sg, sv);
             }
             sg += sstep;
 #pragma unroll
             for (int q = 0; q < PPL; q++) L[q] = Ln[q];
-            m = warp_min_pairs<PPL>(L);
+            m = warp_min_pairs<PPL, EXCL>(L, exm);
         };
 
-        // a vertical line needs masking on every row or on none
-        const bool vcheck = !DIAG && (xs < DSPAN || dmask);
+        // a vertical line needs masking on every row or on none; lines with a
+        // weight class other than 1, and border columns with classes of their
+        // own, take the checked rows throughout
+        const bool vcheck = (!DIAG && (xs < DSPAN || dmask)) || lcls != 1 ||
+                            (k.bw && !DIAG && (xs == 0 || xs == k.W - 1));
+        const int xedge = k.bw ? k.W - 1 : k.W;  // last column a clean row may reach, plus one
         for (int j = 0; j < nslots; j++) {
             const int b = j & (NS - 1);
             if (!__all_sync(FULL, mbar_wait(smem_u32(&full[b]), (uint32_t)(j / NS) & 1u))) {
@@ -539,10 +616,15 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
             const int boff = b * slotBytes;
             const bool full_slot = U * j + U <= nrows;
             bool check = vcheck || !full_slot;
+            if (k.bw) {
+                // border rows carry classes of their own
+                const int ya = y0 + dy * (U * j), yb = ya + dy * (U - 1);
+                check = check || min(ya, yb) <= 0 || max(ya, yb) >= k.H - 1;
+            }
             if (DIAG) {
                 // x = xs + s*y is monotone over the slot's rows: check its ends
                 const int xa = xs + s * (y0 + dy * (U * j)), xb = xa + s * dy * (U - 1);
-                check = check || min(xa, xb) < DSPAN || max(xa, xb) >= k.W || dmask;
+                check = check || min(xa, xb) < DSPAN || max(xa, xb) >= xedge || dmask;
             }
             if (!check) {
 #pragma unroll
@@ -608,7 +690,7 @@ __host__ __device__ inline int hp_smem_bytes(int R, int ppl, bool lr, int W, boo
     return align128(R * hp_bars(two) * 8) + R * hp_warp_bytes(ppl, lr, W, two);
 }
 
-template <int PPL, int MODE, bool TWO>
+template <int PPL, int MODE, bool TWO, bool EXCL = false>
 __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, unsigned char* smem) {
     constexpr int SB = 128 * PPL;
     constexpr int NSL = hp_slots(TWO);   // S slots per row
@@ -720,6 +802,20 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
         const int base_d = lane * 2 * PPL;
         constexpr int NR = CS * kChunk;  // right-plane entries in the chunk ring
         static_assert(8 % NJ == 0, "the window ring must divide the 8-step unroll");
+        uint32_t exm[PPL];
+        if (EXCL) excl_mask<PPL>(base_d, k.D, exm);
+        // reference weights: rows 0 and H-1 and columns 0 and W-1 are border
+        // cells with classes of their own; in the last pass up to two cells of
+        // the row count a repeated line more than once (x, (n-1) << 1 | slot)
+        const bool brow = k.bw && (y == 0 || y == k.H - 1);
+        int cx0 = -1, cc0 = 0, cx1 = -1, cc1 = 0;
+        if (MODE == 2 && k.corner) {
+            const int4 e = *(const int4*)(k.corner + 4 * y);
+            cx0 = e.x;
+            cc0 = e.y;
+            cx1 = e.z;
+            cc1 = e.w;
+        }
 
         // One walk of the row in direction DXP (x increasing) with the
         // left-right chain on or off.  Lane l at column x needs the
@@ -735,7 +831,7 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
             constexpr bool LR = decltype(lrc)::value;
             uint32_t L[PPL], m = 0;
             uint32_t WI[NJ], WN[NJ], WX[NJ];  // window: I, half-sample min, half-sample max
-            uint32_t P[NJ];                   // right-view chain (ring, logical j at (T + j) % NJ)
+            int P[NJ];                        // right-view chain (ring, logical j at (T + j) % NJ)
             uint32_t dpair[PPL];              // (d, d+1) of each pair, u16 halves
 #pragma unroll
             for (int q = 0; q < PPL; q++) {
@@ -745,7 +841,7 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
 #pragma unroll
             for (int j = 0; j < NJ; j++) {
                 WI[j] = WN[j] = WX[j] = 0;
-                P[j] = FULL;
+                P[j] = INT_MAX;
             }
             const bool loader = DXP ? lane == 0 : lane == 31;
             uint32_t* sg = k.S + ((size_t)y * W + (DXP ? 0 : W - 1)) * k.Dp2 + lane * PPL;
@@ -832,8 +928,14 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                 }
                 recur<PPL>(L, m, c, Ln, lane, k);
                 Vec<PPL>::lds((const uint32_t*)(slot + xo * SB) + lane * PPL, sv);
+                if (MASK && k.bw && (brow || x == 0 || x == W - 1) && k.bw[border_index(W, k.H, x, y)] == 0) {
+                    // a border cell a later walk restarts: the offset alone
 #pragma unroll
-                for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
+                    for (int q = 0; q < PPL; q++) sv[q] += k.OFFOFF;
+                } else {
+#pragma unroll
+                    for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
+                }
                 if (TWO) {
                     uint32_t s2[PPL];
                     Vec<PPL>::lds((const uint32_t*)(slot + kHpU * SB + xo * SB) + lane * PPL, s2);
@@ -844,14 +946,42 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                     Vec<PPL>::st(sg, sv);
                 } else {
                     // WTA key (S << 8 | d): lowest S, then lowest d (tdvision/wtacpu.cpp:26-30);
-                    // one byte permute per key from S and the lane's (d, d+1) register
-                    uint32_t key[NJ];
+                    // one byte permute per key from S and the lane's (d, d+1) register.
+                    // Keys are signed: a cell of a repeated line adds (n-1) L more in
+                    // 32 bits (L - OFF may be negative), clamped at 2^23 - 1 so that
+                    // invalid cells stay above every valid one.
+                    int key[NJ];
+                    if (MASK && (x == cx0 || x == cx1)) {
+                        int sl[NJ];
 #pragma unroll
-                    for (int q = 0; q < PPL; q++) {
-                        key[2 * q] = __byte_perm(sv[q], dpair[q], 0x5104);
-                        key[2 * q + 1] = __byte_perm(sv[q], dpair[q], 0x7326);
+                        for (int q = 0; q < PPL; q++) {
+                            sl[2 * q] = (int)(sv[q] & 0xFFFFu);
+                            sl[2 * q + 1] = (int)(sv[q] >> 16);
+                        }
+                        const int off = (int)(k.OFFOFF & 0xFFFFu);
+#pragma unroll
+                        for (int e = 0; e < 2; e++) {
+                            const int cx = e ? cx1 : cx0, cc = e ? cc1 : cc0;
+                            if (x != cx) continue;
+                            const uint32_t* sd = k.side_all + ((size_t)(cc & 1) * k.H + y) * k.Dp2 + lane * PPL;
+                            const int w = cc >> 1;
+#pragma unroll
+                            for (int q = 0; q < PPL; q++) {
+                                const uint32_t u = __ldcg(sd + q);
+                                sl[2 * q] += w * ((int)(u & 0xFFFFu) - off);
+                                sl[2 * q + 1] += w * ((int)(u >> 16) - off);
+                            }
+                        }
+#pragma unroll
+                        for (int j = 0; j < NJ; j++) key[j] = min(sl[j], (1 << 23) - 1) * 256 + base_d + j;
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < PPL; q++) {
+                            key[2 * q] = (int)__byte_perm(sv[q], dpair[q], 0x5104);
+                            key[2 * q + 1] = (int)__byte_perm(sv[q], dpair[q], 0x7326);
+                        }
                     }
-                    uint32_t kmin = key[0];
+                    int kmin = key[0];
 #pragma unroll
                     for (int j = 1; j < NJ; j++) kmin = min(kmin, key[j]);
                     kmin = __reduce_min_sync(FULL, kmin);
@@ -859,8 +989,8 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                         // logical P[j] (right pixel x - base_d - j) at ring position (T + j) % NJ
 #pragma unroll
                         for (int j = 0; j < NJ; j++) P[(T + j) % NJ] = min(P[(T + j) % NJ], key[j]);
-                        uint32_t in = __shfl_down_sync(FULL, P[N], 1);
-                        if (lane == 31) in = FULL;
+                        int in = __shfl_down_sync(FULL, P[N], 1);
+                        if (lane == 31) in = INT_MAX;
                         if (lane == 0) {
                             rowR[x] = (uint16_t)(P[N] & 0xFFu);
                             rowL[x] = (uint16_t)(kmin & 0xFFu);
@@ -876,7 +1006,7 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                 sg += sstep;
 #pragma unroll
                 for (int q = 0; q < PPL; q++) L[q] = Ln[q];
-                m = warp_min_pairs<PPL>(L);
+                m = warp_min_pairs<PPL, EXCL>(L, exm);
             };
 
             // group j at window positions T0 .. T0+3: wait, run, release its slot
@@ -888,7 +1018,9 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                 if (!__all_sync(FULL, good)) return false;
                 const unsigned char* slot = wbase + s * SLOT;
                 const int xlo = group_lo(j), xhi = group_hi(j), n = xhi - xlo + 1;
-                if (n == kHpU && xlo >= DSPAN && k.D >= DSPAN) {
+                const bool special = brow || (k.bw && xhi >= W - 1) || (cx0 >= xlo && cx0 <= xhi) ||
+                                     (cx1 >= xlo && cx1 <= xhi);
+                if (n == kHpU && xlo >= DSPAN && k.D >= DSPAN && !special) {
                     static_for<0, kHpU>([&](auto ic) {
                         constexpr int i = decltype(ic)::value;
                         step(std::integral_constant<int, T0 + i>{}, std::false_type{}, DXP ? xlo + i : xhi - i, slot,

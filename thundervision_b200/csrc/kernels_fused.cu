@@ -31,25 +31,25 @@ struct GroupPairs {
 // producer, so that two blocks (one of each concurrent pass chain) share an SM.
 constexpr int kVdMaxG = 15;
 
-template <int PPL, int MODE, bool DIAG>
+template <int PPL, int MODE, bool DIAG, bool EXCL>
 __global__ void __launch_bounds__((kVdMaxG + 1) * 32, 2)
     vd_pass(FK k, int s, int dy, int kmin, int nlines, int G, GroupPairs gp, int paired) {
     extern __shared__ __align__(128) unsigned char smem[];
     if (!paired) {
-        vd_body<PPL, MODE, DIAG>(k, s, dy, kmin, nlines, G, blockIdx.x, smem);
+        vd_body<PPL, MODE, DIAG, EXCL>(k, s, dy, kmin, nlines, G, blockIdx.x, smem);
         return;
     }
-    vd_body<PPL, MODE, DIAG>(k, s, dy, kmin, nlines, G, gp.first[blockIdx.x], smem);
+    vd_body<PPL, MODE, DIAG, EXCL>(k, s, dy, kmin, nlines, G, gp.first[blockIdx.x], smem);
     const int j2 = gp.second[blockIdx.x];
-    if (j2 >= 0) vd_body<PPL, MODE, DIAG>(k, s, dy, kmin, nlines, G, j2, smem);
+    if (j2 >= 0) vd_body<PPL, MODE, DIAG, EXCL>(k, s, dy, kmin, nlines, G, j2, smem);
 }
 
 constexpr int kHpMaxRows = 16;  // consumer warps per block, horizontal passes
 
-template <int PPL, int MODE, bool TWO>
+template <int PPL, int MODE, bool TWO, bool EXCL>
 __global__ void __launch_bounds__((kHpMaxRows + 1) * 32, 1) hp_pass(FK k, int dx, int R) {
     extern __shared__ __align__(128) unsigned char smem[];
-    hp_body<PPL, MODE, TWO>(k, dx, R, blockIdx.x, smem);
+    hp_body<PPL, MODE, TWO, EXCL>(k, dx, R, blockIdx.x, smem);
 }
 
 // ------------------------------------------------------------- host side
@@ -113,7 +113,7 @@ int pair_count(const GroupPairs& gp) {
     return n;
 }
 
-template <int PPL, int MODE, bool DIAG>
+template <int PPL, int MODE, bool DIAG, bool EXCL>
 cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
     const int s = dx * dy;
     const int nlines = s == 0 ? k.W : k.W + k.H - 1;
@@ -151,15 +151,15 @@ cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
     if (!paired) blocks = (nlines + G - 1) / G;
     const int smem = vd_smem_bytes(G, PPL);
     if (smem > kSmemBudget) return cudaErrorInvalidConfiguration;
-    cudaError_t e = opt_in_smem((const void*)vd_pass<PPL, MODE, DIAG>, smem);
+    cudaError_t e = opt_in_smem((const void*)vd_pass<PPL, MODE, DIAG, EXCL>, smem);
     if (e != cudaSuccess) return e;
-    vd_pass<PPL, MODE, DIAG><<<blocks, (G + 1) * 32, smem, st>>>(k, s, dy, kmin, nlines, G, gp, paired);
+    vd_pass<PPL, MODE, DIAG, EXCL><<<blocks, (G + 1) * 32, smem, st>>>(k, s, dy, kmin, nlines, G, gp, paired);
     return cudaGetLastError();
 }
 
 // rows per block: spread the rows over every SM, at most max_rows (a pass
 // that shares the SMs with a concurrent chain keeps its blocks small)
-template <int PPL, int MODE, bool TWO>
+template <int PPL, int MODE, bool TWO, bool EXCL>
 cudaError_t launch_hp(const FK& k, int dx, int max_rows, cudaStream_t st) {
     const bool lr = MODE == 2 && k.lr_thr >= 0;
     const int nsm = sm_count();
@@ -169,38 +169,56 @@ cudaError_t launch_hp(const FK& k, int dx, int max_rows, cudaStream_t st) {
     while (R > 1 && hp_smem_bytes(R, PPL, lr, k.W, TWO) > kSmemBudget) R--;
     const int smem = hp_smem_bytes(R, PPL, lr, k.W, TWO);
     if (smem > kSmemBudget) return cudaErrorInvalidConfiguration;
-    cudaError_t e = opt_in_smem((const void*)hp_pass<PPL, MODE, TWO>, smem);
+    cudaError_t e = opt_in_smem((const void*)hp_pass<PPL, MODE, TWO, EXCL>, smem);
     if (e != cudaSuccess) return e;
     const int blocks = (k.H + R - 1) / R;
-    hp_pass<PPL, MODE, TWO><<<blocks, (R + 1) * 32, smem, st>>>(k, dx, R);
+    hp_pass<PPL, MODE, TWO, EXCL><<<blocks, (R + 1) * 32, smem, st>>>(k, dx, R);
     return cudaGetLastError();
 }
 
-template <int PPL>
+// The FK of one pass: its direction's weight classes and side rows
+// (fused direction order V+ V- D1+ D1- D2+ D2- H+ H-).
+FK for_dir(const FK& base, const FusedArgs& a, int dir) {
+    FK r = base;
+    const FusedWeights* fw = a.fw;
+    if (!fw || !a.weights) return r;
+    if (fw->has_line && dir < 6) r.lw = a.weights + fw->lw_off + (size_t)dir * fw->nl;
+    if (fw->has_border) r.bw = a.weights + fw->bw_off + (size_t)dir * fw->nb;
+    if (fw->has_corner && (dir == 3 || dir == 5)) r.side = a.side + (size_t)(dir == 3 ? 0 : 1) * a.H * base.Dp2;
+    if (fw->has_corner && dir == 7) {
+        r.corner = (const int*)(a.weights + fw->corner_off);
+        r.side_all = a.side;
+    }
+    return r;
+}
+
+template <int PPL, bool EXCL>
 cudaError_t run_fused(const FK& k, const FusedArgs& a, cudaStream_t st, Timer* tm) {
     cudaError_t e;
     auto mark = [&](const char* n, cudaStream_t s) {
         if (tm) tm->mark_on(n, s);
     };
-    const bool chains = a.paths == 8 && a.agg2 && a.side && a.fork && a.join;
+    const FK kv1 = for_dir(k, a, 0), kv2 = for_dir(k, a, 1), kd1 = for_dir(k, a, 2), kd2 = for_dir(k, a, 3),
+             kd3 = for_dir(k, a, 4), kd4 = for_dir(k, a, 5), kh1 = for_dir(k, a, 6), kh2 = for_dir(k, a, 7);
+    const bool chains = a.paths == 8 && a.agg2 && a.side_stream && a.fork && a.join;
     if (!chains) {
-        if ((e = launch_vd<PPL, 0, false>(k, 0, 1, st)) != cudaSuccess) return e;
+        if ((e = launch_vd<PPL, 0, false, EXCL>(kv1, 0, 1, st)) != cudaSuccess) return e;
         mark("fused_pass_V+", st);
-        if ((e = launch_vd<PPL, 1, false>(k, 0, -1, st)) != cudaSuccess) return e;
+        if ((e = launch_vd<PPL, 1, false, EXCL>(kv2, 0, -1, st)) != cudaSuccess) return e;
         mark("fused_pass_V-", st);
         if (a.paths == 8) {
-            if ((e = launch_vd<PPL, 1, true>(k, 1, 1, st)) != cudaSuccess) return e;
+            if ((e = launch_vd<PPL, 1, true, EXCL>(kd1, 1, 1, st)) != cudaSuccess) return e;
             mark("fused_pass_D1+", st);
-            if ((e = launch_vd<PPL, 1, true>(k, -1, -1, st)) != cudaSuccess) return e;
+            if ((e = launch_vd<PPL, 1, true, EXCL>(kd2, -1, -1, st)) != cudaSuccess) return e;
             mark("fused_pass_D1-", st);
-            if ((e = launch_vd<PPL, 1, true>(k, -1, 1, st)) != cudaSuccess) return e;
+            if ((e = launch_vd<PPL, 1, true, EXCL>(kd3, -1, 1, st)) != cudaSuccess) return e;
             mark("fused_pass_D2+", st);
-            if ((e = launch_vd<PPL, 1, true>(k, 1, -1, st)) != cudaSuccess) return e;
+            if ((e = launch_vd<PPL, 1, true, EXCL>(kd4, 1, -1, st)) != cudaSuccess) return e;
             mark("fused_pass_D2-", st);
         }
-        if ((e = launch_hp<PPL, 1, false>(k, 1, kMaxG, st)) != cudaSuccess) return e;
+        if ((e = launch_hp<PPL, 1, false, EXCL>(kh1, 1, kMaxG, st)) != cudaSuccess) return e;
         mark("fused_pass_H+", st);
-        if ((e = launch_hp<PPL, 2, false>(k, -1, kMaxG, st)) != cudaSuccess) return e;
+        if ((e = launch_hp<PPL, 2, false, EXCL>(kh2, -1, kMaxG, st)) != cudaSuccess) return e;
         mark("fused_pass_H-_wta", st);
         return cudaSuccess;
     }
@@ -211,36 +229,36 @@ cudaError_t run_fused(const FK& k, const FusedArgs& a, cudaStream_t st, Timer* t
     // call's stream (same kernels, same volumes) so that each kernel's
     // events time it alone.
     const bool concurrent = !(tm && tm->on);
-    cudaStream_t sd = concurrent ? a.side : st;
-    FK kb = k;
-    kb.S = (uint32_t*)a.agg2;
+    cudaStream_t sd = concurrent ? a.side_stream : st;
+    FK kb2 = kd2, kb3 = kd3, kb4 = kd4;
+    kb2.S = kb3.S = kb4.S = (uint32_t*)a.agg2;
     if (concurrent) {
         if ((e = cudaEventRecord(a.fork, st)) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(sd, a.fork, 0)) != cudaSuccess) return e;
         if (tm) tm->fork(sd);
     }
-    if ((e = launch_vd<PPL, 0, true>(kb, -1, -1, sd)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 0, true, EXCL>(kb2, -1, -1, sd)) != cudaSuccess) return e;
     mark("fused_pass_D1-", sd);
-    if ((e = launch_vd<PPL, 0, false>(k, 0, 1, st)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 0, false, EXCL>(kv1, 0, 1, st)) != cudaSuccess) return e;
     mark("fused_pass_V+", st);
-    if ((e = launch_vd<PPL, 1, true>(kb, -1, 1, sd)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 1, true, EXCL>(kb3, -1, 1, sd)) != cudaSuccess) return e;
     mark("fused_pass_D2+", sd);
-    if ((e = launch_vd<PPL, 1, false>(k, 0, -1, st)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 1, false, EXCL>(kv2, 0, -1, st)) != cudaSuccess) return e;
     mark("fused_pass_V-", st);
-    if ((e = launch_vd<PPL, 1, true>(kb, 1, -1, sd)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 1, true, EXCL>(kb4, 1, -1, sd)) != cudaSuccess) return e;
     mark("fused_pass_D2-", sd);
-    if ((e = launch_vd<PPL, 1, true>(k, 1, 1, st)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 1, true, EXCL>(kd1, 1, 1, st)) != cudaSuccess) return e;
     mark("fused_pass_D1+", st);
     if (concurrent) {
         if ((e = cudaEventRecord(a.join, sd)) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(st, a.join, 0)) != cudaSuccess) return e;
         if (tm) tm->join();
     }
-    FK kj = k;
+    FK kj = kh1;
     kj.S2 = (const uint32_t*)a.agg2;
-    if ((e = launch_hp<PPL, 1, true>(kj, 1, kMaxG, st)) != cudaSuccess) return e;
+    if ((e = launch_hp<PPL, 1, true, EXCL>(kj, 1, kMaxG, st)) != cudaSuccess) return e;
     mark("fused_pass_H+", st);
-    if ((e = launch_hp<PPL, 2, false>(k, -1, kMaxG, st)) != cudaSuccess) return e;
+    if ((e = launch_hp<PPL, 2, false, EXCL>(kh2, -1, kMaxG, st)) != cudaSuccess) return e;
     mark("fused_pass_H-_wta", st);
     return cudaSuccess;
 }
@@ -274,19 +292,30 @@ cudaError_t launch_fused(const FusedArgs& a, cudaStream_t st, Timer* tm) {
     k.Wp = Wp;
     const int ppl = ppl_for(a.D);
     k.Dp2 = 32 * ppl;
-    const uint32_t big = 511u + 2u * (uint32_t)a.p2h;
+    const uint32_t big = (uint32_t)a.off_h + 511u + 2u * (uint32_t)a.p2h;
     k.P1P1 = (uint32_t)a.p1h * 0x10001u;
     k.P2P2 = (uint32_t)a.p2h * 0x10001u;
     k.BIGBIG = big * 0x10001u;
+    k.OFFOFF = (uint32_t)a.off_h * 0x10001u;
+    k.lw = nullptr;
+    k.bw = nullptr;
+    k.side = nullptr;
+    k.corner = nullptr;
+    k.side_all = nullptr;
     k.disp = a.disp;
     k.disp_norm = a.disp_norm;
     k.disp_right = a.disp_right;
     k.lr_thr = a.lr_thr;
     k.err = a.err;
     k.S2 = nullptr;
-    if (ppl == 1) return run_fused<1>(k, a, st, tm);
-    if (ppl == 2) return run_fused<2>(k, a, st, tm);
-    return run_fused<4>(k, a, st, tm);
+    if (a.excl) {
+        if (ppl == 1) return run_fused<1, true>(k, a, st, tm);
+        if (ppl == 2) return run_fused<2, true>(k, a, st, tm);
+        return run_fused<4, true>(k, a, st, tm);
+    }
+    if (ppl == 1) return run_fused<1, false>(k, a, st, tm);
+    if (ppl == 2) return run_fused<2, false>(k, a, st, tm);
+    return run_fused<4, false>(k, a, st, tm);
 }
 
 }  // namespace tdv

@@ -170,6 +170,11 @@ struct tdv_ctx {
 
     tdv::PassSchedule sched;
     Buf sched_buf;
+    // fused path with the reference recurrence / table: walk weights of the
+    // last size seen (host description and device image) and the side rows
+    tdv::FusedWeights fweights;
+    Buf fw_buf;
+    Buf fside;
     tdv::Timer timer;
     // fused path: side stream and fork/join events of the two pass chains
     cudaStream_t side = nullptr;
@@ -253,10 +258,22 @@ struct FusedArgs {
     // call's stream and D1- D2+ D2- into `agg2` on `side`; H+ joins them
     // (agg += agg2 + its L) and H- finishes agg.
     void* agg2 = nullptr;
-    cudaStream_t side = nullptr;
+    cudaStream_t side_stream = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
+    // The reference recurrence and table (see fused_body.cuh): `excl` leaves
+    // d = D-1 out of the minimum, `off_h` is the per-direction offset in
+    // half-units, `weights` the device image of `fw` (null: every cell counts
+    // every direction once), `side` 2 * H * fused_side_words(D) words of
+    // repeated-line rows when fw->has_corner.
+    int excl = 0;
+    int off_h = 0;
+    const unsigned char* weights = nullptr;
+    const FusedWeights* fw = nullptr;
+    uint32_t* side = nullptr;
 };
 size_t fused_agg_bytes(int W, int H, int D);
+// 32-bit words of one repeated-line side row (a pixel's S vector).
+inline size_t fused_side_words(int D) { return (size_t)32 * (D <= 64 ? 1 : (D <= 128 ? 2 : 4)); }
 
 // Image stages either side of the path (kernels_image.cu).
 cudaError_t launch_to_gray(const RasterArg& color, float* gray, cudaStream_t st);
