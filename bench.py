@@ -1,11 +1,16 @@
 #!/usr/bin/env python
 """Throughput of the dense-stereo hot path on the full-HD configuration:
 1920x1080 rectified u8 pair, D = 256, Birchfield-Tomasi cost, 8-path SGM
-(P1 = 10, P2 = 120), WTA + left-right check (threshold 1).
+(P1 = 10, P2 = 120, constant), WTA + left-right check (threshold 1).  By
+default the aggregation is the reference's own: the CPU recurrence of
+tdvision/semiglobalcpu.cpp:56-126 (start-assign, minimum over d < D-1) over
+the reference's path table (tdvision/semiglobal.cu:57-230, stale diagonal
+ends); --semantics standard runs the textbook recurrence over the full table.
 
 One step = one stereo frame through tdv_stereo_sgm.  Prints one JSON line.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--semantics reference|standard] [--cpu-matrix]
 
 Our arm (default): `value` is frames/s with the pair already in HBM, timed
 per step with CUDA events on the launch stream, L2 flushed (256 MiB write)
@@ -18,10 +23,16 @@ and the kernels of the next overlap the kernels of the previous one;
 sequence on one stream.  Under torchrun every rank processes its own frames (weak scaling, no
 collective on the data path); the time is the max over ranks.
 
-Reference arm (--impl reference): the reference's CPU path restated in C++
-(the oracle: BT cost + SemiGlobalCPU with its table and start-assign
-recurrence + WTACPU) on all host threads, each step a band of rows of the
-same frame sized so the run stays within a few minutes; rank 0 only.
+Reference arm (--impl reference): the same computation on the host cores, rank
+0 only: the oracle's restatement of the reference's CPU path (BT, the
+aggregation of the chosen semantics, WTACPU, the left-right check) on all host
+threads, each step a band of rows of the same frame sized so the run stays
+within a few minutes.  The reference's own compiled code (oracle/_ref, built
+from its sources) is timed beside it on the same band: it hard-wires its
+penalties (P1 = 30/255, P2 = 150/255 divided by |dI|,
+tdvision/semiglobalcpu.cpp:36-37,99-102) and runs on one thread as written, so
+it cannot run this configuration itself; the restatement equals it bit for bit
+in its own configuration (tests/test_oracle_ref.py).
 """
 import argparse
 import datetime
@@ -39,6 +50,16 @@ W, H, D = 1920, 1080, 256
 P1, P2, PATHS, LR = 10.0, 120.0, 8, 1
 METRIC = "1080p D=256 8-path SGM fps"
 UNIT = "frames/s"
+# recurrence and path table per --semantics: stereo_sgm keywords, the
+# oracle's constants, and the excluded-minimum flag of the fused kernels
+SEMANTICS = {
+    "reference": {"kw": {"semantics": "ref_cpu", "table": "ref"}, "orc": (1, 1), "excl": 1,
+                  "recurrence": "reference CPU (tdvision/semiglobalcpu.cpp:56-126: start-assign, min over d < D-1)",
+                  "table": "reference (tdvision/semiglobal.cu:57-230, stale diagonal ends)"},
+    "standard": {"kw": {"semantics": "standard", "table": "full"}, "orc": (0, 0), "excl": 0,
+                 "recurrence": "standard (S += C at path starts, min over all d)",
+                 "table": "full (every line walked once each way)"},
+}
 
 
 def parse():
@@ -47,10 +68,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--semantics", choices=sorted(SEMANTICS), default="reference")
     ap.add_argument("--frames", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batch and soft-SGM measurements")
+    ap.add_argument("--cpu-matrix", action="store_true",
+                    help="time the CPU baselines (reference code, restatement on one and on all threads; "
+                         "384x288 D=16, 640x480 D=64, 1080p D=256; 8 and 4 paths), print one JSON line, exit")
     ap.add_argument("--profile-case", choices=["general", "cost1080"],
                     help="general: one launch of each general-path kernel on 1280x720, D=64; cost1080: "
                          "one BT cost DSI at 1920x1080, D=256 (HWD); then exit (the cases the ncu "
@@ -58,14 +83,15 @@ def parse():
     return ap.parse_args()
 
 
-def config(extra=None):
-    c = {"workload": f"BT + SGM-{PATHS} + WTA + LR, {W}x{H}, D={D}", "width": W, "height": H,
-         "max_disp": D, "paths": PATHS, "p1": P1, "p2": P2, "lr_threshold": LR,
-         "l2": "flushed between timed steps (256 MiB write)",
-         "inputs": "seeded synthetic video frames (moving rectangles over a slanted plane)"}
-    if extra:
-        c.update(extra)
-    return c
+def config(sem):
+    """The workload both arms run (identical dicts for one --semantics)."""
+    s = SEMANTICS[sem]
+    return {"workload": f"BT + SGM-{PATHS} + WTA + LR, {W}x{H}, D={D}", "width": W, "height": H,
+            "max_disp": D, "paths": PATHS, "p1": P1, "p2": P2, "p2_mode": "constant",
+            "recurrence": s["recurrence"], "path_table": s["table"],
+            "domain": "u8 intensities used unscaled", "lr_threshold": LR,
+            "l2": "flushed between timed steps (256 MiB write)",
+            "inputs": "seeded synthetic video frames (moving rectangles over a slanted plane)"}
 
 
 # ------------------------------------------------------------------ clocks
@@ -149,58 +175,200 @@ class Clocks:
 
 
 # ------------------------------------------------------------- CPU arms
-def cpu_reference_run(steps, warmup, budget_s=150.0):
-    """Times the oracle's restatement of the reference CPU path on bands of a
-    full-HD frame; returns (frames/s, description, threads)."""
+def _band(h, frame_seed=1000):
+    """Rows 0..h-1 of the first frame rank 0 times, as a W x h pair."""
+    from thundervision_b200 import synthetic
+    L, R = synthetic.VideoStream(seed=frame_seed).frame(0)[:2]
+    return L[:h].copy(), R[:h].copy()
+
+
+def port_run(L, R, sem, threads, paths=PATHS, d=D):
+    """The oracle's restatement of the reference CPU path on a u8 pair: BT
+    cost, SGM of the semantics, WTA, left-right check; (seconds, dl, dr)."""
+    import oracle
+    sm, tb = SEMANTICS[sem]["orc"]
+    t0 = time.perf_counter()
+    Lf, Rf = oracle.u8_to_f32(L), oracle.u8_to_f32(R)
+    C = oracle.bt_cost(Lf, Rf, d)
+    dd, _, S = oracle.sgm(C, Lf, P1, P2, paths=paths, table=tb, semantics=sm, threads=threads)
+    dl, dr = oracle.lr_check(S, dd, thr=LR)
+    return time.perf_counter() - t0, dl, dr
+
+
+def ref_code_lib():
+    """The reference's own CPU aggregation compiled from its sources
+    (oracle/_ref/libtdvref.so), or None where it was not built."""
+    import ctypes
+    path = os.path.join(ROOT, "oracle", "_ref", "libtdvref.so")
+    if not os.path.exists(path):
+        return None
+    lib = ctypes.CDLL(path)
+    f32p = ctypes.POINTER(ctypes.c_float)
+    lib.ref_semiglobal_cpu.argtypes = [f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, f32p, f32p]
+    return lib
+
+
+def ref_code_run(lib, L, R, d=D):
+    """SemiGlobalCPU::updateImpl + WTACPU of the reference (one thread, as
+    written; TBB disabled, tdvision/semiglobalcpu.cpp:191-222) on the BT cost
+    of a u8 pair in the reference's own configuration ([0,1] intensities,
+    P1 = 30/255, P2 = 150/255 divided by |dI|); the cost DSI is computed
+    before the timed call (the reference computes it on the GPU).  Returns
+    (seconds, d/D map)."""
+    import ctypes
+
     import numpy as np
 
     import oracle
-    from thundervision_b200 import synthetic
+    s = np.float32(1) / np.float32(255)
+    Lf, Rf = oracle.u8_to_f32(L, s), oracle.u8_to_f32(R, s)
+    C = np.ascontiguousarray(oracle.bt_cost(Lf, Rf, d, layout=oracle.LAYOUT_REF_WHD))
+    h, w = L.shape
+    dn = np.empty((h, w), np.float32)
+    p = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    t0 = time.perf_counter()
+    lib.ref_semiglobal_cpu(p(C), w, h, d, p(Lf), p(dn))
+    return time.perf_counter() - t0, dn
+
+
+def _rows_for(seconds_per_step, sem, threads, lo=16):
+    """Band height whose restatement run takes about `seconds_per_step`."""
+    L, R = _band(lo)
+    t, _, _ = port_run(L, R, sem, threads)
+    return int(max(lo, min(H, seconds_per_step / (t / lo))))
+
+
+def cpu_reference_run(steps, warmup, sem, budget_s=150.0):
+    """Times the restatement on bands of a full-HD frame on every host thread;
+    returns (frames/s, seconds per step, rows, threads, description)."""
     threads = os.cpu_count() or 1
-    L, R, _, _ = synthetic.VideoStream(seed=0).frame(0)
-    Lf, Rf = oracle.u8_to_f32(L), oracle.u8_to_f32(R)
-
-    def band(h):
-        t0 = time.perf_counter()
-        C = oracle.bt_cost(Lf[:h], Rf[:h], D, layout=oracle.LAYOUT_REF_WHD)
-        oracle.sgm(C, Lf[:h], P1, P2, paths=PATHS, table=oracle.TABLE_REF,
-                   semantics=oracle.SEM_REF_CPU, layout=oracle.LAYOUT_REF_WHD, threads=threads,
-                   want_S=False)
-        return time.perf_counter() - t0
-
-    t_probe = band(32)
-    per_row = t_probe / 32
     total_steps = max(1, steps + warmup)
-    h = int(max(16, min(H, (budget_s / total_steps) / per_row)))
+    h = _rows_for(budget_s / total_steps, sem, threads)
+    L, R = _band(h)
     for _ in range(warmup):
-        band(h)
-    ts = [band(h) for _ in range(steps)]
+        port_run(L, R, sem, threads)
+    ts = [port_run(L, R, sem, threads)[0] for _ in range(steps)]
     t = sum(ts) / len(ts)
-    fps = (h / H) / t
-    desc = (f"rows 0..{h - 1} of a {W}x{H} frame ({h / H:.3f} frame) per step, D={D}, {PATHS} paths,"
-            f" reference CPU semantics (start-assign, stale-end table), {threads} threads;"
-            f" frames/s scaled by rows")
-    return fps, desc, threads
+    desc = (f"rows 0..{h - 1} of a {W}x{H} frame (a {W}x{h} pair, {h / H:.3f} frame) per step, D={D}, "
+            f"{PATHS} paths, BT + {SEMANTICS[sem]['recurrence']} over the {SEMANTICS[sem]['table']} table + "
+            f"WTACPU + left-right check, the oracle's restatement (pinned to the reference's compiled code) "
+            f"on {threads} threads; frames/s scaled by rows")
+    return (h / H) / t, t, h, threads, desc
 
 
-def cpu_baseline_sample(budget_s=20.0):
-    fps, desc, threads = cpu_reference_run(1, 0, budget_s=budget_s)
-    return {"value": fps, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
+def reference_code_sample(rows=48, reps=1):
+    """The reference's compiled SemiGlobalCPU (one thread) on a band, its own
+    configuration; frames/s scaled by rows, or None without oracle/_ref."""
+    lib = ref_code_lib()
+    if lib is None:
+        return None
+    L, R = _band(rows)
+    t = min(ref_code_run(lib, L, R)[0] for _ in range(reps))
+    return {"value": (rows / H) / t, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"rows 0..{rows - 1} of the {W}x{H} frame ({W}x{rows} pair), D={D}, 8 paths: "
+                      "LibThunderVision's SemiGlobalCPU::updateImpl + WTACPU compiled from its sources "
+                      "(oracle/_ref), one thread as written, its compile-time penalties (P1 = 30/255, "
+                      "P2 = 150/255 / |dI|, [0,1] intensities; the same operations per cell as this "
+                      "configuration's constant P2); cost DSI precomputed; frames/s scaled by rows"}
+
+
+def cpu_baseline_sample(sem, budget_s=20.0):
+    fps, t, h, threads, desc = cpu_reference_run(1, 0, sem, budget_s=budget_s)
+    out = {"value": fps, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc,
+           "seconds_per_sample": t}
+    rc = reference_code_sample()
+    if rc is not None:
+        out["reference_code"] = rc
+    return out
+
+
+def band_parity(ctx, dev, sem, rows=64):
+    """Our GPU path against the CPU path on the same band (as its own W x
+    rows pair): the fused kernels vs the restatement for this configuration,
+    and the general float path in the reference's own configuration vs the
+    reference's compiled SemiGlobalCPU (d/D maps), bit for bit."""
+    import numpy as np
+    import torch
+    L, R = _band(rows)
+    threads = os.cpu_count() or 1
+    _, dl, dr = port_run(L, R, sem, threads)
+    out = ctx.stereo_sgm(torch.from_numpy(L).to(dev), torch.from_numpy(R).to(dev), D, P1, P2, paths=PATHS,
+                         lr=LR, right_disp=True, **SEMANTICS[sem]["kw"])
+    res = {"rows": rows, "fused_vs_restatement_bit_exact":
+           bool(np.array_equal(out["disp"].cpu().numpy(), dl) and np.array_equal(out["disp_right"].cpu().numpy(), dr))}
+    lib = ref_code_lib()
+    if lib is not None:
+        _, dn = ref_code_run(lib, L, R)
+        s = float(np.float32(1) / np.float32(255))
+        g = ctx.stereo_sgm(torch.from_numpy(L).to(dev), torch.from_numpy(R).to(dev), D,
+                           float(np.float32(30) / np.float32(255)), float(np.float32(150) / np.float32(255)),
+                           paths=8, p2_mode="adjust", table="ref", semantics="ref_cpu", scale=s, norm=True)
+        res["general_literal_vs_reference_code_bit_exact"] = bool(np.array_equal(g["disp_norm"].cpu().numpy(), dn))
+    return res
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    fps, desc, threads = cpu_reference_run(args.steps, args.warmup)
+    fps, t, h, threads, desc = cpu_reference_run(args.steps, args.warmup, args.semantics)
     line = {"metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 / fps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * t, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "impl": "reference", "config": config(),
-            "cpu_baseline": {"value": fps, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": desc},
+            "impl": "reference", "config": config(args.semantics),
+            "sample_rows": h, "sample_frame_fraction": h / H,
+            "cpu_baseline": {"value": fps, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
             "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    rc = reference_code_sample()
+    if rc is not None:
+        line["reference_code"] = rc
     print(json.dumps(line), flush=True)
+
+
+def cpu_matrix():
+    """CPU baselines on this host: the reference's compiled code (one thread,
+    its own configuration, 8 paths only: its table always holds the diagonals)
+    and the restatement (this configuration) on one and on all threads, 8 and 4
+    paths; 384x288 D=16 and 640x480 D=64 as whole frames, 1080p D=256 as a
+    64-row band scaled by rows; median of 5 after one warm-up."""
+    import numpy as np
+
+    from thundervision_b200 import synthetic
+    threads = os.cpu_count() or 1
+    model = ""
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    lib = ref_code_lib()
+    cases = [("384x288_D16", synthetic.pair_small(1)[:2], 16, 1.0),
+             ("640x480_D64", synthetic.pair_medium(1)[:2], 64, 1.0),
+             ("1920x1080_D256_band64", _band(64), 256, 64 / H)]
+    res = {"host_threads": threads, "cpu_model": model, "repeats": "median of 5 after 1 warm-up",
+           "note": "seconds per frame (band runs scaled by rows); the reference code runs its own penalties "
+                   "(P1 = 30/255, P2 = 150/255 / |dI| on [0,1] intensities), the restatement this configuration "
+                   "(P1 = 10, P2 = 120 constant, 0..255 intensities, reference CPU recurrence and table); "
+                   "the cost DSI is outside the reference code's time (it computes it on the GPU); the "
+                   "reference's toCpuMem (a device-to-host copy per DSI row) has no host-only counterpart and is "
+                   "not timed"}
+
+    def med(fn):
+        fn()
+        return float(np.median([fn() for _ in range(5)]))
+
+    for name, (L, R), d, frac in cases:
+        row = {}
+        if lib is not None:
+            row["reference_code_1thread_8path"] = med(lambda: ref_code_run(lib, L, R, d)[0]) / frac
+        for paths in (8, 4):
+            for th in (1, threads):
+                row[f"restatement_{th}threads_{paths}path"] = med(
+                    lambda: port_run(L, R, "reference", th, paths=paths, d=d)[0]) / frac
+        res[name] = row
+    print(json.dumps({"cpu_matrix": res}), flush=True)
 
 
 # ----------------------------------------------------------- extra metrics
@@ -293,6 +461,31 @@ def measure_batch(ctx, dev, reps=3):
             "per_pair_fused_gcells_per_s": cells / (t_pair / 1000.0) / 1e9,
             "speedup_vs_per_pair_plain": t_plain / t_graph, "speedup_vs_per_pair_fused": t_pair / t_graph,
             "bit_identical_to_per_pair": equal and plain_equal}
+
+
+def measure_batch_sharded(ctx, dev, rank, world, reps=3):
+    """The 64-pair uneven batch split over the ranks (replicas.shard_pairs:
+    largest pairs first, each to the least-loaded rank): every rank runs one
+    graph-replayed persistent batch over its share with autotuned tiles, no
+    collective on the data path; returns this rank's (ms per run, pairs)."""
+    import torch
+
+    from thundervision_b200 import api, replicas, synthetic
+    shapes = synthetic.batch_shapes(seed=0, n=64)
+    pairs = []
+    for i, (w, h, d) in enumerate(shapes):
+        l, r, _, _ = synthetic.pair_sized(w, h, d, synthetic.pair_seed(0, i) % (2 ** 31))
+        pairs.append((l, r, d))
+    idx, mine = replicas.shard_pairs(pairs, rank, world)
+    dev_pairs = [(torch.from_numpy(l).to(dev), torch.from_numpy(r).to(dev), d) for (l, r, d) in mine]
+    b = api.Batch(ctx, dev_pairs, P1, P2, paths=8)
+    try:
+        b.autotune(reps=2)
+        ms = _event_ms(b.graph_launch, reps, 1, torch.cuda.current_stream())
+        b.status()
+    finally:
+        b.close()
+    return ms, len(idx)
 
 
 def measure_soft(ctx, dev, reps=5):
@@ -540,18 +733,96 @@ def measure_video(ctx, dev, n_frames=300, refit_steps=50):
 
 
 # ------------------------------------------------------------------ ours
-# the compiled kernel behind each timed pass (PPL = 4 at D = 256), as ncu names it
-KERNEL_OF = {
-    "fused_prep": "prep_kernel",
-    "fused_pass_V+": "vd_pass<4, 0, 0>",
-    "fused_pass_D1-": "vd_pass<4, 0, 1>",
-    "fused_pass_V-": "vd_pass<4, 1, 0>",
-    "fused_pass_D1+": "vd_pass<4, 1, 1>",
-    "fused_pass_D2+": "vd_pass<4, 1, 1>",
-    "fused_pass_D2-": "vd_pass<4, 1, 1>",
-    "fused_pass_H+": "hp_pass<4, 1, 1>",
-    "fused_pass_H-_wta": "hp_pass<4, 2, 0>",
-}
+def kernel_of(sem):
+    """The compiled kernel behind each timed pass (PPL = 4 at D = 256), as
+    ncu names it; the last template argument is the excluded-minimum flag of
+    the reference CPU recurrence."""
+    e = SEMANTICS[sem]["excl"]
+    return {
+        "fused_prep": "prep_kernel",
+        "fused_pass_V+": f"vd_pass<4, 0, 0, {e}>",
+        "fused_pass_D1-": f"vd_pass<4, 0, 1, {e}>",
+        "fused_pass_V-": f"vd_pass<4, 1, 0, {e}>",
+        "fused_pass_D1+": f"vd_pass<4, 1, 1, {e}>",
+        "fused_pass_D2+": f"vd_pass<4, 1, 1, {e}>",
+        "fused_pass_D2-": f"vd_pass<4, 1, 1, {e}>",
+        "fused_pass_H+": f"hp_pass<4, 1, 1, {e}>",
+        "fused_pass_H-_wta": f"hp_pass<4, 2, 0, {e}>",
+    }
+
+
+def time_frames(ctx, frames, kw, steps, flush, st):
+    """Device ms per frame of tdv_stereo_sgm over device-resident frames, L2
+    flushed before each, and the per-kernel means (events around each kernel,
+    the two pass chains in sequence)."""
+    import ctypes
+
+    import torch
+
+    from thundervision_b200 import _lib
+    lib = _lib.lib()
+
+    def step(i):
+        l, r = frames[i % len(frames)]
+        return ctx.stereo_sgm(l, r, D, P1, P2, paths=PATHS, lr=LR, **kw)
+
+    for i in range(3):
+        step(i)
+    total = 0.0
+    for i in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        step(i)
+        e1.record(st)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    lib.tdv_ctx_enable_timing(ctx.handle, 1)
+    kbuf = (ctypes.c_float * 64)()
+    ksum, kcnt = {}, {}
+    for i in range(steps):
+        flush.zero_()
+        step(i)
+        n = lib.tdv_ctx_timings(ctx.handle, kbuf, 64)
+        for j in range(n):
+            nm = lib.tdv_ctx_timing_name(ctx.handle, j).decode()
+            ksum[nm] = ksum.get(nm, 0.0) + kbuf[j]
+            kcnt[nm] = kcnt.get(nm, 0) + 1
+    torch.cuda.synchronize()
+    lib.tdv_ctx_enable_timing(ctx.handle, 0)
+    return total / steps, {k: ksum[k] / kcnt[k] for k in sorted(ksum)}
+
+
+def measure_reference_literal(ctx, dev, frames, flush, reps=5):
+    """What the reference's own compiled code computes, on the GPU: BT on
+    [0,1] intensities, its CPU recurrence over its path table with P1 =
+    30/255 and P2 = 150/255 divided by |dI|, WTA (the general float path:
+    cost DSI + scheduled passes), 1080p D=256, device ms per frame."""
+    import numpy as np
+    import torch
+    st = torch.cuda.current_stream()
+    s = float(np.float32(1) / np.float32(255))
+    p1, p2 = float(np.float32(30) / np.float32(255)), float(np.float32(150) / np.float32(255))
+
+    def run(i):
+        l, r = frames[i % len(frames)]
+        ctx.stereo_sgm(l, r, D, p1, p2, paths=8, p2_mode="adjust", table="ref", semantics="ref_cpu", scale=s,
+                       norm=True)
+
+    run(0)
+    ts = []
+    for i in range(reps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        run(i)
+        e1.record(st)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ms = sorted(ts)[len(ts) // 2]
+    return {"workload": f"{W}x{H}, D={D}: BT on [0,1] intensities + reference CPU recurrence and path table, "
+                        "P1 = 30/255, P2 = 150/255 / |dI| + WTA, through tdv_stereo_sgm (general float path)",
+            "ms": ms, "fps": 1000.0 / ms}
 
 
 def alg_bytes(name):
@@ -602,9 +873,12 @@ def run_ours(args):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     st = torch.cuda.current_stream()
 
+    SEM = SEMANTICS[args.semantics]["kw"]
+    KERNEL_OF = kernel_of(args.semantics)
+
     def step(i):
         l, r = dev_frames[i % len(dev_frames)]
-        return ctx.stereo_sgm(l, r, D, P1, P2, paths=PATHS, lr=LR)
+        return ctx.stereo_sgm(l, r, D, P1, P2, paths=PATHS, lr=LR, **SEM)
 
     for i in range(args.warmup):
         step(i)
@@ -667,7 +941,7 @@ def run_ours(args):
         dl.copy_(pl, non_blocking=True)
         dr.copy_(pr, non_blocking=True)
         ev[1].record(st)
-        out = ctx.stereo_sgm(dl, dr, D, P1, P2, paths=PATHS, lr=LR)
+        out = ctx.stereo_sgm(dl, dr, D, P1, P2, paths=PATHS, lr=LR, **SEM)
         ev[2].record(st)
         host_out.copy_(out["disp"], non_blocking=True)
         ev[3].record(st)
@@ -684,7 +958,7 @@ def run_ours(args):
     #      double-buffered so that copies overlap the previous frame's kernels,
     #      each frame one CUDA graph replay of the per-frame kernels ----
     from thundervision_b200 import video
-    loop = video.VideoLoop(ctx, W, H, D, P1, P2, paths=PATHS, lr=LR, engine="launches")
+    loop = video.VideoLoop(ctx, W, H, D, P1, P2, paths=PATHS, lr=LR, engine="launches", **SEM)
     stream_in = [pinned[i % len(pinned)] for i in range(args.steps)]
     stream_out = [torch.empty((H, W), dtype=torch.uint16).pin_memory() for _ in range(args.steps)]
     loop.run(stream_in[:min(len(stream_in), args.warmup)], stream_out[:min(len(stream_in), args.warmup)])
@@ -693,10 +967,19 @@ def run_ours(args):
     stream_ms = loop.run(stream_in, stream_out)
     clocks_stream = clk3.stop()
     stream_ok = bool(torch.equal(stream_out[-1], ctx.stereo_sgm(*dev_frames[(args.steps - 1) % len(dev_frames)], D, P1,
-                                                                  P2, paths=PATHS, lr=LR)["disp"].cpu()))
+                                                                  P2, paths=PATHS, lr=LR, **SEM)["disp"].cpu()))
     loop.close()
 
     from thundervision_b200.replicas import max_over_ranks
+    sharded = None
+    if world > 1 and not args.no_extras:
+        # every rank takes part: the batch split over the ranks, time = max over ranks
+        b_ms, b_n = measure_batch_sharded(ctx, dev, rank, world)
+        b_max, b_min = max_over_ranks([b_ms, -b_ms], device=dev)
+        sharded = {"workload": "the 64-pair uneven batch split over the ranks by cell count, one persistent "
+                               "graph-replayed batch per rank, autotuned per rank",
+                   "ranks": world, "pairs_on_rank0": b_n, "ms_max_over_ranks": b_max, "ms_min_over_ranks": -b_min,
+                   "pairs_per_s": 64 / (b_max / 1000.0)}
     total_ms, e2e_ms, stream_ms = max_over_ranks([total_ms, e2e_ms, stream_ms], device=dev)
     if world > 1:
         dist.barrier()
@@ -743,7 +1026,7 @@ def run_ours(args):
         "metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-        "config": config({"parallelism": f"replicas x{world}, frames sharded by rank"}),
+        "config": config(args.semantics), "replicas": f"{world}, frames sharded by rank",
         "gcells_per_s": cells * fps / 1e9,
         "e2e": {"value": stream_fps, "unit": UNIT, "h2d_bytes_per_step": 2 * W * H,
                 "d2h_bytes_per_step": 2 * W * H, "ms_per_step": stream_ms / args.steps,
@@ -760,6 +1043,9 @@ def run_ours(args):
                            "max_ms_per_step": max(e2e_steps), "clocks": clocks_e2e},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch of this kernel "
+                                       "from the ncu capture in profiles/fused_traffic_1080p_d256.json (not "
+                                       "measured in this run)",
                      "alg_bytes_per_launch": dom_bytes, "avg_launch_ms": avg_ms,
                      "share": fsum[dom] / sum(fsum.values()),
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
@@ -776,7 +1062,20 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if sharded is not None:
+        line["batch_sharded"] = sharded
     if not args.no_extras:
+        # the other recurrence / table on the same frames and kernels
+        other = "standard" if args.semantics == "reference" else "reference"
+        try:
+            oms, okern = time_frames(ctx, dev_frames, SEMANTICS[other]["kw"], args.steps, flush, st)
+            line[f"semantics_{other}"] = {"recurrence": SEMANTICS[other]["recurrence"],
+                                          "path_table": SEMANTICS[other]["table"], "ms_per_step": oms,
+                                          "fps": 1000.0 / oms, "kernel_avg_ms": okern,
+                                          "frame_alg_roofline_frac": frame_own / (oms / 1000.0) / 1e9 / peak}
+            line["reference_literal"] = measure_reference_literal(ctx, dev, dev_frames, flush)
+        except Exception as exc:
+            line[f"semantics_{other}"] = {"error": f"{type(exc).__name__}: {exc}"}
         for key, fn in (("batch", measure_batch), ("soft", measure_soft), ("plain", measure_plain),
                         ("image_stages", measure_image), ("reconstruction", measure_reconstruction),
                         ("video", measure_video)):
@@ -785,7 +1084,8 @@ def run_ours(args):
             except Exception as exc:  # an extra never hides the headline line
                 line[key] = {"error": f"{type(exc).__name__}: {exc}"}
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample()
+        line["cpu_baseline"] = cpu_baseline_sample(args.semantics)
+        line["cpu_baseline"]["band_parity"] = band_parity(ctx, dev, args.semantics)
     print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:
@@ -841,6 +1141,9 @@ def main():
         return
     if args.profile_case == "cost1080":
         profile_case_cost1080()
+        return
+    if args.cpu_matrix:
+        cpu_matrix()
         return
     if args.impl == "reference":
         run_reference(args)

@@ -1,7 +1,7 @@
 // Host model of the fused integer-domain path's arithmetic, for the CPU
 // tests: BT costs and path costs in 16-bit half-units, the per-direction
 // offset and sentinel, the reference CPU recurrence's minimum that leaves out
-// d = D-1, the walk weights of tdv::build_fused_weights (paths.cpp), the
+// d = D-1, the reference GPU recurrence's second step from C + P1, the walk weights of tdv::build_fused_weights (paths.cpp), the
 // repeated-line correction and the signed (S << 8 | d) keys of the last pass
 // (WTA, right-view disparity, left-right check).  It walks every line of each
 // direction once, as the kernels do, and checks every 16-bit value the
@@ -70,6 +70,7 @@ int main(int argc, char** argv) {
 
     const bool excl = SEM == TDV_SEM_REF_CPU;   // min over d < D-1
     const bool assign = SEM == TDV_SEM_REF_CPU;  // start cells restart their sums
+    const bool gstart = SEM == TDV_SEM_REF_GPU;  // second step sees C + P1, minimum of C
     tdv::FusedWeights fw;
     const char* why = nullptr;
     const bool weighted = !(TABLE == TDV_TABLE_FULL && !assign);
@@ -99,6 +100,7 @@ int main(int argc, char** argv) {
                 if (weighted && dy != 0) lcls = fw.image[fw.lw_off + (size_t)k * fw.nl + (x0 - s * y0 - kmin)];
                 std::vector<long> L(DSPAN, 0), Ln(DSPAN);
                 long m = 0;
+                bool first = true;
                 for (int x = x0, y = y0; x >= 0 && x < W && y >= 0 && y < H; x += dx, y += dy) {
                     long* sc = &S[((size_t)y * W + x) * DSPAN];
                     if (lcls == 0) {  // a line no walk of this direction takes
@@ -126,6 +128,9 @@ int main(int argc, char** argv) {
                     m = LONG_MAX;
                     for (int d = 0; d < DSPAN; d++)
                         if (!(excl && d == D - 1)) m = std::min(m, L[d]);
+                    if (gstart && first)
+                        for (int d = 0; d < DSPAN; d++) L[d] += P1h;
+                    first = false;
                 }
             }
     }

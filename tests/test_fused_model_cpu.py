@@ -4,8 +4,9 @@ models the 16-bit half-unit recurrence with its offset and sentinel, the walk
 weights built by paths.cpp (build_fused_weights: the stale table's missing and
 repeated reverse diagonals, the start-assign restarts at border cells) and the
 signed keys of the last pass.  Its disparity maps (WTA + left-right check) must
-equal the oracle's for the reference CPU recurrence and the standard one, both
-tables, 4 and 8 paths, landscape / portrait / square shapes and D above W."""
+equal the oracle's for the reference CPU recurrence, the reference GPU one
+(second step from C + P1) and the standard one, both tables, 4 and 8 paths,
+landscape / portrait / square shapes and D above W."""
 import os
 import shutil
 import struct
@@ -58,7 +59,7 @@ SHAPES = [(40, 24, 16, 1), (24, 40, 16, 2), (31, 31, 8, 3), (57, 13, 64, 4), (13
 
 
 @pytest.mark.parametrize("W,H,D,seed", SHAPES)
-@pytest.mark.parametrize("sem", [oracle.SEM_REF_CPU, oracle.SEM_STANDARD])
+@pytest.mark.parametrize("sem", [oracle.SEM_REF_CPU, oracle.SEM_STANDARD, oracle.SEM_REF_GPU])
 @pytest.mark.parametrize("table", [oracle.TABLE_REF, oracle.TABLE_FULL])
 def test_model_equals_oracle(model_exe, tmp_path, W, H, D, seed, sem, table):
     left, right = synthetic.make_pair(W, H, D, seed, n_rects=3)[:2]

@@ -4,6 +4,7 @@ collective on the data path, time = max over ranks), exercised with two
 import os
 import socket
 
+import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
@@ -29,12 +30,23 @@ def test_max_over_ranks_without_a_group():
 
 def _worker(rank, world, port, out_dir):
     import torch.distributed as dist
+
+    from thundervision_b200 import synthetic
+    from thundervision_b200.replicas import shard_pairs
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
     try:
         got = max_over_ranks([10.0 * (rank + 1), 5.0 - rank])
         mine = shard_indices([3, 1, 4, 1, 5, 9, 2, 6], rank, world)
+        # the uneven 64-pair batch: each rank its own share of the pairs
+        # (stand-in image arrays of each pair's shape), loads gathered
+        shapes = synthetic.batch_shapes(seed=0, n=64)
+        pairs = [(np.empty((h, w), np.uint8), np.empty((h, w), np.uint8), d) for (w, h, d) in shapes]
+        idx, share = shard_pairs(pairs, rank, world)
+        load = sum(p[0].size * p[2] for p in share)
+        gathered = [None] * world
+        dist.all_gather_object(gathered, (idx, load))
         with open(os.path.join(out_dir, f"r{rank}.txt"), "w") as f:
-            f.write(repr((got, mine)))
+            f.write(repr((got, mine, gathered)))
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -46,6 +58,11 @@ def test_two_gloo_ranks_reduce_to_the_max(tmp_path):
         port = s.getsockname()[1]
     mp.spawn(_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True)
     res = [eval(open(tmp_path / f"r{r}.txt").read()) for r in range(2)]
-    for got, _ in res:
+    for got, _, _ in res:
         assert got == [20.0, 5.0]
     assert sorted(res[0][1] + res[1][1]) == list(range(8))
+    # both ranks saw the same split of the 64 pairs: disjoint, complete, balanced
+    assert res[0][2] == res[1][2]
+    (i0, l0), (i1, l1) = res[0][2]
+    assert sorted(i0 + i1) == list(range(64)) and not set(i0) & set(i1)
+    assert abs(l0 - l1) <= 1920 * 1080 * 256

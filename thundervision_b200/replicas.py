@@ -26,6 +26,16 @@ def shard_indices(weights, rank, world):
     return sorted(mine)
 
 
+def shard_pairs(pairs, rank, world):
+    """This rank's share of a batch of stereo pairs, each (left, right,
+    max_disp, ...) with (H, W) images: shard_indices over the pairs' cell
+    counts W*H*D.  Returns (indices into `pairs`, those pairs); every rank
+    then runs its own persistent batch (api.Batch) over its share."""
+    weights = [int(p[0].shape[0]) * int(p[0].shape[1]) * int(p[2]) for p in pairs]
+    idx = shard_indices(weights, rank, world)
+    return idx, [pairs[i] for i in idx]
+
+
 def max_over_ranks(values, device="cpu"):
     """Element-wise maximum of per-rank values (e.g. device milliseconds)
     over all ranks of the default process group; the values themselves when

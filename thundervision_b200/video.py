@@ -91,7 +91,10 @@ class VideoLoop:
     CUDA graph per buffer set.  ``engine="persistent"``: each frame is one
     persistent batch launch (tdv_batch_graph_launch, tiles autotuned once).
     ``paths`` 4 or 8; P1/P2 must be multiples of 1/2 (the integer-domain
-    fused path).
+    fused path).  ``semantics`` / ``table`` (launches engine): "standard" /
+    "full", or "ref_cpu" / "ref" for the reference's own CPU recurrence over
+    its path table (tdvision/semiglobalcpu.cpp:173-230), which the fused
+    kernels also run; the persistent engine takes the standard ones only.
 
     ``overlap=True`` (launches engine): each buffer set has its own private
     context (its own aggregation volumes) and its own compute stream, so
@@ -101,8 +104,10 @@ class VideoLoop:
     """
 
     def __init__(self, ctx, W, H, D, p1, p2, paths=8, lr=1, graph=True, autotune=True, device="cuda",
-                 engine="launches", overlap=True):
+                 engine="launches", overlap=True, semantics="standard", table="full"):
         self.ctx, self.graph, self.engine = ctx, graph, engine
+        if engine == "persistent" and (semantics, table) != ("standard", "full"):
+            raise ValueError("the persistent engine runs the standard recurrence over the full table")
         self.bufs = [(torch.empty((H, W), dtype=torch.uint8, device=device),
                       torch.empty((H, W), dtype=torch.uint8, device=device)) for _ in range(2)]
         self.copy_stream = torch.cuda.Stream(device=device)
@@ -129,8 +134,8 @@ class VideoLoop:
                 c.reserve(W, H, D)
             self.ctx = self._own_ctx = self._ctxs[0]
             self.outputs = [torch.empty((H, W), dtype=torch.uint16, device=device) for _ in range(2)]
-            prm = api.L.tdv_sgm_params(float(p1), float(p2), api.L.P2_CONST, paths, api.L.TABLE_FULL,
-                                       api.L.SEM_STANDARD)
+            prm = api.L.tdv_sgm_params(float(p1), float(p2), api.L.P2_CONST, paths, api._TABLES[table],
+                                       api._SEMS[semantics])
             calls = []
             for (l, r), o in zip(self.bufs, self.outputs):
                 calls.append((api._image(l), api._image(r), api.L.tdv_disparity(o.data_ptr(), None, None,
