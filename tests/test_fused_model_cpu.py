@@ -55,7 +55,8 @@ def oracle_maps(left, right, D, p1, p2, paths, table, sem, lr):
 
 
 SHAPES = [(40, 24, 16, 1), (24, 40, 16, 2), (31, 31, 8, 3), (57, 13, 64, 4), (13, 57, 32, 5), (20, 9, 2, 6),
-          (96, 64, 64, 7), (64, 96, 100, 8)]
+          (96, 64, 64, 7), (64, 96, 100, 8), (3, 2, 16, 9), (17, 2, 8, 10), (2, 17, 8, 11), (1, 5, 3, 12),
+          (5, 1, 3, 13), (2, 2, 2, 14), (3, 3, 16, 15)]
 
 
 @pytest.mark.parametrize("W,H,D,seed", SHAPES)

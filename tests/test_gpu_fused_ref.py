@@ -1,7 +1,8 @@
 """The fused 16-bit path computing the reference's own aggregation: the CPU
 recurrence of tdvision/semiglobalcpu.cpp:56-126 (start-assign, minimum over
-d < D-1) over the reference path table of tdvision/semiglobal.cu:57-230 (stale
-diagonal ends), in the integer domain (u8 intensities unscaled, P1/P2
+d < D-1), and its GPU recurrence (tdvision/semiglobal.cu:283-466), over the
+reference path table of tdvision/semiglobal.cu:57-230 (stale diagonal ends),
+in the integer domain (u8 intensities unscaled, P1/P2
 multiples of 1/2, constant P2).  Every map is compared bit-for-bit with the
 oracle's WTA (+ left-right check), and each test asserts that the fused
 kernels ran (not the general float path)."""
@@ -66,7 +67,8 @@ def test_plain_small_config(ctx, orc, paths, lr):
     check(ctx, orc, L, R, 16, 10, 120, paths, lr)
 
 
-@pytest.mark.parametrize("sem,table", [("ref_cpu", "ref"), ("ref_cpu", "full"), ("standard", "ref")])
+@pytest.mark.parametrize("sem,table", [("ref_cpu", "ref"), ("ref_cpu", "full"), ("standard", "ref"),
+                                       ("ref_gpu", "ref"), ("ref_gpu", "full")])
 @pytest.mark.parametrize("paths", [8, 4])
 def test_plain_gpu_config(ctx, orc, sem, table, paths):
     """640x480, D=64, 8 rectangles + slanted plane + 2 % salt-and-pepper,
@@ -85,6 +87,17 @@ def test_shapes(ctx, orc, W, H, D, lr):
     the width, ranges that are not multiples of 64."""
     L, R, _, _ = syn.make_pair(W, H, D, W + 7 * H + D, n_rects=4, slanted=True)
     check(ctx, orc, L, R, D, 10, 120, 8, lr)
+
+
+@pytest.mark.parametrize("W,H,D", [(1001, 37, 200), (37, 200, 64), (101, 61, 48), (640, 96, 256), (3, 2, 16),
+                                   (17, 2, 8), (1, 1, 4)])
+@pytest.mark.parametrize("paths", [8, 4])
+def test_reference_gpu_recurrence(ctx, orc, W, H, D, paths):
+    """The reference's GPU recurrence (tdvision/semiglobal.cu:283-466 without
+    its race: starts accumulate, the second step sees C + P1 with the minimum
+    of C) over its path table, on the fused path."""
+    L, R, _, _ = syn.make_pair(W, H, D, W + 3 * H + D, n_rects=3, slanted=True)
+    check(ctx, orc, L, R, D, 10, 120, paths, 1, sem="ref_gpu", table="ref")
 
 
 @pytest.mark.parametrize("p1,p2", [(30.0, 20.0), (7.5, 300.0), (100.0, 640.0), (0.0, 0.0), (0.5, 1.0)])

@@ -283,13 +283,13 @@ bool is_half_multiple(float v) { return v >= 0.0f && v <= 4096.0f && std::floor(
 // How an integer-domain call runs on the fused 16-bit path, if it can.
 struct FusedPlan {
     bool ok = false;
-    int p1h = 0, p2h = 0, off_h = 0, excl = 0;
+    int p1h = 0, p2h = 0, off_h = 0, excl = 0, gstart = 0;
     bool weighted = false, assign = false;
 };
 
 // The fused path holds every quantity of the integer domain (u8 images used
 // unscaled, constant P2, penalties multiples of 1/2) exactly in 16-bit
-// half-units: the STANDARD and the reference CPU recurrence, either table.
+// half-units: the STANDARD and both reference recurrences, either table.
 // Ranges (half-units, see fused_body.cuh): with the reference CPU recurrence
 // path costs reach down to -OFF, OFF = 510 + max(P1h, P2h - P1h); the
 // sentinel is BIG = OFF + 511 + 2 P2h and an invalid cell's sum over 8 paths,
@@ -298,9 +298,9 @@ FusedPlan plan_fused(const tdv_image* left, const tdv_image* right, int D, const
     FusedPlan f;
     if (left->dtype != TDV_U8 || right->dtype != TDV_U8 || left->scale != 1.0f || right->scale != 1.0f) return f;
     if (p->p2_mode != TDV_P2_CONST || !is_half_multiple(p->p1) || !is_half_multiple(p->p2)) return f;
-    if (p->semantics != TDV_SEM_STANDARD && p->semantics != TDV_SEM_REF_CPU) return f;
     f.p1h = (int)(2.0f * p->p1);
     f.p2h = (int)(2.0f * p->p2);
+    if (p->semantics == TDV_SEM_REF_GPU) f.gstart = f.p1h;
     if (p->semantics == TDV_SEM_REF_CPU) {
         if (D < 2) return f;  // its minimum over d < D-1 is then empty
         f.excl = 1;
@@ -806,6 +806,7 @@ tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* 
         a.p2h = fp.p2h;
         a.excl = fp.excl;
         a.off_h = fp.off_h;
+        a.gstart = fp.gstart;
         if (fp.weighted) {
             a.fw = &ctx->fweights;
             a.weights = (const unsigned char*)ctx->fw_buf.ptr;

@@ -54,7 +54,10 @@
 // subtraction of m', and a class-0 cell adds OFF alone, so every cell's S
 // carries 8*OFF and cells stay comparable in the left-right check.  The
 // sentinel becomes BIG = OFF + 511 + 2*P2h.  The last pass's keys are signed
-// (a corrected sum can be negative).
+// (a corrected sum can be negative).  The reference's GPU recurrence
+// (tdvision/semiglobal.cu:283-466, without its race) accumulates at path
+// starts and differs from STANDARD only in its second step, which sees the
+// first costs plus P1 with the minimum of the first costs (GSTART).
 //
 // This header holds the device code of those passes as __device__ bodies that
 // take their block index and shared-memory base explicitly, so that the
@@ -268,6 +271,8 @@ struct FK {
     uint32_t* side;           // this pass's repeated-line rows (Dp2 words per row)
     const int* corner;        // last pass: per row two (x or -1, (n-1) << 1 | slot) entries
     const uint32_t* side_all; // last pass: the side rows of both slots, slot * H * Dp2
+    uint32_t GSTART;          // reference GPU recurrence: P1 (both halves) added to a line's
+                              // first path costs before its second step (else 0)
 };
 
 // ---------------------------------------------------------------- compute
@@ -326,13 +331,22 @@ __device__ __forceinline__ uint32_t mask_pair(uint32_t v, int d, int lim, uint32
     return v;
 }
 
-// Minimum over the warp's disparities; with EXCL the half that holds D-1 is
-// left out (exm[q]: 0xFFFF in that half of that lane's pair q, else 0).
-template <int PPL, bool EXCL>
-__device__ __forceinline__ uint32_t warp_min_pairs(const uint32_t* L, const uint32_t* exm) {
-    uint32_t t = EXCL ? (L[0] | exm[0]) : L[0];
+// Minimum over the warp's disparities.  EXCL leaves out the half that holds
+// d = D-1 (the reference CPU recurrence): EXCL 1 when D fills the warp's span
+// (D-1 is the high half of lane 31's last pair: one predicated OR, no
+// register), EXCL 2 otherwise (exm[q]: 0xFFFF in that half of that lane's
+// pair q, else 0).
+template <int PPL, int EXCL>
+__device__ __forceinline__ uint32_t warp_min_pairs(const uint32_t* L, const uint32_t* exm, bool last_lane) {
+    auto val = [&](int q) {
+        uint32_t v = L[q];
+        if (EXCL == 1 && q == PPL - 1 && last_lane) v |= 0xFFFF0000u;
+        if (EXCL == 2) v |= exm[q];
+        return v;
+    };
+    uint32_t t = val(0);
     #pragma unroll
-    for (int q = 1; q < PPL; q++) t = vmin2(t, EXCL ? (L[q] | exm[q]) : L[q]);
+    for (int q = 1; q < PPL; q++) t = vmin2(t, val(q));
     t = min(t & 0xFFFFu, t >> 16);
     return __reduce_min_sync(FULL, t);
 }
@@ -379,7 +393,7 @@ __device__ __forceinline__ void recur(const uint32_t* L, uint32_t m, const uint3
 // a line is one column, so each lane's right-plane offsets are the same on
 // every row and are computed once; the recurrence starts from L = 0, m = 0
 // (first step L = C, as in the horizontal passes).
-template <int PPL, int MODE, bool DIAG, bool EXCL = false>
+template <int PPL, int MODE, bool DIAG, int EXCL = 0>
 __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, int nlines, int G, int blk,
                                         unsigned char* smem) {
     constexpr int SB = 128 * PPL;
@@ -478,7 +492,9 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
         uint32_t L[PPL], m = 0, exm[PPL];
 #pragma unroll
         for (int q = 0; q < PPL; q++) L[q] = 0;
-        if (EXCL) excl_mask<PPL>(base_d, k.D, exm);
+        if (EXCL == 2) excl_mask<PPL>(base_d, k.D, exm);
+        const bool last_lane = lane == 31;
+        bool started = false;  // the line's first cell has been walked
         // weight class of the line (reference table / recurrence): 0 no walk
         // takes it, 1 counts once, 2 the repeated line (leaves side rows)
         const int lcls = k.lw ? (int)k.lw[j0 + warp] : 1;
@@ -517,8 +533,11 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
 
         // CHECK: the row may lie outside the line's span (diagonal) or hold
         // cells with d > x or d >= D; without it the row is known clean
-        auto row = [&](auto chk, int i, int boff) {
-            constexpr bool CHECK = decltype(chk)::value;
+        // CHECK: masking and the diagonal span; SPEC (implies CHECK): the
+        // weight classes, the side rows and the first cell of a line
+        auto row = [&](auto chk, auto spc, int i, int boff) {
+            constexpr bool SPEC = decltype(spc)::value;
+            constexpr bool CHECK = decltype(chk)::value || SPEC;
             uint32_t c[PPL], Ln[PPL];
             const int yc = CHECK ? y0 + dy * i : 0;
             const int xc = CHECK ? xs + s * yc : 0;
@@ -526,7 +545,7 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
                 sg += sstep;
                 return;
             }
-            if (CHECK && lcls == 0) {
+            if (SPEC && lcls == 0) {
                 // no walk of this direction: every cell adds the offset alone
                 uint32_t sv[PPL];
                 if (MODE == 0) {
@@ -577,7 +596,7 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
             uint32_t add[PPL];
 #pragma unroll
             for (int q = 0; q < PPL; q++) add[q] = Ln[q];
-            if (CHECK) {
+            if (SPEC) {
                 // a border cell whose sum a later walk restarts counts the offset alone
                 if (k.bw && (yc == 0 || yc == k.H - 1 || xc == 0 || xc == k.W - 1) &&
                     k.bw[border_index(k.W, k.H, xc, yc)] == 0) {
@@ -598,15 +617,31 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
             sg += sstep;
 #pragma unroll
             for (int q = 0; q < PPL; q++) L[q] = Ln[q];
-            m = warp_min_pairs<PPL, EXCL>(L, exm);
+            m = warp_min_pairs<PPL, EXCL>(L, exm, last_lane);
+            if (SPEC && k.GSTART && !started) {
+                // reference GPU recurrence: the second step sees C + P1 with
+                // the minimum of C (tdvision/semiglobal.cu:353-358)
+#pragma unroll
+                for (int q = 0; q < PPL; q++) L[q] += k.GSTART;
+            }
+            if (SPEC) started = true;
         };
 
         // a vertical line needs masking on every row or on none; lines with a
         // weight class other than 1, and border columns with classes of their
-        // own, take the checked rows throughout
-        const bool vcheck = (!DIAG && (xs < DSPAN || dmask)) || lcls != 1 ||
-                            (k.bw && !DIAG && (xs == 0 || xs == k.W - 1));
+        // own, take the special rows throughout
+        const bool vcheck = !DIAG && (xs < DSPAN || dmask);
+        const bool vspec = lcls != 1 || (k.bw && !DIAG && (xs == 0 || xs == k.W - 1));
         const int xedge = k.bw ? k.W - 1 : k.W;  // last column a clean row may reach, plus one
+        // the row of the line's first cell in walk order (the reference GPU
+        // recurrence treats its second step apart)
+        int yfirst = y0;
+        if (DIAG) {
+            const int kp = kf + warp;
+            const int lo = s > 0 ? max(0, -kp) : max(0, kp - (k.W - 1));
+            const int hi = s > 0 ? min(k.H - 1, k.W - 1 - kp) : min(k.H - 1, kp);
+            yfirst = dy > 0 ? lo : hi;
+        }
         for (int j = 0; j < nslots; j++) {
             const int b = j & (NS - 1);
             if (!__all_sync(FULL, mbar_wait(smem_u32(&full[b]), (uint32_t)(j / NS) & 1u))) {
@@ -616,23 +651,28 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
             const int boff = b * slotBytes;
             const bool full_slot = U * j + U <= nrows;
             bool check = vcheck || !full_slot;
-            if (k.bw) {
-                // border rows carry classes of their own
-                const int ya = y0 + dy * (U * j), yb = ya + dy * (U - 1);
-                check = check || min(ya, yb) <= 0 || max(ya, yb) >= k.H - 1;
-            }
+            bool spec = vspec;
+            const int ya = y0 + dy * (U * j), yb = ya + dy * (U - 1);
+            // border rows carry classes of their own; the first cell of a line
+            if (k.bw) spec = spec || min(ya, yb) <= 0 || max(ya, yb) >= k.H - 1;
+            if (k.GSTART) spec = spec || (yfirst >= min(ya, yb) && yfirst <= max(ya, yb));
             if (DIAG) {
                 // x = xs + s*y is monotone over the slot's rows: check its ends
-                const int xa = xs + s * (y0 + dy * (U * j)), xb = xa + s * dy * (U - 1);
-                check = check || min(xa, xb) < DSPAN || max(xa, xb) >= xedge || dmask;
+                const int xa = xs + s * ya, xb = xa + s * dy * (U - 1);
+                check = check || min(xa, xb) < DSPAN || max(xa, xb) >= k.W || dmask;
+                if (k.bw) spec = spec || min(xa, xb) <= 0 || max(xa, xb) >= xedge;
             }
-            if (!check) {
-#pragma unroll
-                for (int r = 0; r < U; r++) row(std::false_type{}, U * j + r, boff + r * rowBytes);
-            } else {
+            if (spec) {
 #pragma unroll
                 for (int r = 0; r < U; r++)
-                    if (U * j + r < nrows) row(std::true_type{}, U * j + r, boff + r * rowBytes);
+                    if (U * j + r < nrows) row(std::true_type{}, std::true_type{}, U * j + r, boff + r * rowBytes);
+            } else if (check) {
+#pragma unroll
+                for (int r = 0; r < U; r++)
+                    if (U * j + r < nrows) row(std::true_type{}, std::false_type{}, U * j + r, boff + r * rowBytes);
+            } else {
+#pragma unroll
+                for (int r = 0; r < U; r++) row(std::false_type{}, std::false_type{}, U * j + r, boff + r * rowBytes);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&empty[b]));
@@ -690,7 +730,7 @@ __host__ __device__ inline int hp_smem_bytes(int R, int ppl, bool lr, int W, boo
     return align128(R * hp_bars(two) * 8) + R * hp_warp_bytes(ppl, lr, W, two);
 }
 
-template <int PPL, int MODE, bool TWO, bool EXCL = false>
+template <int PPL, int MODE, bool TWO, int EXCL = 0>
 __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, unsigned char* smem) {
     constexpr int SB = 128 * PPL;
     constexpr int NSL = hp_slots(TWO);   // S slots per row
@@ -803,7 +843,8 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
         constexpr int NR = CS * kChunk;  // right-plane entries in the chunk ring
         static_assert(8 % NJ == 0, "the window ring must divide the 8-step unroll");
         uint32_t exm[PPL];
-        if (EXCL) excl_mask<PPL>(base_d, k.D, exm);
+        if (EXCL == 2) excl_mask<PPL>(base_d, k.D, exm);
+        const bool last_lane = lane == 31;
         // reference weights: rows 0 and H-1 and columns 0 and W-1 are border
         // cells with classes of their own; in the last pass up to two cells of
         // the row count a repeated line more than once (x, (n-1) << 1 | slot)
@@ -830,6 +871,7 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
             constexpr bool DXP = decltype(dxc)::value;
             constexpr bool LR = decltype(lrc)::value;
             uint32_t L[PPL], m = 0;
+            bool started = false;             // the row's first cell has been walked
             uint32_t WI[NJ], WN[NJ], WX[NJ];  // window: I, half-sample min, half-sample max
             int P[NJ];                        // right-view chain (ring, logical j at (T + j) % NJ)
             uint32_t dpair[PPL];              // (d, d+1) of each pair, u16 halves
@@ -888,10 +930,13 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                 return good;
             };
 
-            // window position T (mod 8); MASK: cells with d > x or d >= D may occur
-            auto step = [&](auto Tc, auto Mc, int x, const unsigned char* slot, int xo) {
+            // window position T (mod 8); MASK: cells with d > x or d >= D may
+            // occur; SPEC (implies MASK): border classes, the repeated-line
+            // correction, the row's first cell
+            auto step = [&](auto Tc, auto Mc, auto Sc, int x, const unsigned char* slot, int xo) {
                 constexpr int T = decltype(Tc)::value;
-                constexpr bool MASK = decltype(Mc)::value;
+                constexpr bool SPEC = decltype(Sc)::value;
+                constexpr bool MASK = decltype(Mc)::value || SPEC;
                 constexpr int N = T % NJ;
                 {
                     uint32_t vi, vn, vx;
@@ -928,7 +973,7 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                 }
                 recur<PPL>(L, m, c, Ln, lane, k);
                 Vec<PPL>::lds((const uint32_t*)(slot + xo * SB) + lane * PPL, sv);
-                if (MASK && k.bw && (brow || x == 0 || x == W - 1) && k.bw[border_index(W, k.H, x, y)] == 0) {
+                if (SPEC && k.bw && (brow || x == 0 || x == W - 1) && k.bw[border_index(W, k.H, x, y)] == 0) {
                     // a border cell a later walk restarts: the offset alone
 #pragma unroll
                     for (int q = 0; q < PPL; q++) sv[q] += k.OFFOFF;
@@ -951,7 +996,7 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                     // 32 bits (L - OFF may be negative), clamped at 2^23 - 1 so that
                     // invalid cells stay above every valid one.
                     int key[NJ];
-                    if (MASK && (x == cx0 || x == cx1)) {
+                    if (SPEC && (x == cx0 || x == cx1)) {
                         int sl[NJ];
 #pragma unroll
                         for (int q = 0; q < PPL; q++) {
@@ -1006,7 +1051,14 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                 sg += sstep;
 #pragma unroll
                 for (int q = 0; q < PPL; q++) L[q] = Ln[q];
-                m = warp_min_pairs<PPL, EXCL>(L, exm);
+                m = warp_min_pairs<PPL, EXCL>(L, exm, last_lane);
+                if (SPEC && k.GSTART && !started) {
+                    // reference GPU recurrence: the second step sees C + P1 with
+                    // the minimum of C (tdvision/semiglobal.cu:353-358)
+#pragma unroll
+                    for (int q = 0; q < PPL; q++) L[q] += k.GSTART;
+                }
+                if (SPEC) started = true;
             };
 
             // group j at window positions T0 .. T0+3: wait, run, release its slot
@@ -1018,20 +1070,27 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                 if (!__all_sync(FULL, good)) return false;
                 const unsigned char* slot = wbase + s * SLOT;
                 const int xlo = group_lo(j), xhi = group_hi(j), n = xhi - xlo + 1;
-                const bool special = brow || (k.bw && xhi >= W - 1) || (cx0 >= xlo && cx0 <= xhi) ||
-                                     (cx1 >= xlo && cx1 <= xhi);
-                if (n == kHpU && xlo >= DSPAN && k.D >= DSPAN && !special) {
+                const bool special = brow || (k.bw && (xlo == 0 || xhi >= W - 1)) || (cx0 >= xlo && cx0 <= xhi) ||
+                                     (cx1 >= xlo && cx1 <= xhi) || (k.GSTART && j == 0);
+                if (special) {
                     static_for<0, kHpU>([&](auto ic) {
                         constexpr int i = decltype(ic)::value;
-                        step(std::integral_constant<int, T0 + i>{}, std::false_type{}, DXP ? xlo + i : xhi - i, slot,
-                             DXP ? i : kHpU - 1 - i);
+                        if (i < n)
+                            step(std::integral_constant<int, T0 + i>{}, std::true_type{}, std::true_type{},
+                                 DXP ? xlo + i : xhi - i, slot, DXP ? i : n - 1 - i);
+                    });
+                } else if (n == kHpU && xlo >= DSPAN && k.D >= DSPAN) {
+                    static_for<0, kHpU>([&](auto ic) {
+                        constexpr int i = decltype(ic)::value;
+                        step(std::integral_constant<int, T0 + i>{}, std::false_type{}, std::false_type{},
+                             DXP ? xlo + i : xhi - i, slot, DXP ? i : kHpU - 1 - i);
                     });
                 } else {
                     static_for<0, kHpU>([&](auto ic) {
                         constexpr int i = decltype(ic)::value;
                         if (i < n)
-                            step(std::integral_constant<int, T0 + i>{}, std::true_type{}, DXP ? xlo + i : xhi - i, slot,
-                                 DXP ? i : n - 1 - i);
+                            step(std::integral_constant<int, T0 + i>{}, std::true_type{}, std::false_type{},
+                                 DXP ? xlo + i : xhi - i, slot, DXP ? i : n - 1 - i);
                     });
                 }
                 __syncwarp();

@@ -31,7 +31,7 @@ struct GroupPairs {
 // producer, so that two blocks (one of each concurrent pass chain) share an SM.
 constexpr int kVdMaxG = 15;
 
-template <int PPL, int MODE, bool DIAG, bool EXCL>
+template <int PPL, int MODE, bool DIAG, int EXCL>
 __global__ void __launch_bounds__((kVdMaxG + 1) * 32, 2)
     vd_pass(FK k, int s, int dy, int kmin, int nlines, int G, GroupPairs gp, int paired) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -45,9 +45,17 @@ __global__ void __launch_bounds__((kVdMaxG + 1) * 32, 2)
 }
 
 constexpr int kHpMaxRows = 16;  // consumer warps per block, horizontal passes
+// Registers per thread of the horizontal passes: 112 keeps the last pass's
+// keys and register window off the stack, and still leaves room on an SM for
+// one vertical/diagonal block (512 threads x 64 registers) beside a
+// horizontal block of up to 9 warps (a full-HD frame's 8 rows per block), so
+// the next frame's passes can overlap this frame's last pass; a block of
+// kHpMaxRows + 1 warps (17 x 32 x 112 registers) still fits an SM.
+constexpr int kHpRegs = 112;
+static_assert((kHpMaxRows + 1) * 32 * kHpRegs <= 65536, "a horizontal block must fit the register file");
 
-template <int PPL, int MODE, bool TWO, bool EXCL>
-__global__ void __launch_bounds__((kHpMaxRows + 1) * 32, 1) hp_pass(FK k, int dx, int R) {
+template <int PPL, int MODE, bool TWO, int EXCL>
+__global__ void __maxnreg__(kHpRegs) hp_pass(FK k, int dx, int R) {
     extern __shared__ __align__(128) unsigned char smem[];
     hp_body<PPL, MODE, TWO, EXCL>(k, dx, R, blockIdx.x, smem);
 }
@@ -113,7 +121,7 @@ int pair_count(const GroupPairs& gp) {
     return n;
 }
 
-template <int PPL, int MODE, bool DIAG, bool EXCL>
+template <int PPL, int MODE, bool DIAG, int EXCL>
 cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
     const int s = dx * dy;
     const int nlines = s == 0 ? k.W : k.W + k.H - 1;
@@ -159,7 +167,7 @@ cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
 
 // rows per block: spread the rows over every SM, at most max_rows (a pass
 // that shares the SMs with a concurrent chain keeps its blocks small)
-template <int PPL, int MODE, bool TWO, bool EXCL>
+template <int PPL, int MODE, bool TWO, int EXCL>
 cudaError_t launch_hp(const FK& k, int dx, int max_rows, cudaStream_t st) {
     const bool lr = MODE == 2 && k.lr_thr >= 0;
     const int nsm = sm_count();
@@ -192,7 +200,7 @@ FK for_dir(const FK& base, const FusedArgs& a, int dir) {
     return r;
 }
 
-template <int PPL, bool EXCL>
+template <int PPL, int EXCL>
 cudaError_t run_fused(const FK& k, const FusedArgs& a, cudaStream_t st, Timer* tm) {
     cudaError_t e;
     auto mark = [&](const char* n, cudaStream_t s) {
@@ -302,20 +310,29 @@ cudaError_t launch_fused(const FusedArgs& a, cudaStream_t st, Timer* tm) {
     k.side = nullptr;
     k.corner = nullptr;
     k.side_all = nullptr;
+    k.GSTART = (uint32_t)a.gstart * 0x10001u;
     k.disp = a.disp;
     k.disp_norm = a.disp_norm;
     k.disp_right = a.disp_right;
     k.lr_thr = a.lr_thr;
     k.err = a.err;
     k.S2 = nullptr;
-    if (a.excl) {
-        if (ppl == 1) return run_fused<1, true>(k, a, st, tm);
-        if (ppl == 2) return run_fused<2, true>(k, a, st, tm);
-        return run_fused<4, true>(k, a, st, tm);
+    // the excluded disparity D-1 is the high half of lane 31's last pair when
+    // D fills the warp's span (EXCL 1), else anywhere (EXCL 2)
+    const int excl = a.excl ? (a.D == 64 * ppl ? 1 : 2) : 0;
+    if (excl == 1) {
+        if (ppl == 1) return run_fused<1, 1>(k, a, st, tm);
+        if (ppl == 2) return run_fused<2, 1>(k, a, st, tm);
+        return run_fused<4, 1>(k, a, st, tm);
     }
-    if (ppl == 1) return run_fused<1, false>(k, a, st, tm);
-    if (ppl == 2) return run_fused<2, false>(k, a, st, tm);
-    return run_fused<4, false>(k, a, st, tm);
+    if (excl == 2) {
+        if (ppl == 1) return run_fused<1, 2>(k, a, st, tm);
+        if (ppl == 2) return run_fused<2, 2>(k, a, st, tm);
+        return run_fused<4, 2>(k, a, st, tm);
+    }
+    if (ppl == 1) return run_fused<1, 0>(k, a, st, tm);
+    if (ppl == 2) return run_fused<2, 0>(k, a, st, tm);
+    return run_fused<4, 0>(k, a, st, tm);
 }
 
 }  // namespace tdv

@@ -231,21 +231,24 @@ bool build_fused_weights(int W, int H, int table, int paths, bool assign, FusedW
                 if (border(x, y)) bw[(size_t)k * out.nb + border_index(W, H, x, y)] = (unsigned char)cls(nk[(size_t)y * W + x]);
         if (!active) continue;
         // line classes: a line is the set of cells x - s*y = kp (vertical and
-        // diagonal) or a row (horizontal); its interior cells share one weight
+        // diagonal) or a row (horizontal).  A line counts in its cells
+        // nowhere (0: no walk of the direction takes it), once (1), or once
+        // plus a correction from its side rows where a cell counts it n >= 2
+        // times (2); border cells may differ (their own classes) under
+        // start-assign semantics
         const int dx = kFdx[k], dy = kFdy[k];
         const int s = dx * dy;
         const bool horiz = dy == 0;
         const int nlines = horiz ? H : (s == 0 ? W : W + H - 1);
         const int kmin = s > 0 ? -(H - 1) : 0;
         for (int j = 0; j < nlines; j++) {
-            int interior = -1, any = 0;
-            bool mixed = false;
+            bool any = false, rep = false, in_zero = false, in_pos = false;
             auto visit = [&](int x, int y) {
                 const int v = nk[(size_t)y * W + x];
-                any |= v;
+                any |= v > 0;
+                rep |= v > 1;
                 if (border(x, y)) return;
-                if (interior < 0) interior = v;
-                else if (interior != v) mixed = true;
+                (v > 0 ? in_pos : in_zero) = true;
             };
             if (horiz) {
                 for (int x = 0; x < W; x++) visit(x, j);
@@ -256,14 +259,12 @@ bool build_fused_weights(int W, int H, int table, int paths, bool assign, FusedW
                     if (x >= 0 && x < W) visit(x, y);
                 }
             }
-            if (mixed) return bad("cells inside one path line count it differently");
-            int c;
-            if (any == 0) c = 0;            // no walk of this direction: skip the line
-            else if (interior == 0) return bad("a walked line counts only at the border");
-            else c = interior < 0 ? 1 : cls(interior);
+            if (in_zero && in_pos) return bad("cells inside one path line count it differently");
+            if (in_zero && any) return bad("a walked line counts only at the border");
+            const int c = rep ? 2 : (any ? 1 : 0);
             if (horiz) {
                 // rows 0 and H-1 are all border cells: their classes decide
-                if (interior >= 0 && c != 1) return bad("a horizontal line that does not count once");
+                if (rep || (in_pos && c != 1)) return bad("a horizontal line that does not count once");
                 continue;
             }
             lw[(size_t)k * out.nl + j] = (unsigned char)c;
@@ -288,7 +289,10 @@ bool build_fused_weights(int W, int H, int table, int paths, bool assign, FusedW
                 const bool b = border(x, y);
                 int line_cls = 1;
                 if (dy != 0) line_cls = out.image[out.lw_off + (size_t)k * out.nl + (x - s * y - kmin)];
-                if (b && cls(v) != line_cls) {
+                // the kernels add L on a counted line (class 1 or 2) and the
+                // offset alone on a class-0 line; a border cell whose count
+                // disagrees takes a class of its own
+                if (b && (v == 0) != (line_cls == 0)) {
                     if (!assign) return bad("a border cell that counts unlike its line");
                     out.has_border = true;
                 }

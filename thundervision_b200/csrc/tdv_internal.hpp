@@ -260,13 +260,15 @@ struct FusedArgs {
     void* agg2 = nullptr;
     cudaStream_t side_stream = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
-    // The reference recurrence and table (see fused_body.cuh): `excl` leaves
-    // d = D-1 out of the minimum, `off_h` is the per-direction offset in
+    // The reference recurrences and table (see fused_body.cuh): `excl` leaves
+    // d = D-1 out of the minimum, `gstart` starts a line the reference GPU
+    // recurrence's way, `off_h` is the per-direction offset in
     // half-units, `weights` the device image of `fw` (null: every cell counts
     // every direction once), `side` 2 * H * fused_side_words(D) words of
     // repeated-line rows when fw->has_corner.
     int excl = 0;
     int off_h = 0;
+    int gstart = 0;  // the reference GPU recurrence: P1 in half-units, else 0
     const unsigned char* weights = nullptr;
     const FusedWeights* fw = nullptr;
     uint32_t* side = nullptr;
