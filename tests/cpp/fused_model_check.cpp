@@ -96,8 +96,10 @@ int main(int argc, char** argv) {
             for (int x0 = 0; x0 < W; x0++) {
                 const int px0 = x0 - dx, py0 = y0 - dy;
                 if (px0 >= 0 && px0 < W && py0 >= 0 && py0 < H) continue;  // not where a line enters
-                int lcls = 1;
-                if (weighted && dy != 0) lcls = fw.image[fw.lw_off + (size_t)k * fw.nl + (x0 - s * y0 - kmin)];
+                int lw = 1;
+                if (weighted) lw = fw.image[fw.lw_off + (size_t)k * fw.nl + (dy == 0 ? y0 : x0 - s * y0 - kmin)];
+                const int lcls = lw & 3;
+                const bool lbw = weighted && fw.has_border && (lw & 4);
                 std::vector<long> L(DSPAN, 0), Ln(DSPAN);
                 long m = 0;
                 bool first = true;
@@ -116,7 +118,7 @@ int main(int argc, char** argv) {
                         check16(Ln[d]);
                     }
                     int cls = lcls;
-                    if (weighted && fw.has_border && border(x, y))
+                    if (lbw && border(x, y))
                         cls = fw.image[fw.bw_off + (size_t)k * fw.nb + tdv::border_index(W, H, x, y)];
                     for (int d = 0; d < DSPAN; d++) {
                         sc[d] += cls == 0 ? OFF : Ln[d];

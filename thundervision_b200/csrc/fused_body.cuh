@@ -266,7 +266,7 @@ struct FK {
     int* err;
     // reference semantics (all zero / null for the STANDARD recurrence over the FULL table)
     uint32_t OFFOFF;          // per-direction offset, half-units in both halves
-    const uint8_t* lw;        // this pass's line classes (vertical/diagonal), null: all 1
+    const uint8_t* lw;        // this pass's line classes (+4: border cells differ), null: all 1
     const uint8_t* bw;        // this pass's border-cell classes, null: as the line
     uint32_t* side;           // this pass's repeated-line rows (Dp2 words per row)
     const int* corner;        // last pass: per row two (x or -1, (n-1) << 1 | slot) entries
@@ -495,9 +495,12 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
         if (EXCL == 2) excl_mask<PPL>(base_d, k.D, exm);
         const bool last_lane = lane == 31;
         bool started = false;  // the line's first cell has been walked
-        // weight class of the line (reference table / recurrence): 0 no walk
-        // takes it, 1 counts once, 2 the repeated line (leaves side rows)
-        const int lcls = k.lw ? (int)k.lw[j0 + warp] : 1;
+        // weight class of the line (reference table / recurrence): 0 counts
+        // nowhere, 1 counts once, 2 the repeated line (leaves side rows); lbw:
+        // some border cells of the line have classes of their own
+        const int lwv = k.lw ? (int)k.lw[j0 + warp] : 1;
+        const int lcls = lwv & 3;
+        const bool lbw = k.bw && (lwv & 4);
         // vertical (s = 0): column x = kp on every row, offsets computed once
         const int xs = kf + warp;
         const int lim_s = min(xs + 1, k.D);
@@ -598,7 +601,7 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
             for (int q = 0; q < PPL; q++) add[q] = Ln[q];
             if (SPEC) {
                 // a border cell whose sum a later walk restarts counts the offset alone
-                if (k.bw && (yc == 0 || yc == k.H - 1 || xc == 0 || xc == k.W - 1) &&
+                if (lbw && (yc == 0 || yc == k.H - 1 || xc == 0 || xc == k.W - 1) &&
                     k.bw[border_index(k.W, k.H, xc, yc)] == 0) {
 #pragma unroll
                     for (int q = 0; q < PPL; q++) add[q] = k.OFFOFF;
@@ -631,8 +634,8 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
         // weight class other than 1, and border columns with classes of their
         // own, take the special rows throughout
         const bool vcheck = !DIAG && (xs < DSPAN || dmask);
-        const bool vspec = lcls != 1 || (k.bw && !DIAG && (xs == 0 || xs == k.W - 1));
-        const int xedge = k.bw ? k.W - 1 : k.W;  // last column a clean row may reach, plus one
+        const bool vspec = lcls != 1 || (lbw && !DIAG && (xs == 0 || xs == k.W - 1));
+        const int xedge = lbw ? k.W - 1 : k.W;  // last column a clean row may reach, plus one
         // the row of the line's first cell in walk order (the reference GPU
         // recurrence treats its second step apart)
         int yfirst = y0;
@@ -654,13 +657,13 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
             bool spec = vspec;
             const int ya = y0 + dy * (U * j), yb = ya + dy * (U - 1);
             // border rows carry classes of their own; the first cell of a line
-            if (k.bw) spec = spec || min(ya, yb) <= 0 || max(ya, yb) >= k.H - 1;
+            if (lbw) spec = spec || min(ya, yb) <= 0 || max(ya, yb) >= k.H - 1;
             if (k.GSTART) spec = spec || (yfirst >= min(ya, yb) && yfirst <= max(ya, yb));
             if (DIAG) {
                 // x = xs + s*y is monotone over the slot's rows: check its ends
                 const int xa = xs + s * ya, xb = xa + s * dy * (U - 1);
                 check = check || min(xa, xb) < DSPAN || max(xa, xb) >= k.W || dmask;
-                if (k.bw) spec = spec || min(xa, xb) <= 0 || max(xa, xb) >= xedge;
+                if (lbw) spec = spec || min(xa, xb) <= 0 || max(xa, xb) >= xedge;
             }
             if (spec) {
 #pragma unroll
@@ -845,10 +848,15 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
         uint32_t exm[PPL];
         if (EXCL == 2) excl_mask<PPL>(base_d, k.D, exm);
         const bool last_lane = lane == 31;
-        // reference weights: rows 0 and H-1 and columns 0 and W-1 are border
-        // cells with classes of their own; in the last pass up to two cells of
-        // the row count a repeated line more than once (x, (n-1) << 1 | slot)
-        const bool brow = k.bw && (y == 0 || y == k.H - 1);
+        // reference weights: the row counts nowhere (rcls 0: every step adds
+        // the offset alone, no recurrence), or once with border cells that
+        // may have classes of their own (rbw); in the last pass up to two
+        // cells of the row count a repeated line more than once
+        // (x, (n-1) << 1 | slot)
+        const int rwv = k.lw ? (int)k.lw[y] : 1;
+        const int rcls = rwv & 3;
+        const bool rbw = k.bw && (rwv & 4);
+        const bool brow = rbw && (y == 0 || y == k.H - 1);
         int cx0 = -1, cc0 = 0, cx1 = -1, cc1 = 0;
         if (MODE == 2 && k.corner) {
             const int4 e = *(const int4*)(k.corner + 4 * y);
@@ -938,7 +946,10 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                 constexpr bool SPEC = decltype(Sc)::value;
                 constexpr bool MASK = decltype(Mc)::value || SPEC;
                 constexpr int N = T % NJ;
-                {
+                // a row that counts nowhere: no right-plane window, cost or recurrence
+                const bool zero = SPEC && rcls == 0;
+                uint32_t c[PPL], Ln[PPL], sv[PPL];
+                if (!zero) {
                     uint32_t vi, vn, vx;
                     if (DXP) {
                         vi = __shfl_up_sync(FULL, WI[N], 1);
@@ -958,22 +969,22 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                     WI[N] = vi;
                     WN[N] = vn;
                     WX[N] = vx;
-                }
-                const uint4 lp = *(const uint4*)(slot + LPOFF + xo * 16);
-                uint32_t c[PPL], Ln[PPL], sv[PPL];
+                    const uint4 lp = *(const uint4*)(slot + LPOFF + xo * 16);
 #pragma unroll
-                for (int q = 0; q < PPL; q++) {
-                    const int w = DXP ? ((T - 2 * q) % NJ + NJ) % NJ : (T + 2 * q + 1) % NJ;
-                    c[q] = bt_pair(lp, make_uint4(WI[w], WN[w], WX[w], 0u));
-                }
-                if (MASK) {
-                    const int lim = min(x + 1, k.D);
+                    for (int q = 0; q < PPL; q++) {
+                        const int w = DXP ? ((T - 2 * q) % NJ + NJ) % NJ : (T + 2 * q + 1) % NJ;
+                        c[q] = bt_pair(lp, make_uint4(WI[w], WN[w], WX[w], 0u));
+                    }
+                    if (MASK) {
+                        const int lim = min(x + 1, k.D);
 #pragma unroll
-                    for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
+                        for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
+                    }
+                    recur<PPL>(L, m, c, Ln, lane, k);
                 }
-                recur<PPL>(L, m, c, Ln, lane, k);
                 Vec<PPL>::lds((const uint32_t*)(slot + xo * SB) + lane * PPL, sv);
-                if (SPEC && k.bw && (brow || x == 0 || x == W - 1) && k.bw[border_index(W, k.H, x, y)] == 0) {
+                if (zero || (SPEC && rbw && (brow || x == 0 || x == W - 1) &&
+                             k.bw[border_index(W, k.H, x, y)] == 0)) {
                     // a border cell a later walk restarts: the offset alone
 #pragma unroll
                     for (int q = 0; q < PPL; q++) sv[q] += k.OFFOFF;
@@ -1049,6 +1060,7 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                     }
                 }
                 sg += sstep;
+                if (zero) return;
 #pragma unroll
                 for (int q = 0; q < PPL; q++) L[q] = Ln[q];
                 m = warp_min_pairs<PPL, EXCL>(L, exm, last_lane);
@@ -1070,8 +1082,8 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                 if (!__all_sync(FULL, good)) return false;
                 const unsigned char* slot = wbase + s * SLOT;
                 const int xlo = group_lo(j), xhi = group_hi(j), n = xhi - xlo + 1;
-                const bool special = brow || (k.bw && (xlo == 0 || xhi >= W - 1)) || (cx0 >= xlo && cx0 <= xhi) ||
-                                     (cx1 >= xlo && cx1 <= xhi) || (k.GSTART && j == 0);
+                const bool special = rcls == 0 || brow || (rbw && (xlo == 0 || xhi >= W - 1)) ||
+                                     (cx0 >= xlo && cx0 <= xhi) || (cx1 >= xlo && cx1 <= xhi) || (k.GSTART && j == 0);
                 if (special) {
                     static_for<0, kHpU>([&](auto ic) {
                         constexpr int i = decltype(ic)::value;

@@ -190,7 +190,7 @@ FK for_dir(const FK& base, const FusedArgs& a, int dir) {
     FK r = base;
     const FusedWeights* fw = a.fw;
     if (!fw || !a.weights) return r;
-    if (fw->has_line && dir < 6) r.lw = a.weights + fw->lw_off + (size_t)dir * fw->nl;
+    if (fw->has_line) r.lw = a.weights + fw->lw_off + (size_t)dir * fw->nl;
     if (fw->has_border) r.bw = a.weights + fw->bw_off + (size_t)dir * fw->nb;
     if (fw->has_corner && (dir == 3 || dir == 5)) r.side = a.side + (size_t)(dir == 3 ? 0 : 1) * a.H * base.Dp2;
     if (fw->has_corner && dir == 7) {

@@ -209,7 +209,7 @@ bool build_fused_weights(int W, int H, int table, int paths, bool assign, FusedW
     out.nl = W + H - 1;
     out.nb = 2 * W + 2 * H;
     out.lw_off = 0;
-    out.bw_off = (size_t)6 * out.nl;
+    out.bw_off = (size_t)kFusedDirs * out.nl;
     out.corner_off = (out.bw_off + (size_t)kFusedDirs * out.nb + 15) & ~(size_t)15;
     out.bytes = out.corner_off + (size_t)H * 16;
     out.image.assign(out.bytes, 0);
@@ -262,11 +262,7 @@ bool build_fused_weights(int W, int H, int table, int paths, bool assign, FusedW
             if (in_zero && in_pos) return bad("cells inside one path line count it differently");
             if (in_zero && any) return bad("a walked line counts only at the border");
             const int c = rep ? 2 : (any ? 1 : 0);
-            if (horiz) {
-                // rows 0 and H-1 are all border cells: their classes decide
-                if (rep || (in_pos && c != 1)) return bad("a horizontal line that does not count once");
-                continue;
-            }
+            if (horiz && rep) return bad("a horizontal line that counts more than once");
             lw[(size_t)k * out.nl + j] = (unsigned char)c;
             if (c != 1) out.has_line = true;
             if (c == 2) {
@@ -287,14 +283,17 @@ bool build_fused_weights(int W, int H, int table, int paths, bool assign, FusedW
             for (int x = 0; x < W; x++) {
                 const int v = nk[(size_t)y * W + x];
                 const bool b = border(x, y);
-                int line_cls = 1;
-                if (dy != 0) line_cls = out.image[out.lw_off + (size_t)k * out.nl + (x - s * y - kmin)];
+                unsigned char& lc = lw[(size_t)k * out.nl + (dy == 0 ? y : x - s * y - kmin)];
+                const int line_cls = lc & 3;
                 // the kernels add L on a counted line (class 1 or 2) and the
                 // offset alone on a class-0 line; a border cell whose count
-                // disagrees takes a class of its own
+                // disagrees takes a class of its own, and its line is flagged
+                // (4) so that only flagged lines look border classes up
                 if (b && (v == 0) != (line_cls == 0)) {
                     if (!assign) return bad("a border cell that counts unlike its line");
                     out.has_border = true;
+                    out.has_line = true;
+                    lc |= 4;
                 }
                 if (v >= 2) {
                     const int slot = k == 3 ? 0 : (k == 5 ? 1 : -1);
@@ -308,7 +307,6 @@ bool build_fused_weights(int W, int H, int table, int paths, bool assign, FusedW
                 }
             }
     }
-    if (assign) out.has_border = true;  // the horizontal passes' ends always restart
     return true;
 }
 

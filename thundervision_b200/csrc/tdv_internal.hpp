@@ -116,20 +116,23 @@ bool build_schedule(int W, int H, int table, int paths, PassSchedule& out);
 //   0 = the cell does not count L_k, 1 = it counts once, 2 = it counts
 //   n >= 2 times (only on the one "corner" line of the reverse diagonal
 //   directions whose table ends are stale).
+// Every line of a direction (a column, a diagonal or a row) has one class for
+// its interior cells; a line whose border cells count otherwise carries the
+// flag 4, and only flagged lines look up their border cells' classes.
 // Fused direction order: V+ V- D1+ D1- D2+ D2- H+ H- with (dx, dy) =
 // (0,1) (0,-1) (1,1) (-1,-1) (-1,1) (1,-1) (1,0) (-1,0); D1- and D2- are the
 // corner slots 0 and 1.
 constexpr int kFusedDirs = 8;
 struct FusedWeights {
     int W = 0, H = 0, table = -1, paths = 0, assign = -1;
-    bool has_line = false;    // some vertical/diagonal line is not all-ones
-    bool has_border = false;  // border cells carry their own classes
+    bool has_line = false;    // some line is not all-ones (or is flagged)
+    bool has_border = false;  // some border cells carry their own classes
     bool has_corner = false;  // some cell counts a direction more than once
     int max_wm1 = 0;          // largest n - 1 over the corner cells
     int nl = 0, nb = 0;       // line slots per direction (W + H - 1), border cells (2W + 2H)
-    // device image: [6][nl] line classes of the vertical/diagonal passes,
-    // [8][nb] border classes, then per row two corner entries (int32 x or -1,
-    // int32 (n-1) << 1 | slot)
+    // device image: [8][nl] line classes (the horizontal directions indexed
+    // by row), [8][nb] border classes, then per row two corner entries
+    // (int32 x or -1, int32 (n-1) << 1 | slot)
     size_t lw_off = 0, bw_off = 0, corner_off = 0, bytes = 0;
     std::vector<unsigned char> image;
 };
