@@ -344,9 +344,11 @@ __device__ __forceinline__ uint32_t warp_min_pairs(const uint32_t* L, const uint
         if (EXCL == 2) v |= exm[q];
         return v;
     };
-    uint32_t t = val(0);
+    // the pair that may hold D-1 first: the recurrence produces it first, so
+    // its mask overlaps the other pairs' work
+    uint32_t t = val(PPL - 1);
     #pragma unroll
-    for (int q = 1; q < PPL; q++) t = vmin2(t, val(q));
+    for (int q = 0; q < PPL - 1; q++) t = vmin2(t, val(q));
     t = min(t & 0xFFFFu, t >> 16);
     return __reduce_min_sync(FULL, t);
 }
@@ -360,21 +362,23 @@ __device__ __forceinline__ void excl_mask(int base_d, int D, uint32_t* exm) {
     }
 }
 
-// One step of the min-plus recurrence for this lane's pairs.
-template <int PPL>
+// One step of the min-plus recurrence for this lane's pairs; OFFSET: the
+// per-direction offset of the reference CPU recurrence may be nonzero.
+template <int PPL, bool OFFSET>
 __device__ __forceinline__ void recur(const uint32_t* L, uint32_t m, const uint32_t* c, uint32_t* Ln,
                                       int lane, const FK& k) {
     // L = C + tv - m' + OFF per half: the 32-bit sum is exact modulo 2^32 and
     // each half's result lies in [0, 65535], so no half borrows from the other
     const uint32_t MM = m * 0x10001u;
     const uint32_t MP2 = MM + k.P2P2;
-    const uint32_t MMO = MM - k.OFFOFF;
+    const uint32_t MMO = OFFSET ? MM - k.OFFOFF : MM;
     uint32_t up = __shfl_up_sync(FULL, L[PPL - 1], 1);
     uint32_t dn = __shfl_down_sync(FULL, L[0], 1);
     if (lane == 0) up = k.BIGBIG;
     if (lane == 31) dn = k.BIGBIG;
     #pragma unroll
-    for (int q = 0; q < PPL; q++) {
+    for (int qq = 0; qq < PPL; qq++) {
+        const int q = PPL - 1 - qq;  // the last pair first (see warp_min_pairs)
         const uint32_t lm = hi_lo(q > 0 ? L[q - 1] : up, L[q]);
         const uint32_t lp = hi_lo(L[q], q < PPL - 1 ? L[q + 1] : dn);
         uint32_t tv = vmin2(lm, lp) + k.P1P1;
@@ -393,9 +397,15 @@ __device__ __forceinline__ void recur(const uint32_t* L, uint32_t m, const uint3
 // a line is one column, so each lane's right-plane offsets are the same on
 // every row and are computed once; the recurrence starts from L = 0, m = 0
 // (first step L = C, as in the horizontal passes).
-template <int PPL, int MODE, bool DIAG, int EXCL = 0>
+// VAR 0: the STANDARD recurrence over the full table (no weight, offset or
+// first-step code is compiled in); 1: weights / reference recurrences, 2: as
+// 1 with the excluded minimum of D-1 at lane 31 (D fills the span), 3: as 1
+// with the excluded minimum anywhere.
+template <int PPL, int MODE, bool DIAG, int VAR = 0>
 __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, int nlines, int G, int blk,
                                         unsigned char* smem) {
+    constexpr bool WTD = VAR != 0;
+    constexpr int EXCL = VAR == 2 ? 1 : (VAR == 3 ? 2 : 0);
     constexpr int SB = 128 * PPL;
     constexpr int DSPAN = 64 * PPL;
     constexpr int U = kVdRowsPerSlot;
@@ -498,9 +508,9 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
         // weight class of the line (reference table / recurrence): 0 counts
         // nowhere, 1 counts once, 2 the repeated line (leaves side rows); lbw:
         // some border cells of the line have classes of their own
-        const int lwv = k.lw ? (int)k.lw[j0 + warp] : 1;
-        const int lcls = lwv & 3;
-        const bool lbw = k.bw && (lwv & 4);
+        const int lwv = (WTD && k.lw) ? (int)k.lw[j0 + warp] : 1;
+        const int lcls = WTD ? (lwv & 3) : 1;
+        const bool lbw = WTD && k.bw && (lwv & 4);
         // vertical (s = 0): column x = kp on every row, offsets computed once
         const int xs = kf + warp;
         const int lim_s = min(xs + 1, k.D);
@@ -536,6 +546,9 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
 
         // CHECK: the row may lie outside the line's span (diagonal) or hold
         // cells with d > x or d >= D; without it the row is known clean
+        // the repeated line's side row of the current walk row
+        uint32_t* sidep = (WTD && DIAG && lcls == 2) ? k.side + (size_t)y0 * k.Dp2 + lane * PPL : nullptr;
+        const long long sidestep = (long long)dy * k.Dp2;
         // CHECK: masking and the diagonal span; SPEC (implies CHECK): the
         // weight classes, the side rows and the first cell of a line
         auto row = [&](auto chk, auto spc, int i, int boff) {
@@ -546,6 +559,7 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
             const int xc = CHECK ? xs + s * yc : 0;
             if (DIAG && CHECK && (xc < 0 || xc >= k.W)) {  // uniform: one line per warp
                 sg += sstep;
+                if constexpr (WTD && DIAG) sidep += sidestep;
                 return;
             }
             if (SPEC && lcls == 0) {
@@ -561,6 +575,7 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
                 }
                 Vec<PPL>::st(sg, sv);
                 sg += sstep;
+                if constexpr (WTD && DIAG) sidep += sidestep;
                 return;
             }
             if (!DIAG) {
@@ -595,7 +610,7 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
                     for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
                 }
             }
-            recur<PPL>(L, m, c, Ln, lane, k);  // from L = 0, m = 0 the first step gives L = C (+ OFF)
+            recur<PPL, WTD>(L, m, c, Ln, lane, k);  // from L = 0, m = 0 the first step gives L = C (+ OFF)
             uint32_t add[PPL];
 #pragma unroll
             for (int q = 0; q < PPL; q++) add[q] = Ln[q];
@@ -606,7 +621,11 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
 #pragma unroll
                     for (int q = 0; q < PPL; q++) add[q] = k.OFFOFF;
                 }
-                if (lcls == 2) Vec<PPL>::st(k.side + (size_t)yc * k.Dp2 + lane * PPL, Ln);
+            }
+            // the repeated line leaves its path costs in the side rows (one
+            // line per warp: a predicated store in every row variant)
+            if constexpr (WTD && DIAG) {
+                if (lcls == 2) Vec<PPL>::st(sidep, Ln);
             }
             if (MODE == 0) {
                 Vec<PPL>::st(sg, add);
@@ -618,6 +637,7 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
                 Vec<PPL>::st(sg, sv);
             }
             sg += sstep;
+            if constexpr (WTD && DIAG) sidep += sidestep;
 #pragma unroll
             for (int q = 0; q < PPL; q++) L[q] = Ln[q];
             m = warp_min_pairs<PPL, EXCL>(L, exm, last_lane);
@@ -630,20 +650,30 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
             if (SPEC) started = true;
         };
 
-        // a vertical line needs masking on every row or on none; lines with a
-        // weight class other than 1, and border columns with classes of their
-        // own, take the special rows throughout
+        // a vertical line needs masking on every row or on none; lines that
+        // count nowhere, and border columns with classes of their own, take
+        // the special rows throughout
         const bool vcheck = !DIAG && (xs < DSPAN || dmask);
-        const bool vspec = lcls != 1 || (lbw && !DIAG && (xs == 0 || xs == k.W - 1));
-        const int xedge = lbw ? k.W - 1 : k.W;  // last column a clean row may reach, plus one
-        // the row of the line's first cell in walk order (the reference GPU
-        // recurrence treats its second step apart)
-        int yfirst = y0;
-        if (DIAG) {
-            const int kp = kf + warp;
-            const int lo = s > 0 ? max(0, -kp) : max(0, kp - (k.W - 1));
-            const int hi = s > 0 ? min(k.H - 1, k.W - 1 - kp) : min(k.H - 1, kp);
-            yfirst = dy > 0 ? lo : hi;
+        const bool vspec = WTD && (lcls == 0 || (lbw && !DIAG && (xs == 0 || xs == k.W - 1)));
+        // the slots that hold the line's first and last cells in walk order:
+        // a line's border cells are its two end cells (besides whole border
+        // columns, above), and the reference GPU recurrence treats the first
+        // cell's successor apart
+        int jsa = -1, jsb = -1;
+        if (WTD && (lbw || k.GSTART)) {
+            int yf = 0, yl = k.H - 1;
+            if (DIAG) {
+                const int kp = kf + warp;
+                yf = s > 0 ? max(0, -kp) : max(0, kp - (k.W - 1));
+                yl = s > 0 ? min(k.H - 1, k.W - 1 - kp) : min(k.H - 1, kp);
+            }
+            if (dy < 0) {
+                const int t = yf;
+                yf = yl;
+                yl = t;
+            }
+            jsa = (yf - y0) * dy / U;
+            jsb = lbw ? (yl - y0) * dy / U : jsa;
         }
         for (int j = 0; j < nslots; j++) {
             const int b = j & (NS - 1);
@@ -654,21 +684,18 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
             const int boff = b * slotBytes;
             const bool full_slot = U * j + U <= nrows;
             bool check = vcheck || !full_slot;
-            bool spec = vspec;
-            const int ya = y0 + dy * (U * j), yb = ya + dy * (U - 1);
-            // border rows carry classes of their own; the first cell of a line
-            if (lbw) spec = spec || min(ya, yb) <= 0 || max(ya, yb) >= k.H - 1;
-            if (k.GSTART) spec = spec || (yfirst >= min(ya, yb) && yfirst <= max(ya, yb));
+            const bool spec = WTD && (vspec || j == jsa || j == jsb);
             if (DIAG) {
                 // x = xs + s*y is monotone over the slot's rows: check its ends
-                const int xa = xs + s * ya, xb = xa + s * dy * (U - 1);
+                const int xa = xs + s * (y0 + dy * (U * j)), xb = xa + s * dy * (U - 1);
                 check = check || min(xa, xb) < DSPAN || max(xa, xb) >= k.W || dmask;
-                if (lbw) spec = spec || min(xa, xb) <= 0 || max(xa, xb) >= xedge;
             }
             if (spec) {
+                if constexpr (WTD) {
 #pragma unroll
-                for (int r = 0; r < U; r++)
-                    if (U * j + r < nrows) row(std::true_type{}, std::true_type{}, U * j + r, boff + r * rowBytes);
+                    for (int r = 0; r < U; r++)
+                        if (U * j + r < nrows) row(std::true_type{}, std::true_type{}, U * j + r, boff + r * rowBytes);
+                }
             } else if (check) {
 #pragma unroll
                 for (int r = 0; r < U; r++)
@@ -733,8 +760,10 @@ __host__ __device__ inline int hp_smem_bytes(int R, int ppl, bool lr, int W, boo
     return align128(R * hp_bars(two) * 8) + R * hp_warp_bytes(ppl, lr, W, two);
 }
 
-template <int PPL, int MODE, bool TWO, int EXCL = 0>
+template <int PPL, int MODE, bool TWO, int VAR = 0>
 __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, unsigned char* smem) {
+    constexpr bool WTD = VAR != 0;  // VAR as for vd_body
+    constexpr int EXCL = VAR == 2 ? 1 : (VAR == 3 ? 2 : 0);
     constexpr int SB = 128 * PPL;
     constexpr int NSL = hp_slots(TWO);   // S slots per row
     constexpr int kHpU = hp_px(TWO);     // pixels per S slot
@@ -848,22 +877,22 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
         uint32_t exm[PPL];
         if (EXCL == 2) excl_mask<PPL>(base_d, k.D, exm);
         const bool last_lane = lane == 31;
-        // reference weights: the row counts nowhere (rcls 0: every step adds
-        // the offset alone, no recurrence), or once with border cells that
-        // may have classes of their own (rbw); in the last pass up to two
-        // cells of the row count a repeated line more than once
-        // (x, (n-1) << 1 | slot)
-        const int rwv = k.lw ? (int)k.lw[y] : 1;
-        const int rcls = rwv & 3;
-        const bool rbw = k.bw && (rwv & 4);
-        const bool brow = rbw && (y == 0 || y == k.H - 1);
-        int cx0 = -1, cc0 = 0, cx1 = -1, cc1 = 0;
-        if (MODE == 2 && k.corner) {
-            const int4 e = *(const int4*)(k.corner + 4 * y);
-            cx0 = e.x;
-            cc0 = e.y;
-            cx1 = e.z;
-            cc1 = e.w;
+        // reference weights: a row counts nowhere (every step adds the offset
+        // alone, no recurrence), or once with border cells that may have
+        // classes of their own; in the last pass up to two cells of the row
+        // count a repeated line more than once
+        // the row's state in two registers: flags (1 counts nowhere, 2 border
+        // cells with classes of their own, 4 an all-border row of those) and
+        // the columns of the repeated cells, 16 bits each (0xFFFF: none;
+        // their counts are read again where a group holds one)
+        const int rwv = (WTD && k.lw) ? (int)k.lw[y] : 1;
+        const bool rbw0 = WTD && k.bw && (rwv & 4);
+        const uint32_t rflags = ((rwv & 3) == 0 ? 1u : 0u) | (rbw0 ? 2u : 0u) |
+                                (rbw0 && (y == 0 || y == k.H - 1) ? 4u : 0u);
+        uint32_t cxs = 0xFFFFFFFFu;
+        if (WTD && MODE == 2 && k.corner) {
+            const int2 e0 = *(const int2*)(k.corner + 4 * y), e1 = *(const int2*)(k.corner + 4 * y + 2);
+            cxs = (e0.x < 0 ? 0xFFFFu : (uint32_t)e0.x) | ((e1.x < 0 ? 0xFFFFu : (uint32_t)e1.x) << 16);
         }
 
         // One walk of the row in direction DXP (x increasing) with the
@@ -947,7 +976,7 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                 constexpr bool MASK = decltype(Mc)::value || SPEC;
                 constexpr int N = T % NJ;
                 // a row that counts nowhere: no right-plane window, cost or recurrence
-                const bool zero = SPEC && rcls == 0;
+                const bool zero = SPEC && (rflags & 1u);
                 uint32_t c[PPL], Ln[PPL], sv[PPL];
                 if (!zero) {
                     uint32_t vi, vn, vx;
@@ -980,10 +1009,10 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
 #pragma unroll
                         for (int q = 0; q < PPL; q++) c[q] = mask_pair(c[q], base_d + 2 * q, lim, k.BIGBIG);
                     }
-                    recur<PPL>(L, m, c, Ln, lane, k);
+                    recur<PPL, WTD>(L, m, c, Ln, lane, k);
                 }
                 Vec<PPL>::lds((const uint32_t*)(slot + xo * SB) + lane * PPL, sv);
-                if (zero || (SPEC && rbw && (brow || x == 0 || x == W - 1) &&
+                if (zero || (SPEC && (rflags & 2u) && ((rflags & 4u) || x == 0 || x == W - 1) &&
                              k.bw[border_index(W, k.H, x, y)] == 0)) {
                     // a border cell a later walk restarts: the offset alone
 #pragma unroll
@@ -1007,7 +1036,7 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                     // 32 bits (L - OFF may be negative), clamped at 2^23 - 1 so that
                     // invalid cells stay above every valid one.
                     int key[NJ];
-                    if (SPEC && (x == cx0 || x == cx1)) {
+                    if (SPEC && (x == (int)(cxs & 0xFFFFu) || x == (int)(cxs >> 16))) {
                         int sl[NJ];
 #pragma unroll
                         for (int q = 0; q < PPL; q++) {
@@ -1017,7 +1046,7 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                         const int off = (int)(k.OFFOFF & 0xFFFFu);
 #pragma unroll
                         for (int e = 0; e < 2; e++) {
-                            const int cx = e ? cx1 : cx0, cc = e ? cc1 : cc0;
+                            const int cx = (int)((cxs >> (16 * e)) & 0xFFFFu), cc = k.corner[4 * y + 2 * e + 1];
                             if (x != cx) continue;
                             const uint32_t* sd = k.side_all + ((size_t)(cc & 1) * k.H + y) * k.Dp2 + lane * PPL;
                             const int w = cc >> 1;
@@ -1082,15 +1111,19 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                 if (!__all_sync(FULL, good)) return false;
                 const unsigned char* slot = wbase + s * SLOT;
                 const int xlo = group_lo(j), xhi = group_hi(j), n = xhi - xlo + 1;
-                const bool special = rcls == 0 || brow || (rbw && (xlo == 0 || xhi >= W - 1)) ||
-                                     (cx0 >= xlo && cx0 <= xhi) || (cx1 >= xlo && cx1 <= xhi) || (k.GSTART && j == 0);
+                const int cxa = (int)(cxs & 0xFFFFu), cxb = (int)(cxs >> 16);
+                const bool special = WTD && ((rflags & 5u) || ((rflags & 2u) && (xlo == 0 || xhi >= W - 1)) ||
+                                             (cxa >= xlo && cxa <= xhi) || (cxb >= xlo && cxb <= xhi) ||
+                                             (k.GSTART && j == 0));
                 if (special) {
-                    static_for<0, kHpU>([&](auto ic) {
-                        constexpr int i = decltype(ic)::value;
-                        if (i < n)
-                            step(std::integral_constant<int, T0 + i>{}, std::true_type{}, std::true_type{},
-                                 DXP ? xlo + i : xhi - i, slot, DXP ? i : n - 1 - i);
-                    });
+                    if constexpr (WTD) {
+                        static_for<0, kHpU>([&](auto ic) {
+                            constexpr int i = decltype(ic)::value;
+                            if (i < n)
+                                step(std::integral_constant<int, T0 + i>{}, std::true_type{}, std::true_type{},
+                                     DXP ? xlo + i : xhi - i, slot, DXP ? i : n - 1 - i);
+                        });
+                    }
                 } else if (n == kHpU && xlo >= DSPAN && k.D >= DSPAN) {
                     static_for<0, kHpU>([&](auto ic) {
                         constexpr int i = decltype(ic)::value;

@@ -31,17 +31,17 @@ struct GroupPairs {
 // producer, so that two blocks (one of each concurrent pass chain) share an SM.
 constexpr int kVdMaxG = 15;
 
-template <int PPL, int MODE, bool DIAG, int EXCL>
+template <int PPL, int MODE, bool DIAG, int VAR>
 __global__ void __launch_bounds__((kVdMaxG + 1) * 32, 2)
     vd_pass(FK k, int s, int dy, int kmin, int nlines, int G, GroupPairs gp, int paired) {
     extern __shared__ __align__(128) unsigned char smem[];
     if (!paired) {
-        vd_body<PPL, MODE, DIAG, EXCL>(k, s, dy, kmin, nlines, G, blockIdx.x, smem);
+        vd_body<PPL, MODE, DIAG, VAR>(k, s, dy, kmin, nlines, G, blockIdx.x, smem);
         return;
     }
-    vd_body<PPL, MODE, DIAG, EXCL>(k, s, dy, kmin, nlines, G, gp.first[blockIdx.x], smem);
+    vd_body<PPL, MODE, DIAG, VAR>(k, s, dy, kmin, nlines, G, gp.first[blockIdx.x], smem);
     const int j2 = gp.second[blockIdx.x];
-    if (j2 >= 0) vd_body<PPL, MODE, DIAG, EXCL>(k, s, dy, kmin, nlines, G, j2, smem);
+    if (j2 >= 0) vd_body<PPL, MODE, DIAG, VAR>(k, s, dy, kmin, nlines, G, j2, smem);
 }
 
 constexpr int kHpMaxRows = 16;  // consumer warps per block, horizontal passes
@@ -54,10 +54,10 @@ constexpr int kHpMaxRows = 16;  // consumer warps per block, horizontal passes
 constexpr int kHpRegs = 112;
 static_assert((kHpMaxRows + 1) * 32 * kHpRegs <= 65536, "a horizontal block must fit the register file");
 
-template <int PPL, int MODE, bool TWO, int EXCL>
+template <int PPL, int MODE, bool TWO, int VAR>
 __global__ void __maxnreg__(kHpRegs) hp_pass(FK k, int dx, int R) {
     extern __shared__ __align__(128) unsigned char smem[];
-    hp_body<PPL, MODE, TWO, EXCL>(k, dx, R, blockIdx.x, smem);
+    hp_body<PPL, MODE, TWO, VAR>(k, dx, R, blockIdx.x, smem);
 }
 
 // ------------------------------------------------------------- host side
@@ -121,7 +121,7 @@ int pair_count(const GroupPairs& gp) {
     return n;
 }
 
-template <int PPL, int MODE, bool DIAG, int EXCL>
+template <int PPL, int MODE, bool DIAG, int VAR>
 cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
     const int s = dx * dy;
     const int nlines = s == 0 ? k.W : k.W + k.H - 1;
@@ -159,15 +159,15 @@ cudaError_t launch_vd(const FK& k, int dx, int dy, cudaStream_t st) {
     if (!paired) blocks = (nlines + G - 1) / G;
     const int smem = vd_smem_bytes(G, PPL);
     if (smem > kSmemBudget) return cudaErrorInvalidConfiguration;
-    cudaError_t e = opt_in_smem((const void*)vd_pass<PPL, MODE, DIAG, EXCL>, smem);
+    cudaError_t e = opt_in_smem((const void*)vd_pass<PPL, MODE, DIAG, VAR>, smem);
     if (e != cudaSuccess) return e;
-    vd_pass<PPL, MODE, DIAG, EXCL><<<blocks, (G + 1) * 32, smem, st>>>(k, s, dy, kmin, nlines, G, gp, paired);
+    vd_pass<PPL, MODE, DIAG, VAR><<<blocks, (G + 1) * 32, smem, st>>>(k, s, dy, kmin, nlines, G, gp, paired);
     return cudaGetLastError();
 }
 
 // rows per block: spread the rows over every SM, at most max_rows (a pass
 // that shares the SMs with a concurrent chain keeps its blocks small)
-template <int PPL, int MODE, bool TWO, int EXCL>
+template <int PPL, int MODE, bool TWO, int VAR>
 cudaError_t launch_hp(const FK& k, int dx, int max_rows, cudaStream_t st) {
     const bool lr = MODE == 2 && k.lr_thr >= 0;
     const int nsm = sm_count();
@@ -177,10 +177,10 @@ cudaError_t launch_hp(const FK& k, int dx, int max_rows, cudaStream_t st) {
     while (R > 1 && hp_smem_bytes(R, PPL, lr, k.W, TWO) > kSmemBudget) R--;
     const int smem = hp_smem_bytes(R, PPL, lr, k.W, TWO);
     if (smem > kSmemBudget) return cudaErrorInvalidConfiguration;
-    cudaError_t e = opt_in_smem((const void*)hp_pass<PPL, MODE, TWO, EXCL>, smem);
+    cudaError_t e = opt_in_smem((const void*)hp_pass<PPL, MODE, TWO, VAR>, smem);
     if (e != cudaSuccess) return e;
     const int blocks = (k.H + R - 1) / R;
-    hp_pass<PPL, MODE, TWO, EXCL><<<blocks, (R + 1) * 32, smem, st>>>(k, dx, R);
+    hp_pass<PPL, MODE, TWO, VAR><<<blocks, (R + 1) * 32, smem, st>>>(k, dx, R);
     return cudaGetLastError();
 }
 
@@ -200,7 +200,7 @@ FK for_dir(const FK& base, const FusedArgs& a, int dir) {
     return r;
 }
 
-template <int PPL, int EXCL>
+template <int PPL, int VAR>
 cudaError_t run_fused(const FK& k, const FusedArgs& a, cudaStream_t st, Timer* tm) {
     cudaError_t e;
     auto mark = [&](const char* n, cudaStream_t s) {
@@ -210,23 +210,23 @@ cudaError_t run_fused(const FK& k, const FusedArgs& a, cudaStream_t st, Timer* t
              kd3 = for_dir(k, a, 4), kd4 = for_dir(k, a, 5), kh1 = for_dir(k, a, 6), kh2 = for_dir(k, a, 7);
     const bool chains = a.paths == 8 && a.agg2 && a.side_stream && a.fork && a.join;
     if (!chains) {
-        if ((e = launch_vd<PPL, 0, false, EXCL>(kv1, 0, 1, st)) != cudaSuccess) return e;
+        if ((e = launch_vd<PPL, 0, false, VAR>(kv1, 0, 1, st)) != cudaSuccess) return e;
         mark("fused_pass_V+", st);
-        if ((e = launch_vd<PPL, 1, false, EXCL>(kv2, 0, -1, st)) != cudaSuccess) return e;
+        if ((e = launch_vd<PPL, 1, false, VAR>(kv2, 0, -1, st)) != cudaSuccess) return e;
         mark("fused_pass_V-", st);
         if (a.paths == 8) {
-            if ((e = launch_vd<PPL, 1, true, EXCL>(kd1, 1, 1, st)) != cudaSuccess) return e;
+            if ((e = launch_vd<PPL, 1, true, VAR>(kd1, 1, 1, st)) != cudaSuccess) return e;
             mark("fused_pass_D1+", st);
-            if ((e = launch_vd<PPL, 1, true, EXCL>(kd2, -1, -1, st)) != cudaSuccess) return e;
+            if ((e = launch_vd<PPL, 1, true, VAR>(kd2, -1, -1, st)) != cudaSuccess) return e;
             mark("fused_pass_D1-", st);
-            if ((e = launch_vd<PPL, 1, true, EXCL>(kd3, -1, 1, st)) != cudaSuccess) return e;
+            if ((e = launch_vd<PPL, 1, true, VAR>(kd3, -1, 1, st)) != cudaSuccess) return e;
             mark("fused_pass_D2+", st);
-            if ((e = launch_vd<PPL, 1, true, EXCL>(kd4, 1, -1, st)) != cudaSuccess) return e;
+            if ((e = launch_vd<PPL, 1, true, VAR>(kd4, 1, -1, st)) != cudaSuccess) return e;
             mark("fused_pass_D2-", st);
         }
-        if ((e = launch_hp<PPL, 1, false, EXCL>(kh1, 1, kMaxG, st)) != cudaSuccess) return e;
+        if ((e = launch_hp<PPL, 1, false, VAR>(kh1, 1, kMaxG, st)) != cudaSuccess) return e;
         mark("fused_pass_H+", st);
-        if ((e = launch_hp<PPL, 2, false, EXCL>(kh2, -1, kMaxG, st)) != cudaSuccess) return e;
+        if ((e = launch_hp<PPL, 2, false, VAR>(kh2, -1, kMaxG, st)) != cudaSuccess) return e;
         mark("fused_pass_H-_wta", st);
         return cudaSuccess;
     }
@@ -245,17 +245,17 @@ cudaError_t run_fused(const FK& k, const FusedArgs& a, cudaStream_t st, Timer* t
         if ((e = cudaStreamWaitEvent(sd, a.fork, 0)) != cudaSuccess) return e;
         if (tm) tm->fork(sd);
     }
-    if ((e = launch_vd<PPL, 0, true, EXCL>(kb2, -1, -1, sd)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 0, true, VAR>(kb2, -1, -1, sd)) != cudaSuccess) return e;
     mark("fused_pass_D1-", sd);
-    if ((e = launch_vd<PPL, 0, false, EXCL>(kv1, 0, 1, st)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 0, false, VAR>(kv1, 0, 1, st)) != cudaSuccess) return e;
     mark("fused_pass_V+", st);
-    if ((e = launch_vd<PPL, 1, true, EXCL>(kb3, -1, 1, sd)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 1, true, VAR>(kb3, -1, 1, sd)) != cudaSuccess) return e;
     mark("fused_pass_D2+", sd);
-    if ((e = launch_vd<PPL, 1, false, EXCL>(kv2, 0, -1, st)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 1, false, VAR>(kv2, 0, -1, st)) != cudaSuccess) return e;
     mark("fused_pass_V-", st);
-    if ((e = launch_vd<PPL, 1, true, EXCL>(kb4, 1, -1, sd)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 1, true, VAR>(kb4, 1, -1, sd)) != cudaSuccess) return e;
     mark("fused_pass_D2-", sd);
-    if ((e = launch_vd<PPL, 1, true, EXCL>(kd1, 1, 1, st)) != cudaSuccess) return e;
+    if ((e = launch_vd<PPL, 1, true, VAR>(kd1, 1, 1, st)) != cudaSuccess) return e;
     mark("fused_pass_D1+", st);
     if (concurrent) {
         if ((e = cudaEventRecord(a.join, sd)) != cudaSuccess) return e;
@@ -264,9 +264,9 @@ cudaError_t run_fused(const FK& k, const FusedArgs& a, cudaStream_t st, Timer* t
     }
     FK kj = kh1;
     kj.S2 = (const uint32_t*)a.agg2;
-    if ((e = launch_hp<PPL, 1, true, EXCL>(kj, 1, kMaxG, st)) != cudaSuccess) return e;
+    if ((e = launch_hp<PPL, 1, true, VAR>(kj, 1, kMaxG, st)) != cudaSuccess) return e;
     mark("fused_pass_H+", st);
-    if ((e = launch_hp<PPL, 2, false, EXCL>(kh2, -1, kMaxG, st)) != cudaSuccess) return e;
+    if ((e = launch_hp<PPL, 2, false, VAR>(kh2, -1, kMaxG, st)) != cudaSuccess) return e;
     mark("fused_pass_H-_wta", st);
     return cudaSuccess;
 }
@@ -317,22 +317,26 @@ cudaError_t launch_fused(const FusedArgs& a, cudaStream_t st, Timer* tm) {
     k.lr_thr = a.lr_thr;
     k.err = a.err;
     k.S2 = nullptr;
-    // the excluded disparity D-1 is the high half of lane 31's last pair when
-    // D fills the warp's span (EXCL 1), else anywhere (EXCL 2)
-    const int excl = a.excl ? (a.D == 64 * ppl ? 1 : 2) : 0;
-    if (excl == 1) {
-        if (ppl == 1) return run_fused<1, 1>(k, a, st, tm);
-        if (ppl == 2) return run_fused<2, 1>(k, a, st, tm);
-        return run_fused<4, 1>(k, a, st, tm);
+    // kernel variant: 0 the STANDARD recurrence over the full table (none of
+    // the reference-weight code compiled in); else 1, with the excluded
+    // minimum of the reference CPU recurrence 2 (D-1 is the high half of lane
+    // 31's last pair: D fills the warp's span) or 3 (anywhere)
+    const bool wtd = a.excl || a.gstart || a.off_h || (a.fw && a.weights);
+    const int var = !wtd ? 0 : (!a.excl ? 1 : (a.D == 64 * ppl ? 2 : 3));
+    switch (var * 4 + ppl) {
+        case 1: return run_fused<1, 0>(k, a, st, tm);
+        case 2: return run_fused<2, 0>(k, a, st, tm);
+        case 4: return run_fused<4, 0>(k, a, st, tm);
+        case 5: return run_fused<1, 1>(k, a, st, tm);
+        case 6: return run_fused<2, 1>(k, a, st, tm);
+        case 8: return run_fused<4, 1>(k, a, st, tm);
+        case 9: return run_fused<1, 2>(k, a, st, tm);
+        case 10: return run_fused<2, 2>(k, a, st, tm);
+        case 12: return run_fused<4, 2>(k, a, st, tm);
+        case 13: return run_fused<1, 3>(k, a, st, tm);
+        case 14: return run_fused<2, 3>(k, a, st, tm);
+        default: return run_fused<4, 3>(k, a, st, tm);
     }
-    if (excl == 2) {
-        if (ppl == 1) return run_fused<1, 2>(k, a, st, tm);
-        if (ppl == 2) return run_fused<2, 2>(k, a, st, tm);
-        return run_fused<4, 2>(k, a, st, tm);
-    }
-    if (ppl == 1) return run_fused<1, 0>(k, a, st, tm);
-    if (ppl == 2) return run_fused<2, 0>(k, a, st, tm);
-    return run_fused<4, 0>(k, a, st, tm);
 }
 
 }  // namespace tdv
