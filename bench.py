@@ -51,12 +51,13 @@ P1, P2, PATHS, LR = 10.0, 120.0, 8, 1
 METRIC = "1080p D=256 8-path SGM fps"
 UNIT = "frames/s"
 # recurrence and path table per --semantics: stereo_sgm keywords, the
-# oracle's constants, and the excluded-minimum flag of the fused kernels
+# oracle's constants, and the fused kernels' variant at D = 256 (0 standard
+# over the full table; 2 reference weights with the minimum over d < D-1)
 SEMANTICS = {
-    "reference": {"kw": {"semantics": "ref_cpu", "table": "ref"}, "orc": (1, 1), "excl": 1,
+    "reference": {"kw": {"semantics": "ref_cpu", "table": "ref"}, "orc": (1, 1), "var": 2,
                   "recurrence": "reference CPU (tdvision/semiglobalcpu.cpp:56-126: start-assign, min over d < D-1)",
                   "table": "reference (tdvision/semiglobal.cu:57-230, stale diagonal ends)"},
-    "standard": {"kw": {"semantics": "standard", "table": "full"}, "orc": (0, 0), "excl": 0,
+    "standard": {"kw": {"semantics": "standard", "table": "full"}, "orc": (0, 0), "var": 0,
                  "recurrence": "standard (S += C at path starts, min over all d)",
                  "table": "full (every line walked once each way)"},
 }
@@ -735,9 +736,8 @@ def measure_video(ctx, dev, n_frames=300, refit_steps=50):
 # ------------------------------------------------------------------ ours
 def kernel_of(sem):
     """The compiled kernel behind each timed pass (PPL = 4 at D = 256), as
-    ncu names it; the last template argument is the excluded-minimum flag of
-    the reference CPU recurrence."""
-    e = SEMANTICS[sem]["excl"]
+    ncu names it; the last template argument is the kernel variant."""
+    e = SEMANTICS[sem]["var"]
     return {
         "fused_prep": "prep_kernel",
         "fused_pass_V+": f"vd_pass<4, 0, 0, {e}>",
@@ -747,7 +747,7 @@ def kernel_of(sem):
         "fused_pass_D2+": f"vd_pass<4, 1, 1, {e}>",
         "fused_pass_D2-": f"vd_pass<4, 1, 1, {e}>",
         "fused_pass_H+": f"hp_pass<4, 1, 1, {e}>",
-        "fused_pass_H-_wta": f"hp_pass<4, 2, 0, {e}>",
+        "fused_pass_H-_wta": f"hp_wta_pass<4, 0, {e}>",
     }
 
 

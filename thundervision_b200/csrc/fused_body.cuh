@@ -760,6 +760,47 @@ __host__ __device__ inline int hp_smem_bytes(int R, int ppl, bool lr, int W, boo
     return align128(R * hp_bars(two) * 8) + R * hp_warp_bytes(ppl, lr, W, two);
 }
 
+// The last pass's keys of a cell that counts a repeated line more than once:
+// the cell's packed 16-bit sums plus (n-1) L from the side row(s) of its row,
+// as signed 32-bit (S << 8 | d) clamped at 2^23 - 1 so that invalid cells stay
+// above every valid one.  Out of line (two cells of a row take it, and the
+// horizontal step it would sit in is unrolled many times over); sums and keys
+// travel by value so that the callers' arrays stay in registers.
+template <int PPL>
+struct PairRow {
+    uint32_t v[PPL];
+};
+template <int PPL>
+struct KeyRow {
+    int v[2 * PPL];
+};
+template <int PPL>
+__device__ __noinline__ KeyRow<PPL> corner_keys(const int* corner, const uint32_t* side_all, int H, int Dp2, int off,
+                                                int y, int x, uint32_t cxs, int lane, int base_d, PairRow<PPL> sv) {
+    KeyRow<PPL> r;
+#pragma unroll
+    for (int q = 0; q < PPL; q++) {
+        r.v[2 * q] = (int)(sv.v[q] & 0xFFFFu);
+        r.v[2 * q + 1] = (int)(sv.v[q] >> 16);
+    }
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+        if (x != (int)((cxs >> (16 * e)) & 0xFFFFu)) continue;
+        const int cc = corner[4 * y + 2 * e + 1];
+        const uint32_t* sd = side_all + ((size_t)(cc & 1) * H + y) * Dp2 + lane * PPL;
+        const int w = cc >> 1;
+#pragma unroll
+        for (int q = 0; q < PPL; q++) {
+            const uint32_t u = __ldcg(sd + q);
+            r.v[2 * q] += w * ((int)(u & 0xFFFFu) - off);
+            r.v[2 * q + 1] += w * ((int)(u >> 16) - off);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 2 * PPL; j++) r.v[j] = min(r.v[j], (1 << 23) - 1) * 256 + base_d + j;
+    return r;
+}
+
 template <int PPL, int MODE, bool TWO, int VAR = 0>
 __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, unsigned char* smem) {
     constexpr bool WTD = VAR != 0;  // VAR as for vd_body
@@ -1037,28 +1078,13 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                     // invalid cells stay above every valid one.
                     int key[NJ];
                     if (SPEC && (x == (int)(cxs & 0xFFFFu) || x == (int)(cxs >> 16))) {
-                        int sl[NJ];
+                        PairRow<PPL> pr;
 #pragma unroll
-                        for (int q = 0; q < PPL; q++) {
-                            sl[2 * q] = (int)(sv[q] & 0xFFFFu);
-                            sl[2 * q + 1] = (int)(sv[q] >> 16);
-                        }
-                        const int off = (int)(k.OFFOFF & 0xFFFFu);
+                        for (int q = 0; q < PPL; q++) pr.v[q] = sv[q];
+                        const KeyRow<PPL> kr = corner_keys<PPL>(k.corner, k.side_all, k.H, k.Dp2,
+                                                                (int)(k.OFFOFF & 0xFFFFu), y, x, cxs, lane, base_d, pr);
 #pragma unroll
-                        for (int e = 0; e < 2; e++) {
-                            const int cx = (int)((cxs >> (16 * e)) & 0xFFFFu), cc = k.corner[4 * y + 2 * e + 1];
-                            if (x != cx) continue;
-                            const uint32_t* sd = k.side_all + ((size_t)(cc & 1) * k.H + y) * k.Dp2 + lane * PPL;
-                            const int w = cc >> 1;
-#pragma unroll
-                            for (int q = 0; q < PPL; q++) {
-                                const uint32_t u = __ldcg(sd + q);
-                                sl[2 * q] += w * ((int)(u & 0xFFFFu) - off);
-                                sl[2 * q + 1] += w * ((int)(u >> 16) - off);
-                            }
-                        }
-#pragma unroll
-                        for (int j = 0; j < NJ; j++) key[j] = min(sl[j], (1 << 23) - 1) * 256 + base_d + j;
+                        for (int j = 0; j < NJ; j++) key[j] = kr.v[j];
                     } else {
 #pragma unroll
                         for (int q = 0; q < PPL; q++) {

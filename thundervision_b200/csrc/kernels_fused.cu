@@ -60,6 +60,21 @@ __global__ void __maxnreg__(kHpRegs) hp_pass(FK k, int dx, int R) {
     hp_body<PPL, MODE, TWO, VAR>(k, dx, R, blockIdx.x, smem);
 }
 
+// The last pass runs alone at the end of a frame: under the reference
+// weights (VAR > 0) its keys, border flags and repeated-cell columns stay in
+// registers at 168 per thread (measured on a full-HD frame, D = 256: 0.58 ms
+// against 0.64 ms at 112); the standard variant needs no more than 112 and
+// keeps room for the next frame's first pass beside it.
+constexpr int hp_wta_regs(int var) { return var == 0 ? kHpRegs : 168; }
+constexpr int hp_wta_max_rows(int var) {
+    return 65536 / (32 * hp_wta_regs(var)) - 1 < kHpMaxRows ? 65536 / (32 * hp_wta_regs(var)) - 1 : kHpMaxRows;
+}
+template <int PPL, bool TWO, int VAR>
+__global__ void __maxnreg__(hp_wta_regs(VAR)) hp_wta_pass(FK k, int dx, int R) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    hp_body<PPL, 2, TWO, VAR>(k, dx, R, blockIdx.x, smem);
+}
+
 // ------------------------------------------------------------- host side
 int sm_count() {
     static int cache[64] = {0};
@@ -172,15 +187,22 @@ cudaError_t launch_hp(const FK& k, int dx, int max_rows, cudaStream_t st) {
     const bool lr = MODE == 2 && k.lr_thr >= 0;
     const int nsm = sm_count();
     int R = (k.H + nsm - 1) / nsm;
-    if (max_rows > kHpMaxRows) max_rows = kHpMaxRows;
+    const int cap = MODE == 2 ? hp_wta_max_rows(VAR) : kHpMaxRows;
+    if (max_rows > cap) max_rows = cap;
     R = R < 1 ? 1 : (R > max_rows ? max_rows : R);
     while (R > 1 && hp_smem_bytes(R, PPL, lr, k.W, TWO) > kSmemBudget) R--;
     const int smem = hp_smem_bytes(R, PPL, lr, k.W, TWO);
     if (smem > kSmemBudget) return cudaErrorInvalidConfiguration;
-    cudaError_t e = opt_in_smem((const void*)hp_pass<PPL, MODE, TWO, VAR>, smem);
-    if (e != cudaSuccess) return e;
     const int blocks = (k.H + R - 1) / R;
-    hp_pass<PPL, MODE, TWO, VAR><<<blocks, (R + 1) * 32, smem, st>>>(k, dx, R);
+    if constexpr (MODE == 2) {
+        cudaError_t e = opt_in_smem((const void*)hp_wta_pass<PPL, TWO, VAR>, smem);
+        if (e != cudaSuccess) return e;
+        hp_wta_pass<PPL, TWO, VAR><<<blocks, (R + 1) * 32, smem, st>>>(k, dx, R);
+    } else {
+        cudaError_t e = opt_in_smem((const void*)hp_pass<PPL, MODE, TWO, VAR>, smem);
+        if (e != cudaSuccess) return e;
+        hp_pass<PPL, MODE, TWO, VAR><<<blocks, (R + 1) * 32, smem, st>>>(k, dx, R);
+    }
     return cudaGetLastError();
 }
 
