@@ -227,9 +227,21 @@ def ref_code_run(lib, L, R, d=D):
     h, w = L.shape
     dn = np.empty((h, w), np.float32)
     p = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-    t0 = time.perf_counter()
-    lib.ref_semiglobal_cpu(p(C), w, h, d, p(Lf), p(dn))
-    return time.perf_counter() - t0, dn
+    # the reference prints its own timer to stdout (semiglobalcpu.cpp:229,
+    # wtacpu.cpp:54): send it to stderr so that stdout stays one JSON line
+    libc = ctypes.CDLL(None)
+    sys.stdout.flush()
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        t0 = time.perf_counter()
+        lib.ref_semiglobal_cpu(p(C), w, h, d, p(Lf), p(dn))
+        t = time.perf_counter() - t0
+        libc.fflush(None)
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+    return t, dn
 
 
 def _rows_for(seconds_per_step, sem, threads, lo=16):
@@ -519,6 +531,45 @@ def measure_soft(ctx, dev, reps=5):
     return {"workload": "960x540, D=128, FP32 BT cost, 8 paths, tau=1, L1 loss, checkpoint 32",
             "fwd_adjoint_ms": t_fb, "plain_soft_forward_ms": t_f, "hard_sgm_wta_ms": t_h,
             "ratio_vs_plain_forward": t_fb / t_f, "ratio_vs_hard_sgm": t_fb / t_h}
+
+
+def measure_configs(ctx, dev, sem, reps=20):
+    """The fused call (tdv_stereo_sgm: BT + SGM + WTA + L-R, threshold 1) on
+    each plain-method configuration under the bench's semantics: 384x288
+    D=16 and 640x480 D=64 (8 paths), 1920x1080 D=256 with 8 and 4 paths;
+    device ms per pair, L2 flushed before each call (mean of `reps`)."""
+    import torch
+
+    from thundervision_b200 import synthetic
+    st = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    out = {"semantics": sem, "l2": "flushed before each call"}
+    cases = [("384x288_D16_P8", synthetic.pair_small(1)[:2], 16, 8),
+             ("640x480_D64_P8", synthetic.pair_medium(1)[:2], 64, 8),
+             ("1920x1080_D256_P8", _band(H), 256, 8),
+             ("1920x1080_D256_P4", _band(H), 256, 4)]
+    for name, (L, R), d, paths in cases:
+        l, r = torch.from_numpy(L).to(dev), torch.from_numpy(R).to(dev)
+        h, w = L.shape
+
+        def call():
+            return ctx.stereo_sgm(l, r, d, P1, P2, paths=paths, lr=LR, **SEMANTICS[sem]["kw"])
+
+        for _ in range(3):
+            call()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(reps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            call()
+            e1.record(st)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        ms = tot / reps
+        out[name] = {"ms": ms, "fps": 1000.0 / ms, "gcells_per_s": w * h * d * paths / (ms / 1000.0) / 1e9}
+    return out
 
 
 def measure_plain(ctx, dev, reps=3):
@@ -1076,6 +1127,10 @@ def run_ours(args):
             line["reference_literal"] = measure_reference_literal(ctx, dev, dev_frames, flush)
         except Exception as exc:
             line[f"semantics_{other}"] = {"error": f"{type(exc).__name__}: {exc}"}
+        try:
+            line["configs"] = measure_configs(ctx, dev, args.semantics)
+        except Exception as exc:
+            line["configs"] = {"error": f"{type(exc).__name__}: {exc}"}
         for key, fn in (("batch", measure_batch), ("soft", measure_soft), ("plain", measure_plain),
                         ("image_stages", measure_image), ("reconstruction", measure_reconstruction),
                         ("video", measure_video)):
