@@ -155,11 +155,28 @@ tdv_status tdv_fast_wta(tdv_ctx* ctx, const tdv_image* left, const tdv_image* ri
 /* Birchfield-Tomasi cost recomputed inside the aggregation, no cost DSI:
  * the role of SemiGlobalLabDevRun (tdvision/semiglobal_lab.cu:232-282) with
  * the reference's cost and recurrence.  Integer-domain inputs (u8, scale 1,
- * P1/P2 multiples of 1/2, STANDARD, FULL, P2_CONST, D <= 256) take the fused
- * 16-bit path; anything else runs tdv_cost + tdv_sgm on context scratch. */
+ * P1/P2 multiples of 1/2, P2_CONST, D <= 256; any semantics and table whose
+ * 16-bit ranges hold) take the fused 16-bit path; anything else runs
+ * tdv_cost + tdv_sgm on context scratch. */
 tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right,
                           int32_t max_disp, const tdv_sgm_params* params, tdv_disparity* out,
                           tdv_stream stream);
+
+/* tdv_stereo_sgm's fused path over n frame pairs of one size (left[i],
+ * right[i] -> out[i]), for a frame stream: the frames alternate between two
+ * lanes, each with its own planes, aggregation volumes and streams, so that
+ * one frame's DRAM-bound passes run while the other lane's last pass (WTA and
+ * left-right check, bound by its instruction stream) finishes.  The call
+ * orders everything after the work already queued on `stream` and before the
+ * work queued on it afterwards; the outputs must not overlap one another.
+ * Maps are identical to n tdv_stereo_sgm calls.  Inputs outside the fused
+ * path return TDV_ERR_UNSUPPORTED.  The second lane's scratch (about as much
+ * as the first's) is allocated on the first call with n > 1.  No reference
+ * counterpart: the reference matches one pair per pipeline update
+ * (tdvision/devstereomatcher.cpp:36-48). */
+tdv_status tdv_stereo_sgm_frames(tdv_ctx* ctx, int32_t n, const tdv_image* left, const tdv_image* right,
+                                 int32_t max_disp, const tdv_sgm_params* params, tdv_disparity* out,
+                                 tdv_stream stream);
 
 /* Allocation-free variant of tdv_stereo_sgm's fused integer-domain path, for
  * callers that cannot call cudaMalloc while they run (a capture or control

@@ -29,7 +29,7 @@ EXPORTS = [
     "tdv_last_error_string", "tdv_status_string", "tdv_version", "tdv_volume_bytes",
     "tdv_ctx_enable_timing", "tdv_ctx_timings", "tdv_ctx_timing_name", "tdv_ctx_device_status",
     "tdv_soft_sgm_tape_bytes", "tdv_soft_sgm_forward", "tdv_soft_sgm_backward",
-    "tdv_stereo_sgm_static",
+    "tdv_stereo_sgm_static", "tdv_stereo_sgm_frames",
     "tdv_batch_create", "tdv_batch_destroy", "tdv_batch_set_tiles", "tdv_batch_get_tiles",
     "tdv_batch_autotune", "tdv_batch_run", "tdv_batch_graph_launch", "tdv_batch_status",
     "tdv_batch_set_wait_limit", "tdv_batch_work_queue",
@@ -123,6 +123,8 @@ def _declare(lib):
                                 P(tdv_disparity), vp]),
         "tdv_stereo_sgm_static": (st, [P(tdv_image), P(tdv_image), ctypes.c_int32, P(tdv_sgm_params),
                                        P(tdv_disparity), vp]),
+        "tdv_stereo_sgm_frames": (st, [vp, ctypes.c_int32, P(tdv_image), P(tdv_image), ctypes.c_int32,
+                                       P(tdv_sgm_params), P(tdv_disparity), vp]),
         "tdv_ctx_create": (st, [ctypes.c_int32, P(vp)]),
         "tdv_ctx_destroy": (None, [vp]),
         "tdv_ctx_set_allocator": (st, [vp, ALLOC_FN, FREE_FN, vp]),

@@ -335,6 +335,37 @@ class Context:
                                           ctypes.byref(prm), ctypes.byref(o), _stream()))
         return self._result(disp, dn, dr)
 
+    def stereo_sgm_frames(self, lefts, rights, max_disp, p1, p2, paths=8, table="full", semantics="standard",
+                          lr=None, norm=False, right_disp=False, outs=None):
+        """``stereo_sgm``'s fused path over a sequence of equal-size uint8
+        frame pairs (tdv_stereo_sgm_frames): consecutive frames run on two
+        lanes, so one frame's passes overlap the other's last pass.  Returns
+        one result dict per frame; ``outs`` (the dicts a previous call
+        returned) are written again instead of allocating new maps."""
+        n = len(lefts)
+        if n != len(rights) or n == 0:
+            raise ValueError("need as many right frames as left frames, at least one")
+        H, W = lefts[0].shape
+        li = (L.tdv_image * n)(*[_image(x) for x in lefts])
+        ri = (L.tdv_image * n)(*[_image(x) for x in rights])
+        prm = L.tdv_sgm_params(p1, p2, L.P2_CONST, paths, _TABLES[table], _SEMS[semantics])
+        oa = (L.tdv_disparity * n)()
+        results = []
+        for i in range(n):
+            if outs is not None:
+                r = outs[i]
+                dn, dr = r.get("disp_norm"), r.get("disp_right")
+                oa[i] = L.tdv_disparity(r["disp"].data_ptr(), dn.data_ptr() if dn is not None else None,
+                                        dr.data_ptr() if dr is not None else None, -1 if lr is None else int(lr))
+                results.append(r)
+            else:
+                o, disp, dn, dr = self._outputs(W, H, lefts[i].device, norm, right_disp, lr)
+                oa[i] = o
+                results.append(self._result(disp, dn, dr))
+        self.check(L.lib().tdv_stereo_sgm_frames(self.handle, n, li, ri, max_disp, ctypes.byref(prm), oa,
+                                                 _stream()))
+        return results
+
 
 class Batch:
     """Many uint8 pairs of uneven size and disparity range aggregated by one

@@ -120,6 +120,30 @@ tdv_status ensure_err(tdv_ctx* ctx, cudaStream_t st) {
     return TDV_OK;
 }
 
+// The second lane of tdv_stereo_sgm_frames: its two streams and four events.
+tdv_status ensure_lane(tdv_ctx* ctx) {
+    if (ctx->lane_main) return TDV_OK;
+    cudaStream_t m = nullptr, sd = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaError_t e = cudaStreamCreateWithFlags(&m, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sd, cudaStreamNonBlocking);
+    for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        if (m) cudaStreamDestroy(m);
+        if (sd) cudaStreamDestroy(sd);
+        for (int i = 0; i < 4; i++)
+            if (ev[i]) cudaEventDestroy(ev[i]);
+        return fail(ctx, TDV_ERR_CUDA, "creating the second frame lane failed: %s", cudaGetErrorString(e));
+    }
+    ctx->lane_main = m;
+    ctx->lane_side = sd;
+    ctx->lane_fork = ev[0];
+    ctx->lane_join = ev[1];
+    ctx->lane_start = ev[2];
+    ctx->lane_done = ev[3];
+    return TDV_OK;
+}
+
 tdv_status ensure_schedule(tdv_ctx* ctx, int W, int H, int table, int paths, cudaStream_t st) {
     tdv::PassSchedule& sc = ctx->sched;
     if (sc.W == W && sc.H == H && sc.table == table && sc.paths == paths && sc.d_walks) return TDV_OK;
@@ -346,6 +370,34 @@ bool fused_weights_ready(tdv_ctx* ctx, int W, int H, int D, const tdv_sgm_params
     return true;
 }
 
+// The fused launch's arguments for one pair, without its scratch, streams
+// and events (the caller's lane supplies those).
+tdv::FusedArgs fused_args(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right, int D,
+                          const tdv_sgm_params* params, const FusedPlan& fp, const tdv_disparity* out) {
+    tdv::FusedArgs a;
+    a.L = tdv::make_img(*left);
+    a.R = tdv::make_img(*right);
+    a.W = left->width;
+    a.H = left->height;
+    a.D = D;
+    a.p1h = fp.p1h;
+    a.p2h = fp.p2h;
+    a.excl = fp.excl;
+    a.off_h = fp.off_h;
+    a.gstart = fp.gstart;
+    if (fp.weighted) {
+        a.fw = &ctx->fweights;
+        a.weights = (const unsigned char*)ctx->fw_buf.ptr;
+    }
+    a.paths = params->paths;
+    a.disp = out->disp;
+    a.disp_norm = out->disp_norm;
+    a.disp_right = out->disp_right;
+    a.lr_thr = out->lr_threshold >= 0 ? out->lr_threshold : (out->disp_right ? 0x7FFFFFFF : -1);
+    a.err = (int*)ctx->err.ptr;
+    return a;
+}
+
 }  // namespace
 
 namespace tdv {
@@ -417,7 +469,8 @@ void tdv_ctx_destroy(tdv_ctx* ctx) {
     if (!ctx) return;
     const bool any = ctx->agg.ptr || ctx->cost.ptr || ctx->planes.ptr || ctx->codes.ptr ||
                      ctx->misc.ptr || ctx->sched_buf.ptr || ctx->err.ptr || ctx->soft.ptr ||
-                     ctx->agg2.ptr || ctx->defer.ptr || ctx->side || ctx->fw_buf.ptr || ctx->fside.ptr;
+                     ctx->agg2.ptr || ctx->defer.ptr || ctx->side || ctx->fw_buf.ptr || ctx->fside.ptr ||
+                     ctx->lane_main || ctx->planes_b.ptr || ctx->agg_b.ptr || ctx->agg2_b.ptr || ctx->fside_b.ptr;
     if (any) {
         DeviceScope ds(ctx->device);
         cudaDeviceSynchronize();
@@ -436,6 +489,14 @@ void tdv_ctx_destroy(tdv_ctx* ctx) {
         release_buf(ctx, ctx->defer);
         release_buf(ctx, ctx->fw_buf);
         release_buf(ctx, ctx->fside);
+        release_buf(ctx, ctx->planes_b);
+        release_buf(ctx, ctx->agg_b);
+        release_buf(ctx, ctx->agg2_b);
+        release_buf(ctx, ctx->fside_b);
+        if (ctx->lane_main) cudaStreamDestroy(ctx->lane_main);
+        if (ctx->lane_side) cudaStreamDestroy(ctx->lane_side);
+        for (cudaEvent_t e : {ctx->lane_fork, ctx->lane_join, ctx->lane_start, ctx->lane_done})
+            if (e) cudaEventDestroy(e);
     }
     if (!ctx->timer.ev.empty()) {
         DeviceScope ds(ctx->device);
@@ -796,32 +857,12 @@ tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* 
     if (fused) {
         TDV_TRY(reserve_fused(ctx, W, H, D));
         TDV_TRY(ensure_side(ctx));
-        tdv::FusedArgs a;
-        a.L = tdv::make_img(*left);
-        a.R = tdv::make_img(*right);
-        a.W = W;
-        a.H = H;
-        a.D = D;
-        a.p1h = fp.p1h;
-        a.p2h = fp.p2h;
-        a.excl = fp.excl;
-        a.off_h = fp.off_h;
-        a.gstart = fp.gstart;
-        if (fp.weighted) {
-            a.fw = &ctx->fweights;
-            a.weights = (const unsigned char*)ctx->fw_buf.ptr;
-            a.side = (uint32_t*)ctx->fside.ptr;
-        }
-        a.paths = params->paths;
-        a.disp = out->disp;
-        a.disp_norm = out->disp_norm;
-        a.disp_right = out->disp_right;
-        a.lr_thr = out->lr_threshold >= 0 ? out->lr_threshold : (out->disp_right ? 0x7FFFFFFF : -1);
+        TDV_TRY(ensure_err(ctx, S(stream)));
+        tdv::FusedArgs a = fused_args(ctx, left, right, D, params, fp, out);
         a.planes = ctx->planes.ptr;
         a.agg = ctx->agg.ptr;
-        TDV_TRY(ensure_err(ctx, S(stream)));
-        a.err = (int*)ctx->err.ptr;
         a.agg2 = ctx->agg2.ptr;
+        if (fp.weighted) a.side = (uint32_t*)ctx->fside.ptr;
         a.side_stream = ctx->side;
         a.fork = ctx->fork_ev;
         a.join = ctx->join_ev;
@@ -840,6 +881,71 @@ tdv_status tdv_stereo_sgm(tdv_ctx* ctx, const tdv_image* left, const tdv_image* 
     TDV_CUDA(tdv::launch_cost(tdv::make_img(*left), tdv::make_img(*right), TDV_COST_BT, 0,
                               tdv::make_vol(cv), S(stream), &ctx->timer));
     return run_sgm(ctx, &cv, left, params, nullptr, out, S(stream));
+}
+
+tdv_status tdv_stereo_sgm_frames(tdv_ctx* ctx, int32_t n, const tdv_image* left, const tdv_image* right,
+                                 int32_t D, const tdv_sgm_params* params, tdv_disparity* out,
+                                 tdv_stream stream) {
+    if (!ctx) return TDV_ERR_INVALID_ARG;
+    if (n < 1 || !left || !right || !out) return fail(ctx, TDV_ERR_INVALID_ARG, "need n >= 1 frames and arrays");
+    TDV_TRY(check_params(ctx, params));
+    if (D <= 0 || D > tdv::kMaxDispSgm)
+        return fail(ctx, TDV_ERR_UNSUPPORTED, "SGM supports 1 <= D <= %d (got %d)", tdv::kMaxDispSgm, D);
+    const int W = left[0].width, H = left[0].height;
+    FusedPlan fp;
+    for (int i = 0; i < n; i++) {
+        TDV_TRY(check_image(ctx, &left[i], "left"));
+        TDV_TRY(check_image(ctx, &right[i], "right"));
+        TDV_TRY(check_out(ctx, &out[i]));
+        if (left[i].width != W || left[i].height != H || right[i].width != W || right[i].height != H)
+            return fail(ctx, TDV_ERR_INVALID_ARG, "frame %d differs in size from frame 0", i);
+        const FusedPlan f = plan_fused(&left[i], &right[i], D, params);
+        if (!f.ok)
+            return fail(ctx, TDV_ERR_UNSUPPORTED,
+                        "frame sequences take the fused path only (u8 images at scale 1, P1/P2 multiples of "
+                        "1/2, P2_CONST)");
+        if (i == 0) fp = f;
+    }
+    TDV_DEVICE_SCOPE(ctx);
+    cudaStream_t st = S(stream);
+    if (fp.weighted) {
+        tdv_status werr;
+        const bool ok = fused_weights_ready(ctx, W, H, D, params, fp, st, &werr);
+        TDV_TRY(werr);
+        if (!ok)
+            return fail(ctx, TDV_ERR_UNSUPPORTED, "this size, table and semantics leave the fused path's ranges");
+    }
+    TDV_TRY(reserve_fused(ctx, W, H, D));
+    TDV_TRY(ensure_side(ctx));
+    TDV_TRY(ensure_err(ctx, st));
+    if (n > 1) {
+        TDV_TRY(ensure_lane(ctx));
+        TDV_TRY(ensure(ctx, ctx->planes_b, tdv::fused_plane_bytes(W, H)));
+        TDV_TRY(ensure(ctx, ctx->agg_b, tdv::fused_agg_bytes(W, H, D)));
+        TDV_TRY(ensure(ctx, ctx->agg2_b, tdv::fused_agg_bytes(W, H, D)));
+        if (fp.weighted && ctx->fside.bytes) TDV_TRY(ensure(ctx, ctx->fside_b, ctx->fside.bytes));
+        // the second lane starts after what the call's stream holds
+        TDV_CUDA(cudaEventRecord(ctx->lane_start, st));
+        TDV_CUDA(cudaStreamWaitEvent(ctx->lane_main, ctx->lane_start, 0));
+    }
+    for (int i = 0; i < n; i++) {
+        tdv::FusedArgs a = fused_args(ctx, &left[i], &right[i], D, params, fp, &out[i]);
+        const bool b = (i & 1) != 0;
+        a.planes = b ? ctx->planes_b.ptr : ctx->planes.ptr;
+        a.agg = b ? ctx->agg_b.ptr : ctx->agg.ptr;
+        a.agg2 = b ? ctx->agg2_b.ptr : ctx->agg2.ptr;
+        if (fp.weighted) a.side = (uint32_t*)(b ? ctx->fside_b.ptr : ctx->fside.ptr);
+        a.side_stream = b ? ctx->lane_side : ctx->side;
+        a.fork = b ? ctx->lane_fork : ctx->fork_ev;
+        a.join = b ? ctx->lane_join : ctx->join_ev;
+        TDV_CUDA(tdv::launch_fused(a, b ? ctx->lane_main : st, nullptr));
+    }
+    if (n > 1) {
+        // the call's stream continues once the second lane is done
+        TDV_CUDA(cudaEventRecord(ctx->lane_done, ctx->lane_main));
+        TDV_CUDA(cudaStreamWaitEvent(st, ctx->lane_done, 0));
+    }
+    return TDV_OK;
 }
 
 // ------------------------------------------------------------ batched pairs

@@ -182,6 +182,12 @@ struct tdv_ctx {
     // fused path: side stream and fork/join events of the two pass chains
     cudaStream_t side = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    // fused path over a frame sequence (tdv_stereo_sgm_frames): the second
+    // lane's planes, volumes and side rows, its two streams, its chains'
+    // fork/join events and the events that tie it to the call's stream
+    Buf planes_b, agg_b, agg2_b, fside_b;
+    cudaStream_t lane_main = nullptr, lane_side = nullptr;
+    cudaEvent_t lane_fork = nullptr, lane_join = nullptr, lane_start = nullptr, lane_done = nullptr;
 };
 
 namespace tdv {
