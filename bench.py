@@ -419,6 +419,17 @@ def measure_batch(ctx, dev, reps=3):
         l, r, _, _ = synthetic.pair_sized(w, h, d, synthetic.pair_seed(0, i) % (2 ** 31))
         pairs.append((torch.from_numpy(l).to(dev), torch.from_numpy(r).to(dev), d))
     cells = sum(w * h * d * 8 for (w, h, d) in shapes)
+    # algorithmic bytes of the fused kernels: each pair's 16-bit volume holds
+    # 64 * ceil-to-{1,2,4}(D / 64) disparities per pixel and is touched 14 times
+    # (two first stores, four read-modify-writes, the join's two reads and one
+    # write, the last pass's read), plus the BT planes (34 B per pixel) per pass
+    span = lambda d: 64 if d <= 64 else (128 if d <= 128 else 256)
+    batch_bytes = sum(w * h * (2 * span(d) * 14 + 34 * 8) for (w, h, d) in shapes)
+    peak = 6650.0
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+    except (OSError, KeyError, ValueError):
+        pass
     st = torch.cuda.current_stream()
     lib = _lib.lib()
     prm = _lib.tdv_sgm_params(P1, P2, _lib.P2_CONST, 8, _lib.TABLE_FULL, _lib.SEM_STANDARD)
@@ -475,6 +486,10 @@ def measure_batch(ctx, dev, reps=3):
             "gcells_per_s": cells / (t_graph / 1000.0) / 1e9,
             "per_pair_fused_gcells_per_s": cells / (t_pair / 1000.0) / 1e9,
             "speedup_vs_per_pair_plain": t_plain / t_graph, "speedup_vs_per_pair_fused": t_pair / t_graph,
+            "roofline": {"alg_bytes": batch_bytes, "hbm_floor_ms": batch_bytes / (peak * 1e9) * 1e3,
+                         "batch_frac": batch_bytes / (peak * 1e9) / (t_graph / 1000.0),
+                         "per_pair_fused_frac": batch_bytes / (peak * 1e9) / (t_pair / 1000.0),
+                         "max_speedup_vs_per_pair_fused": t_pair / (batch_bytes / (peak * 1e9) * 1e3)},
             "bit_identical_to_per_pair": equal and plain_equal}
 
 
