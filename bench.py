@@ -616,6 +616,25 @@ def measure_plain(ctx, dev, reps=3):
         del dsi
     out["workload"] = ("tdv_cost (BT, REF_WHD, [0,1] floats) + tdv_sgm (REF table, REF_GPU semantics, "
                        "P2 adjusted, 8 paths) + WTA")
+    # the same stage chain on u8 intensities (the integer domain: P1 = 10,
+    # P2 = 120, reference CPU recurrence and table, WTA + left-right check)
+    # with the DSI as F32 and as the exact 16-bit half-unit DSI
+    l, r, _, _ = synthetic.pair_sized(1920, 1080, 256, 3)
+    l8, r8 = torch.from_numpy(l).to(dev), torch.from_numpy(r).to(dev)
+    ints = {"workload": "1920x1080, D=256, u8 images: tdv_cost BT (HWD) + tdv_sgm (reference CPU recurrence "
+                        "and table, P1 = 10, P2 = 120, 8 paths) + WTA + left-right check; device ms per pair"}
+    for dt in ("f32", "u16"):
+        dsi = torch.empty((1080, 1920, 256), dtype=torch.float32 if dt == "f32" else torch.uint16, device=dev)
+
+        def run_int():
+            ctx.cost(l8, r8, 256, kind="bt", out=dsi)
+            return ctx.sgm(dsi, 10.0, 120.0, table="ref", semantics="ref_cpu", lr=1)
+
+        ints[f"dsi_{dt}_ms"] = _event_ms(run_int, reps, 1, st)
+        ints[f"dsi_{dt}_map"] = run_int()["disp"].clone()
+        del dsi
+    ints["maps_equal"] = bool(torch.equal(ints.pop("dsi_f32_map"), ints.pop("dsi_u16_map")))
+    out["1920x1080_D256_integer_domain"] = ints
     # every stage of the 640x480, D=64 configuration timed alone: the three
     # costs at the configuration's windows (SSD 5x5, NCC 9x9) and the
     # reference's (SSD 7x7, NCC 3x3), 8-path SGM with WTA + left-right check,

@@ -65,7 +65,10 @@ typedef struct {
     void* ptr;        /* device, dense, no padding between pixels */
     int32_t width, height, depth;
     int32_t layout;   /* tdv_layout */
-    int32_t dtype;    /* TDV_F32; the soft-SGM calls also take TDV_F64 */
+    int32_t dtype;    /* TDV_F32; cost DSIs may be TDV_U16 (BT of TDV_U8 images at
+                         scale 1, in half-units: value = 2 * cost, +INF = 0xFFFF,
+                         exact) for tdv_cost, tdv_sgm's cost, tdv_wta and
+                         tdv_dp_scanline; the soft-SGM calls also take TDV_F64 */
 } tdv_volume;
 
 typedef struct {
@@ -85,7 +88,8 @@ typedef struct {
                        (tdvision/crosscorrelation.cu:17-18); ignored for BT */
 } tdv_cost_params;
 
-/* Fills the cost DSI `out` (F32, either layout) from a rectified pair.
+/* Fills the cost DSI `out` (F32, either layout; or U16 for BT of u8 images
+ * at scale 1, else TDV_ERR_UNSUPPORTED) from a rectified pair.
  * Replaces BirchfieldCostRun (tdvision/birchfieldcost.cu:194-212),
  * SSDDevRun (tdvision/ssd.cu:79-114) and CrossCorrelationDevRun
  * (tdvision/crosscorrelation.cu:53-76), i.e. the updateImpl of

@@ -103,7 +103,7 @@ def test_sgm_argument_validation(lib, hctx):
         (_vol(ptr=0), _params(), "null data pointer"),
         (_vol(w=0), _params(), "bad size"),
         (_vol(layout=7), _params(), "bad layout"),
-        (_vol(dt=L.U16), _params(), "dtype"),
+        (_vol(dt=L.F64), _params(), "dtype"),
         (v, _params(paths=6), "paths"),
         (v, _params(table=3), "bad table"),
         (v, _params(semantics=9), "bad semantics"),

@@ -63,9 +63,14 @@ def _raster(t):
     return L.tdv_raster(t.data_ptr(), t.shape[1], t.shape[0], t.stride(0) * size, dt, ch)
 
 
+_U16_TYPES = (torch.uint16, torch.int16)
+
+
 def _volume(t, layout):
-    if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float32:
-        raise TypeError("volumes must be float32 CUDA tensors")
+    """A float32 volume, or a 16-bit cost DSI (uint16 or int16 storage: BT of
+    integer intensities in half-units, 0xFFFF = +INF)."""
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype not in (torch.float32,) + _U16_TYPES:
+        raise TypeError("volumes must be float32 (or 16-bit cost) CUDA tensors")
     if t.dim() != 3 or not t.is_contiguous():
         raise ValueError("volumes must be contiguous 3-d tensors")
     lay = _LAYOUTS[layout]
@@ -73,7 +78,7 @@ def _volume(t, layout):
         H, W, D = t.shape
     else:
         W, H, D = t.shape
-    return L.tdv_volume(t.data_ptr(), W, H, D, lay, L.F32)
+    return L.tdv_volume(t.data_ptr(), W, H, D, lay, L.U16 if t.dtype in _U16_TYPES else L.F32)
 
 
 def _vol_dims(t, layout):
@@ -147,15 +152,17 @@ class Context:
 
     # ---- stages ---------------------------------------------------------
     def cost(self, left, right, max_disp, kind="bt", radius=None, layout="hwd", scale=1.0,
-             out=None):
-        """Matching-cost DSI (BirchfieldCostRun / SSDDevRun / CrossCorrelationDevRun)."""
+             out=None, dtype="f32"):
+        """Matching-cost DSI (BirchfieldCostRun / SSDDevRun / CrossCorrelationDevRun).
+        ``dtype="u16"``: BT of uint8 images at scale 1 as a 16-bit DSI in
+        half-units (0xFFFF = +INF), exact and half the bytes."""
         if radius is None:
             radius = {"bt": 0, "ssd": 3, "ncc": 1}[kind]
         H = min(left.shape[0], right.shape[0])
         W = min(left.shape[1], right.shape[1])
         if out is None:
             shape = (H, W, max_disp) if _LAYOUTS[layout] == L.LAYOUT_HWD else (W, H, max_disp)
-            out = torch.empty(shape, dtype=torch.float32, device=left.device)
+            out = torch.empty(shape, dtype=torch.uint16 if dtype == "u16" else torch.float32, device=left.device)
         li, ri = _image(left, scale), _image(right, scale)
         vol = _volume(out, layout)
         p = L.tdv_cost_params(_COSTS[kind], radius)

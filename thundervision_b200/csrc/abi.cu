@@ -37,7 +37,7 @@ tdv_status check_image(tdv_ctx* ctx, const tdv_image* im, const char* name) {
     return TDV_OK;
 }
 
-tdv_status check_volume(tdv_ctx* ctx, const tdv_volume* v, const char* name) {
+tdv_status check_volume(tdv_ctx* ctx, const tdv_volume* v, const char* name, bool allow_u16 = false) {
     if (!v) return fail(ctx, TDV_ERR_INVALID_ARG, "%s: null volume", name);
     if (!v->ptr) return fail(ctx, TDV_ERR_INVALID_ARG, "%s: null data pointer", name);
     if (v->width <= 0 || v->height <= 0 || v->depth <= 0 || v->width > kMaxSide ||
@@ -46,7 +46,9 @@ tdv_status check_volume(tdv_ctx* ctx, const tdv_volume* v, const char* name) {
                     v->depth);
     if (v->layout != TDV_LAYOUT_REF_WHD && v->layout != TDV_LAYOUT_HWD)
         return fail(ctx, TDV_ERR_INVALID_ARG, "%s: bad layout %d", name, v->layout);
-    if (v->dtype != TDV_F32) return fail(ctx, TDV_ERR_INVALID_ARG, "%s: dtype must be TDV_F32", name);
+    if (v->dtype == TDV_U16 && allow_u16) return TDV_OK;
+    if (v->dtype != TDV_F32)
+        return fail(ctx, TDV_ERR_INVALID_ARG, "%s: dtype must be TDV_F32%s", name, allow_u16 ? " or TDV_U16" : "");
     return TDV_OK;
 }
 
@@ -176,6 +178,7 @@ tdv_status run_sgm(tdv_ctx* ctx, const tdv_volume* cost, const tdv_image* guide,
         TDV_TRY(ensure(ctx, ctx->agg, (size_t)W * H * D * sizeof(float)));
         tdv_volume tmp = *cost;
         tmp.ptr = ctx->agg.ptr;
+        tmp.dtype = TDV_F32;  // the aggregation is float whatever the cost's type
         Sv = tdv::make_vol(tmp);
     }
     TDV_TRY(ensure_schedule(ctx, W, H, p->table, p->paths, st));
@@ -408,6 +411,7 @@ VolArg make_vol(const tdv_volume& v) {
     a.W = v.width;
     a.H = v.height;
     a.D = v.depth;
+    a.u16 = v.dtype == TDV_U16 ? 1 : 0;
     if (v.layout == TDV_LAYOUT_REF_WHD) {
         a.sx = (long long)v.height * v.depth;
         a.sy = v.depth;
@@ -685,12 +689,18 @@ tdv_status tdv_cost(tdv_ctx* ctx, const tdv_image* left, const tdv_image* right,
     if (!ctx) return TDV_ERR_INVALID_ARG;
     TDV_TRY(check_image(ctx, left, "left"));
     TDV_TRY(check_image(ctx, right, "right"));
-    TDV_TRY(check_volume(ctx, out, "out"));
+    TDV_TRY(check_volume(ctx, out, "out", true));
     if (!params) return fail(ctx, TDV_ERR_INVALID_ARG, "null cost params");
     if (params->kind < TDV_COST_BT || params->kind > TDV_COST_NCC)
         return fail(ctx, TDV_ERR_INVALID_ARG, "bad cost kind %d", params->kind);
     if (params->kind != TDV_COST_BT && (params->radius < 0 || params->radius > 15))
         return fail(ctx, TDV_ERR_INVALID_ARG, "window radius %d outside [0,15]", params->radius);
+    // a 16-bit DSI holds BT of integer intensities exactly, in half-units
+    if (out->dtype == TDV_U16 &&
+        (params->kind != TDV_COST_BT || left->dtype != TDV_U8 || right->dtype != TDV_U8 || left->scale != 1.0f ||
+         right->scale != 1.0f))
+        return fail(ctx, TDV_ERR_UNSUPPORTED,
+                    "a TDV_U16 DSI holds BT of TDV_U8 images at scale 1 only (half-units, exact)");
     // The reference sizes the DSI to the smaller of the two images
     // (tdvision/matchingcost.cpp:20-24).
     const int W = std::min(left->width, right->width), H = std::min(left->height, right->height);
@@ -752,7 +762,7 @@ tdv_status tdv_sgm(tdv_ctx* ctx, const tdv_volume* cost, const tdv_image* guide,
                    const tdv_sgm_params* params, tdv_volume* aggreg, tdv_disparity* out,
                    tdv_stream stream) {
     if (!ctx) return TDV_ERR_INVALID_ARG;
-    TDV_TRY(check_volume(ctx, cost, "cost"));
+    TDV_TRY(check_volume(ctx, cost, "cost", true));
     TDV_TRY(check_params(ctx, params));
     TDV_TRY(check_out(ctx, out));
     if (cost->depth > tdv::kMaxDispSgm)
@@ -779,7 +789,7 @@ tdv_status tdv_sgm(tdv_ctx* ctx, const tdv_volume* cost, const tdv_image* guide,
 
 tdv_status tdv_wta(tdv_ctx* ctx, const tdv_volume* vol, tdv_disparity* out, tdv_stream stream) {
     if (!ctx) return TDV_ERR_INVALID_ARG;
-    TDV_TRY(check_volume(ctx, vol, "vol"));
+    TDV_TRY(check_volume(ctx, vol, "vol", true));
     TDV_TRY(check_out(ctx, out));
     if (out->lr_threshold >= 0 || out->disp_right) {
         if (!out->disp) return fail(ctx, TDV_ERR_INVALID_ARG, "left-right check needs out->disp");
@@ -798,7 +808,7 @@ tdv_status tdv_wta(tdv_ctx* ctx, const tdv_volume* vol, tdv_disparity* out, tdv_
 tdv_status tdv_dp_scanline(tdv_ctx* ctx, const tdv_volume* cost, tdv_disparity* out,
                            tdv_stream stream) {
     if (!ctx) return TDV_ERR_INVALID_ARG;
-    TDV_TRY(check_volume(ctx, cost, "cost"));
+    TDV_TRY(check_volume(ctx, cost, "cost", true));
     TDV_TRY(check_out(ctx, out));
     if (cost->depth > tdv::kMaxDispWide)
         return fail(ctx, TDV_ERR_UNSUPPORTED, "DP supports D <= %d (got %d)", tdv::kMaxDispWide,

@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(kThreads) cost_band_kernel(ImgArg L, ImgArg Ri
                 const bool dok = d < D;
                 const int de = dok ? d : D - 1;
                 const int r0 = row * (kTX + D - 1) + (xs - de) - (x0 - (D - 1));
-                float* const op = outp + y * out.sy + d + xs * out.sx;
+                const long long oi = y * out.sy + d + xs * out.sx;
                 float v[P];
 #pragma unroll
                 for (int p = 0; p < P; p++) {
@@ -322,11 +322,25 @@ __global__ void __launch_bounds__(kThreads) cost_band_kernel(ImgArg L, ImgArg Ri
                     const float b = fmaxf(0.0f, fmaxf(__fsub_rn(rI, lIma[p]), __fsub_rn(lImi[p], rI)));
                     v[p] = __fadd_rn(0.0f, fminf(a, b));
                 }
-                if (dok && rows_in && xs - d >= 0) {
+                if (out.u16) {
+                    // 16-bit DSI (integer intensities only): half-units, +INF as 0xFFFF
+                    uint16_t* const op = (uint16_t*)out.ptr + oi;
+                    if (dok && y < H) {
+#pragma unroll
+                        for (int p = 0; p < P; p++) {
+                            const int x = xs + p;
+                            if (x < W)
+                                op[p * out.sx] = (x - d < 0) ? (uint16_t)0xFFFFu
+                                                             : (uint16_t)__float2uint_rn(__fmul_rn(v[p], 2.0f));
+                        }
+                    }
+                } else if (dok && rows_in && xs - d >= 0) {
                     // all P cells in the image and in range: plain stores
+                    float* const op = outp + oi;
 #pragma unroll
                     for (int p = 0; p < P; p++) op[p * out.sx] = v[p];
                 } else if (dok && y < H) {
+                    float* const op = outp + oi;
 #pragma unroll
                     for (int p = 0; p < P; p++) {
                         const int x = xs + p;

@@ -68,6 +68,15 @@ __device__ float ncc_cell(const ImgArg& L, const ImgArg& R, int x, int y, int d,
     return __fsub_rn(1.0f, __fdiv_rn(dom, __fsqrt_rn(__fmul_rn(ls, rs))));
 }
 
+// Cost elements as float: a float DSI as stored; a TDV_U16 DSI holds BT of
+// integer intensities in half-units (every value a multiple of 1/2, so 2v is
+// an integer in [0, 510]), +INF as 0xFFFF: both directions exact.
+__device__ __forceinline__ float cdec(float v) { return v; }
+__device__ __forceinline__ float cdec(uint16_t u) { return u == 0xFFFFu ? CUDART_INF_F : (float)u * 0.5f; }
+__device__ __forceinline__ uint16_t cenc16(float v) {
+    return v == CUDART_INF_F ? (uint16_t)0xFFFFu : (uint16_t)__float2uint_rn(__fmul_rn(v, 2.0f));
+}
+
 // One thread per cell in memory order (disparity fastest), so the DSI stores
 // are fully coalesced whatever the layout.
 __global__ void cost_kernel(ImgArg L, ImgArg R, int kind, int radius, VolArg out, int xmajor) {
@@ -84,7 +93,8 @@ __global__ void cost_kernel(ImgArg L, ImgArg R, int kind, int radius, VolArg out
         else if (x - d < 0) v = CUDART_INF_F;
         else if (kind == TDV_COST_BT) v = bt_cell(L, R, x, y, d);
         else v = ssd_cell(L, R, x, y, d, radius);
-        ((float*)out.ptr)[i] = v;
+        if (out.u16) ((uint16_t*)out.ptr)[i] = cenc16(v);
+        else ((float*)out.ptr)[i] = v;
     }
 }
 
@@ -107,7 +117,7 @@ __device__ __forceinline__ float smin(float a, float b) { return (b < a) ? b : a
 // the previous group for lane 0) and lane l+1 (lane 0 of the next group for
 // lane 31).  SEM and FIRST (the pass that writes S instead of adding to it)
 // are compile-time, so a step carries no branch on either.
-template <int NPL, int SEM, bool FIRST>
+template <int NPL, int SEM, bool FIRST, typename CT>
 __global__ void __launch_bounds__(128) sgm_pass_kernel(SgmArgs a, const Walk* __restrict__ walks,
                                                        int nwalks, int dx, int dy) {
     const int lane = threadIdx.x & 31;
@@ -120,7 +130,7 @@ __global__ void __launch_bounds__(128) sgm_pass_kernel(SgmArgs a, const Walk* __
     const int mlim = refcpu ? D - 1 : D;  // REF_CPU scans {sentinel, L(0..D-2)}
     const int src_up = (lane + 31) & 31, src_dn = (lane + 1) & 31;
     // the walk's cells: base + t * stride
-    const float* const cbase = (const float*)a.C.ptr + wk.sx * a.C.sx + wk.sy * a.C.sy;
+    const CT* const cbase = (const CT*)a.C.ptr + wk.sx * a.C.sx + wk.sy * a.C.sy;
     float* const sbase = (float*)a.S.ptr + wk.sx * a.S.sx + wk.sy * a.S.sy;
     const long long cstride = dx * a.C.sx + dy * a.C.sy, sstride = dx * a.S.sx + dy * a.S.sy;
 
@@ -129,7 +139,7 @@ __global__ void __launch_bounds__(128) sgm_pass_kernel(SgmArgs a, const Walk* __
 #pragma unroll
     for (int j = 0; j < NPL; j++) {
         const int d = lane + 32 * j;
-        const float c = d < D ? cbase[d] : CUDART_INF_F;
+        const float c = d < D ? cdec(cbase[d]) : CUDART_INF_F;
         if (d < mlim) mo = min(mo, ford(c));
         if (d < D) {
             if (refcpu || FIRST) {
@@ -168,12 +178,12 @@ __global__ void __launch_bounds__(128) sgm_pass_kernel(SgmArgs a, const Walk* __
     constexpr int K = NPL <= 2 ? 8 : 4;
     float cr[K][NPL], sr[K][NPL];
     auto issue = [&](int t, float (&cs)[NPL], float (&ss)[NPL]) {
-        const float* cq = cbase + t * cstride;
+        const CT* cq = cbase + t * cstride;
         const float* sq = sbase + t * sstride;
 #pragma unroll
         for (int j = 0; j < NPL; j++) {
             const int d = lane + 32 * j;
-            cs[j] = d < D ? cq[d] : CUDART_INF_F;
+            cs[j] = d < D ? cdec(cq[d]) : CUDART_INF_F;
             ss[j] = (!FIRST && d < D) ? sq[d] : 0.0f;
         }
     };
@@ -264,7 +274,7 @@ __global__ void sgm_deferred_kernel(SgmArgs a, const Walk* __restrict__ walks, c
     }
 }
 
-template <int NPL>
+template <int NPL, typename CT>
 cudaError_t run_passes(const SgmArgs& a, const PassSchedule& sch, cudaStream_t st, Timer* tm) {
     const int wpb = 4;
     for (size_t p = 0; p < sch.passes.size(); p++) {
@@ -272,12 +282,12 @@ cudaError_t run_passes(const SgmArgs& a, const PassSchedule& sch, cudaStream_t s
         const int nw = (int)ps.count;
         const int blocks = (nw + wpb - 1) / wpb;
         const bool first = p == 0;
-        auto kern = a.sem == TDV_SEM_REF_CPU ? (first ? sgm_pass_kernel<NPL, TDV_SEM_REF_CPU, true>
-                                                      : sgm_pass_kernel<NPL, TDV_SEM_REF_CPU, false>)
-                    : a.sem == TDV_SEM_REF_GPU ? (first ? sgm_pass_kernel<NPL, TDV_SEM_REF_GPU, true>
-                                                        : sgm_pass_kernel<NPL, TDV_SEM_REF_GPU, false>)
-                    : (first ? sgm_pass_kernel<NPL, TDV_SEM_STANDARD, true>
-                             : sgm_pass_kernel<NPL, TDV_SEM_STANDARD, false>);
+        auto kern = a.sem == TDV_SEM_REF_CPU ? (first ? sgm_pass_kernel<NPL, TDV_SEM_REF_CPU, true, CT>
+                                                      : sgm_pass_kernel<NPL, TDV_SEM_REF_CPU, false, CT>)
+                    : a.sem == TDV_SEM_REF_GPU ? (first ? sgm_pass_kernel<NPL, TDV_SEM_REF_GPU, true, CT>
+                                                        : sgm_pass_kernel<NPL, TDV_SEM_REF_GPU, false, CT>)
+                    : (first ? sgm_pass_kernel<NPL, TDV_SEM_STANDARD, true, CT>
+                             : sgm_pass_kernel<NPL, TDV_SEM_STANDARD, false, CT>);
         kern<<<blocks, wpb * 32, 0, st>>>(a, sch.d_walks + ps.first, nw, ps.dx, ps.dy);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -301,18 +311,19 @@ __device__ __forceinline__ void argmin_merge(uint32_t& vo, int& vd, uint32_t o2,
 
 // Winner-take-all, one warp per pixel, strict '<' so the lowest d wins ties
 // (tdvision/wtacpu.cpp:14-39); NaN never wins; no finite value -> d = 0.
+template <typename T>
 __global__ void wta_kernel(VolArg V, uint16_t* disp, float* disp_norm) {
     const int lane = threadIdx.x & 31;
     const size_t npix = (size_t)V.W * V.H;
-    const float* base = (const float*)V.ptr;
+    const T* base = (const T*)V.ptr;
     for (size_t p = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < npix;
          p += ((size_t)gridDim.x * blockDim.x) >> 5) {
         const int x = (int)(p % V.W), y = (int)(p / V.W);
-        const float* vp = base + x * V.sx + y * V.sy;
+        const T* vp = base + x * V.sx + y * V.sy;
         uint32_t bo = ford(CUDART_INF_F);
         int bd = 0x7FFFFFFF;
         for (int d = lane; d < V.D; d += 32) {
-            const float v = vp[d];
+            const float v = cdec(vp[d]);
             if (v < CUDART_INF_F) argmin_merge(bo, bd, ford(v), d);
         }
 #pragma unroll
@@ -388,6 +399,7 @@ __global__ void __launch_bounds__(256) wta_thread_kernel(VolArg V, uint16_t* dis
 // (t + 2 dd) mod 32.  Each thread keeps its right pixel's best (cost, d) in
 // increasing d.  Then the row's left pixels are checked as in lr_kernel.
 constexpr int kLrTile = 256;
+template <typename T>
 __global__ void __launch_bounds__(256) lr_tiled_kernel(VolArg S, uint16_t* dispL, float* disp_norm,
                                                        uint16_t* dispR, int thr) {
     extern __shared__ float lsm[];
@@ -395,7 +407,7 @@ __global__ void __launch_bounds__(256) lr_tiled_kernel(VolArg S, uint16_t* dispL
     uint16_t* sdr = reinterpret_cast<uint16_t*>(lsm + (kLrTile + 32) * 33);  // [W]
     const int y = blockIdx.x;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const float* base = (const float*)S.ptr;
+    const T* base = (const T*)S.ptr;
     const int W = S.W, D = S.D;
     for (int xr0 = 0; xr0 < W; xr0 += kLrTile) {
         uint32_t bo = ford(CUDART_INF_F);
@@ -405,7 +417,7 @@ __global__ void __launch_bounds__(256) lr_tiled_kernel(VolArg S, uint16_t* dispL
             __syncthreads();
             for (int i = warp; i < kLrTile + 32; i += 8) {
                 const int x = xr0 + c + i, d = c + lane;
-                tile[i * 33 + lane] = (x < W && d < D) ? base[x * S.sx + y * S.sy + d] : CUDART_INF_F;
+                tile[i * 33 + lane] = (x < W && d < D) ? cdec(base[x * S.sx + y * S.sy + d]) : CUDART_INF_F;
             }
             __syncthreads();
 #pragma unroll 8
@@ -444,16 +456,17 @@ __global__ void __launch_bounds__(256) lr_tiled_kernel(VolArg S, uint16_t* dispL
 // Left-right check, one block per row.  dR(xr) = argmin_d S(xr+d, y, d) over
 // xr+d < W; a left pixel is rejected (0xFFFF, d/D = -1) when x-dL < 0 or
 // |dL - dR(x-dL)| > thr.
+template <typename T>
 __global__ void lr_kernel(VolArg S, uint16_t* dispL, float* disp_norm, uint16_t* dispR, int thr) {
     extern __shared__ uint16_t sdr[];
     const int y = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const float* base = (const float*)S.ptr;
+    const T* base = (const T*)S.ptr;
     for (int xr = warp; xr < S.W; xr += nw) {
         uint32_t bo = ford(CUDART_INF_F);
         int bd = 0x7FFFFFFF;
         for (int d = lane; d < S.D && xr + d < S.W; d += 32) {
-            const float v = base[(xr + d) * S.sx + y * S.sy + d];
+            const float v = cdec(base[(xr + d) * S.sx + y * S.sy + d]);
             if (v < CUDART_INF_F) argmin_merge(bo, bd, ford(v), d);
         }
 #pragma unroll
@@ -487,7 +500,7 @@ __global__ void lr_kernel(VolArg S, uint16_t* dispL, float* disp_norm, uint16_t*
 // columns of the next 4 steps are in flight in a register ring, and the
 // backtrack stages the codes of CW columns at a time in shared memory with
 // the whole warp, so lane 0's dependent chain reads shared memory.
-template <int NPL>
+template <int NPL, typename T>
 __global__ void __launch_bounds__(128) dp_kernel(VolArg C, uint8_t* codes, uint16_t* disp,
                                                  float* disp_norm) {
     constexpr int CW = NPL <= 8 ? 32 : 256 / NPL;  // backtrack columns per stage
@@ -499,24 +512,24 @@ __global__ void __launch_bounds__(128) dp_kernel(VolArg C, uint8_t* codes, uint1
     uint8_t* const stage = stage_all[wib];
     int* const zs = zs_all[wib];
     const int D = C.D, W = C.W;
-    const float* base = (const float*)C.ptr;
+    const T* base = (const T*)C.ptr;
     uint8_t* crow = codes + (size_t)y * W * D;
     const int src_up = (lane + 31) & 31, src_dn = (lane + 1) & 31;
     float A[NPL];
 #pragma unroll
     for (int j = 0; j < NPL; j++) {
         const int d = lane + 32 * j;
-        A[j] = d < D ? base[y * C.sy + d] : CUDART_INF_F;
+        A[j] = d < D ? cdec(base[y * C.sy + d]) : CUDART_INF_F;
         if (d < D) crow[d] = 1;
     }
     constexpr int K = NPL >= 16 ? 2 : 4;
     float cr[K][NPL];
     auto issue = [&](int x, float (&cs)[NPL]) {
-        const float* cp = base + x * C.sx + y * C.sy;
+        const T* cp = base + x * C.sx + y * C.sy;
 #pragma unroll
         for (int j = 0; j < NPL; j++) {
             const int d = lane + 32 * j;
-            cs[j] = d < D ? cp[d] : 0.0f;
+            cs[j] = d < D ? cdec(cp[d]) : 0.0f;
         }
     };
 #pragma unroll
@@ -653,18 +666,26 @@ cudaError_t launch_cost(const ImgArg& L, const ImgArg& R, int kind, int radius, 
 
 cudaError_t launch_sgm_passes(const SgmArgs& a, const PassSchedule& sch, cudaStream_t st, Timer* tm) {
     const int D = a.C.D;
-    if (D <= 32) return run_passes<1>(a, sch, st, tm);
-    if (D <= 64) return run_passes<2>(a, sch, st, tm);
-    if (D <= 128) return run_passes<4>(a, sch, st, tm);
-    return run_passes<8>(a, sch, st, tm);
+    if (a.C.u16) {
+        if (D <= 32) return run_passes<1, uint16_t>(a, sch, st, tm);
+        if (D <= 64) return run_passes<2, uint16_t>(a, sch, st, tm);
+        if (D <= 128) return run_passes<4, uint16_t>(a, sch, st, tm);
+        return run_passes<8, uint16_t>(a, sch, st, tm);
+    }
+    if (D <= 32) return run_passes<1, float>(a, sch, st, tm);
+    if (D <= 64) return run_passes<2, float>(a, sch, st, tm);
+    if (D <= 128) return run_passes<4, float>(a, sch, st, tm);
+    return run_passes<8, float>(a, sch, st, tm);
 }
 
 cudaError_t launch_wta(const VolArg& V, uint16_t* disp, float* disp_norm, cudaStream_t st, Timer* tm) {
     const size_t npix = (size_t)V.W * V.H;
-    if ((V.D & 3) == 0 && ((uintptr_t)V.ptr & 15) == 0)
+    if (V.u16)
+        wta_kernel<uint16_t><<<grid_for(npix * 32, 256), 256, 0, st>>>(V, disp, disp_norm);
+    else if ((V.D & 3) == 0 && ((uintptr_t)V.ptr & 15) == 0)
         wta_thread_kernel<<<grid_for(npix, 256), 256, 0, st>>>(V, disp, disp_norm, V.sx > V.sy ? 1 : 0);
     else
-        wta_kernel<<<grid_for(npix * 32, 256), 256, 0, st>>>(V, disp, disp_norm);
+        wta_kernel<float><<<grid_for(npix * 32, 256), 256, 0, st>>>(V, disp, disp_norm);
     if (tm) tm->mark("wta");
     return cudaGetLastError();
 }
@@ -672,10 +693,13 @@ cudaError_t launch_wta(const VolArg& V, uint16_t* disp, float* disp_norm, cudaSt
 cudaError_t launch_lr(const VolArg& S, uint16_t* dispL, float* disp_norm, uint16_t* dispR, int thr,
                       cudaStream_t st, Timer* tm) {
     const size_t tiled = (size_t)(kLrTile + 32) * 33 * sizeof(float) + (size_t)S.W * sizeof(uint16_t);
-    if (tiled <= 48 * 1024)
-        lr_tiled_kernel<<<S.H, 256, tiled, st>>>(S, dispL, disp_norm, dispR, thr);
-    else
-        lr_kernel<<<S.H, 256, S.W * sizeof(uint16_t), st>>>(S, dispL, disp_norm, dispR, thr);
+    if (tiled <= 48 * 1024) {
+        if (S.u16) lr_tiled_kernel<uint16_t><<<S.H, 256, tiled, st>>>(S, dispL, disp_norm, dispR, thr);
+        else lr_tiled_kernel<float><<<S.H, 256, tiled, st>>>(S, dispL, disp_norm, dispR, thr);
+    } else {
+        if (S.u16) lr_kernel<uint16_t><<<S.H, 256, S.W * sizeof(uint16_t), st>>>(S, dispL, disp_norm, dispR, thr);
+        else lr_kernel<float><<<S.H, 256, S.W * sizeof(uint16_t), st>>>(S, dispL, disp_norm, dispR, thr);
+    }
     if (tm) tm->mark("lr_check");
     return cudaGetLastError();
 }
@@ -686,12 +710,21 @@ cudaError_t launch_dp(const VolArg& C, uint16_t* disp, float* disp_norm, void* c
     const int blocks = (C.H + 3) / 4;
     const int D = C.D;
     uint8_t* cd = (uint8_t*)codes;
-    if (D <= 32) dp_kernel<1><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
-    else if (D <= 64) dp_kernel<2><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
-    else if (D <= 128) dp_kernel<4><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
-    else if (D <= 256) dp_kernel<8><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
-    else if (D <= 512) dp_kernel<16><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
-    else dp_kernel<32><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+    if (C.u16) {
+        if (D <= 32) dp_kernel<1, uint16_t><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+        else if (D <= 64) dp_kernel<2, uint16_t><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+        else if (D <= 128) dp_kernel<4, uint16_t><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+        else if (D <= 256) dp_kernel<8, uint16_t><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+        else if (D <= 512) dp_kernel<16, uint16_t><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+        else dp_kernel<32, uint16_t><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+    } else {
+        if (D <= 32) dp_kernel<1, float><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+        else if (D <= 64) dp_kernel<2, float><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+        else if (D <= 128) dp_kernel<4, float><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+        else if (D <= 256) dp_kernel<8, float><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+        else if (D <= 512) dp_kernel<16, float><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+        else dp_kernel<32, float><<<blocks, 128, 0, st>>>(C, cd, disp, disp_norm);
+    }
     if (tm) tm->mark("dp_scanline");
     return cudaGetLastError();
 }

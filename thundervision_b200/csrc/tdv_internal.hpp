@@ -214,6 +214,7 @@ struct VolArg {
     void* ptr;
     int W, H, D;
     long long sx, sy;  // element strides of the pixel (x, y)
+    int u16 = 0;       // 1: TDV_U16 cost in half-units (0xFFFF = +INF), else float elements
 };
 
 VolArg make_vol(const tdv_volume& v);
