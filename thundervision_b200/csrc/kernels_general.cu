@@ -497,7 +497,7 @@ __global__ void lr_kernel(VolArg S, uint16_t* dispL, float* disp_norm, uint16_t*
 // tdvision/dynamicprog.cu:68-101 backtrack).  Choice codes (1 byte per cell,
 // -1/0/+1 stored as 0/1/2) go to scratch in [y][x][d] order.  Lane l holds
 // disparities l, l+32, ... (whole-line loads of C and stores of codes), the C
-// columns of the next 4 steps are in flight in a register ring, and the
+// columns of the next steps are in flight in a register ring, and the
 // backtrack stages the codes of CW columns at a time in shared memory with
 // the whole warp, so lane 0's dependent chain reads shared memory.
 template <int NPL, typename T>
@@ -522,7 +522,10 @@ __global__ void __launch_bounds__(128) dp_kernel(VolArg C, uint8_t* codes, uint1
         A[j] = d < D ? cdec(base[y * C.sy + d]) : CUDART_INF_F;
         if (d < D) crow[d] = 1;
     }
-    constexpr int K = NPL >= 16 ? 2 : 4;
+    // columns in flight: a row of D <= 64 has so little work per step that
+    // 12 columns of loads ahead are needed to cover their latency (640x480
+    // D=64: 0.19 -> 0.13 ms); wider rows keep their registers for the state
+    constexpr int K = NPL <= 2 ? 12 : (NPL >= 16 ? 2 : 4);
     float cr[K][NPL];
     auto issue = [&](int x, float (&cs)[NPL]) {
         const T* cp = base + x * C.sx + y * C.sy;
