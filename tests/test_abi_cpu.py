@@ -153,6 +153,47 @@ def test_other_entry_points_validate(lib, hctx):
     assert lib.tdv_stereo_sgm(hctx, B(_img(w=20000)), B(ri), 16, B(_params()), B(o), None) == L.TDV_ERR_INVALID_ARG
 
 
+def test_frame_sequence_validation(lib, hctx):
+    """tdv_stereo_sgm_frames rejects bad sequences before any CUDA call."""
+    n = 3
+    ls = (L.tdv_image * n)(*[_img() for _ in range(n)])
+    rs = (L.tdv_image * n)(*[_img() for _ in range(n)])
+    os_ = (L.tdv_disparity * n)(*[_out() for _ in range(n)])
+    f = lib.tdv_stereo_sgm_frames
+    assert f(None, n, ls, rs, 16, B(_params()), os_, None) == L.TDV_ERR_INVALID_ARG
+    assert f(hctx, 0, ls, rs, 16, B(_params()), os_, None) == L.TDV_ERR_INVALID_ARG
+    assert f(hctx, n, None, rs, 16, B(_params()), os_, None) == L.TDV_ERR_INVALID_ARG
+    assert f(hctx, n, ls, rs, 300, B(_params()), os_, None) == L.TDV_ERR_UNSUPPORTED
+    assert f(hctx, n, ls, rs, 16, B(_params(paths=5)), os_, None) == L.TDV_ERR_INVALID_ARG
+    # a frame of another size
+    odd = (L.tdv_image * n)(_img(), _img(w=10), _img())
+    assert f(hctx, n, odd, rs, 16, B(_params()), os_, None) == L.TDV_ERR_INVALID_ARG
+    assert "frame 1" in lib.tdv_last_error_string(hctx).decode()
+    # outside the fused path: float images, a P2 that is not a multiple of 1/2
+    fl = (L.tdv_image * n)(*[_img(dt=L.F32) for _ in range(n)])
+    assert f(hctx, n, fl, fl, 16, B(_params()), os_, None) == L.TDV_ERR_UNSUPPORTED
+    assert f(hctx, n, ls, rs, 16, B(_params(p2=120.3)), os_, None) == L.TDV_ERR_UNSUPPORTED
+    # an output with every pointer null
+    bad = (L.tdv_disparity * n)(_out(), L.tdv_disparity(None, None, None, -1), _out())
+    assert f(hctx, n, ls, rs, 16, B(_params()), bad, None) == L.TDV_ERR_INVALID_ARG
+
+
+def test_u16_dsi_validation(lib, hctx):
+    """A 16-bit DSI: BT of u8 images at scale 1 only; never an aggregation."""
+    li, ri = _img(), _img()
+    v16 = _vol(dt=L.U16)
+    assert lib.tdv_cost(hctx, B(li), B(ri), B(L.tdv_cost_params(L.COST_SSD, 1)), B(v16),
+                        None) == L.TDV_ERR_UNSUPPORTED
+    assert lib.tdv_cost(hctx, B(_img(scale=0.5)), B(_img(scale=0.5)), B(L.tdv_cost_params(L.COST_BT, 0)), B(v16),
+                        None) == L.TDV_ERR_UNSUPPORTED
+    assert lib.tdv_cost(hctx, B(_img(dt=L.F32)), B(_img(dt=L.F32)), B(L.tdv_cost_params(L.COST_BT, 0)), B(v16),
+                        None) == L.TDV_ERR_UNSUPPORTED
+    assert lib.tdv_sgm(hctx, B(v16), None, B(_params()), B(_vol(dt=L.U16)), B(_out()),
+                       None) == L.TDV_ERR_INVALID_ARG
+    assert "aggreg" in lib.tdv_last_error_string(hctx).decode()
+    assert lib.tdv_volume_bytes(640, 480, 64, L.U16) == 640 * 480 * 64 * 2
+
+
 def test_injected_allocator_failure(lib, hctx):
     calls = []
 
