@@ -325,7 +325,10 @@ __global__ void __launch_bounds__(kThreads) cost_band_kernel(ImgArg L, ImgArg Ri
                 if (out.u16) {
                     // 16-bit DSI (integer intensities only): half-units, +INF as 0xFFFF
                     uint16_t* const op = (uint16_t*)out.ptr + oi;
-                    if (dok && y < H) {
+                    if (dok && rows_in && xs - d >= 0) {
+#pragma unroll
+                        for (int p = 0; p < P; p++) op[p * out.sx] = (uint16_t)__float2uint_rn(__fmul_rn(v[p], 2.0f));
+                    } else if (dok && y < H) {
 #pragma unroll
                         for (int p = 0; p < P; p++) {
                             const int x = xs + p;

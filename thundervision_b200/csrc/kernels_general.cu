@@ -73,6 +73,12 @@ __device__ float ncc_cell(const ImgArg& L, const ImgArg& R, int x, int y, int d,
 // an integer in [0, 510]), +INF as 0xFFFF: both directions exact.
 __device__ __forceinline__ float cdec(float v) { return v; }
 __device__ __forceinline__ float cdec(uint16_t u) { return u == 0xFFFFu ? CUDART_INF_F : (float)u * 0.5f; }
+template <typename T>
+__device__ __forceinline__ T cinf();
+template <>
+__device__ __forceinline__ float cinf<float>() { return CUDART_INF_F; }
+template <>
+__device__ __forceinline__ uint16_t cinf<uint16_t>() { return (uint16_t)0xFFFFu; }
 __device__ __forceinline__ uint16_t cenc16(float v) {
     return v == CUDART_INF_F ? (uint16_t)0xFFFFu : (uint16_t)__float2uint_rn(__fmul_rn(v, 2.0f));
 }
@@ -176,14 +182,17 @@ __global__ void __launch_bounds__(128) sgm_pass_kernel(SgmArgs a, const Walk* __
     // cells are distinct along a walk and across the walks of a pass, so a
     // prefetched S is never stale.
     constexpr int K = NPL <= 2 ? 8 : 4;
-    float cr[K][NPL], sr[K][NPL];
-    auto issue = [&](int t, float (&cs)[NPL], float (&ss)[NPL]) {
+    // the ring holds the cost elements as loaded (decoded where they are
+    // used, so that a 16-bit load does not have to land before the next issue)
+    CT cr[K][NPL];
+    float sr[K][NPL];
+    auto issue = [&](int t, CT (&cs)[NPL], float (&ss)[NPL]) {
         const CT* cq = cbase + t * cstride;
         const float* sq = sbase + t * sstride;
 #pragma unroll
         for (int j = 0; j < NPL; j++) {
             const int d = lane + 32 * j;
-            cs[j] = d < D ? cdec(cq[d]) : CUDART_INF_F;
+            cs[j] = d < D ? cq[d] : cinf<CT>();
             ss[j] = (!FIRST && d < D) ? sq[d] : 0.0f;
         }
     };
@@ -224,7 +233,7 @@ __global__ void __launch_bounds__(128) sgm_pass_kernel(SgmArgs a, const Walk* __
                 float mn;
                 if (refcpu) mn = smin(L[j], smin(b, smin(e, mp2)));
                 else mn = fminf(L[j], fminf(b, fminf(e, mp2)));
-                float v = __fsub_rn(__fadd_rn(cr[k][j], mn), m);
+                float v = __fsub_rn(__fadd_rn(cdec(cr[k][j]), mn), m);
                 if (d >= D) v = CUDART_INF_F;
                 Ln[j] = v;
                 if (d < mlim) mn_o = min(mn_o, ford(v));
@@ -526,13 +535,13 @@ __global__ void __launch_bounds__(128) dp_kernel(VolArg C, uint8_t* codes, uint1
     // 12 columns of loads ahead are needed to cover their latency (640x480
     // D=64: 0.19 -> 0.13 ms); wider rows keep their registers for the state
     constexpr int K = NPL <= 2 ? 12 : (NPL >= 16 ? 2 : 4);
-    float cr[K][NPL];
-    auto issue = [&](int x, float (&cs)[NPL]) {
+    T cr[K][NPL];  // as loaded, decoded where used
+    auto issue = [&](int x, T (&cs)[NPL]) {
         const T* cp = base + x * C.sx + y * C.sy;
 #pragma unroll
         for (int j = 0; j < NPL; j++) {
             const int d = lane + 32 * j;
-            cs[j] = d < D ? cdec(cp[d]) : 0.0f;
+            cs[j] = d < D ? cp[d] : T(0);
         }
     };
 #pragma unroll
@@ -562,7 +571,7 @@ __global__ void __launch_bounds__(128) dp_kernel(VolArg C, uint8_t* codes, uint1
                 else if (c2 < c3) { m = c2; code = 1; }
                 else { m = c3; code = 2; }
                 if (d < D) {
-                    An[j] = __fadd_rn(cr[k][j], m);
+                    An[j] = __fadd_rn(cdec(cr[k][j]), m);
                     crow[(size_t)x * D + d] = code;
                 } else {
                     An[j] = CUDART_INF_F;
