@@ -60,6 +60,10 @@ SEMANTICS = {
     "standard": {"kw": {"semantics": "standard", "table": "full"}, "orc": (0, 0), "var": 0,
                  "recurrence": "standard (S += C at path starts, min over all d)",
                  "table": "full (every line walked once each way)"},
+    "reference_gpu": {"kw": {"semantics": "ref_gpu", "table": "ref"}, "orc": (2, 1), "var": 1,
+                      "recurrence": "reference GPU (tdvision/semiglobal.cu:283-466 without its race: "
+                                    "the second step from C + P1)",
+                      "table": "reference (tdvision/semiglobal.cu:57-230, stale diagonal ends)"},
 }
 
 
@@ -1184,29 +1188,32 @@ def run_ours(args):
     if sharded is not None:
         line["batch_sharded"] = sharded
     if not args.no_extras:
-        # the other recurrence / table on the same frames and kernels
-        other = "standard" if args.semantics == "reference" else "reference"
+        # the other recurrences / tables on the same frames and kernels
+        for other in [o for o in SEMANTICS if o != args.semantics]:
+            try:
+                oms, okern = time_frames(ctx, dev_frames, SEMANTICS[other]["kw"], args.steps, flush, st)
+                okw = SEMANTICS[other]["kw"]
+                oouts = ctx.stereo_sgm_frames(seq_l, seq_r, D, P1, P2, paths=PATHS, lr=LR, **okw)
+                torch.cuda.synchronize()
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                ctx.stereo_sgm_frames(seq_l, seq_r, D, P1, P2, paths=PATHS, lr=LR, outs=oouts, **okw)
+                e1.record(st)
+                e1.synchronize()
+                sms = e0.elapsed_time(e1) / args.steps
+                line[f"semantics_{other}"] = {"recurrence": SEMANTICS[other]["recurrence"],
+                                              "path_table": SEMANTICS[other]["table"],
+                                              "fps": 1000.0 / sms, "ms_per_step": sms,
+                                              "frame_alg_roofline_frac": frame_own / (sms / 1000.0) / 1e9 / peak,
+                                              "single_frame": {"fps": 1000.0 / oms, "ms_per_frame": oms},
+                                              "kernel_avg_ms": okern}
+            except Exception as exc:
+                line[f"semantics_{other}"] = {"error": f"{type(exc).__name__}: {exc}"}
         try:
-            oms, okern = time_frames(ctx, dev_frames, SEMANTICS[other]["kw"], args.steps, flush, st)
-            okw = SEMANTICS[other]["kw"]
-            oouts = ctx.stereo_sgm_frames(seq_l, seq_r, D, P1, P2, paths=PATHS, lr=LR, **okw)
-            torch.cuda.synchronize()
-            flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(st)
-            ctx.stereo_sgm_frames(seq_l, seq_r, D, P1, P2, paths=PATHS, lr=LR, outs=oouts, **okw)
-            e1.record(st)
-            e1.synchronize()
-            sms = e0.elapsed_time(e1) / args.steps
-            line[f"semantics_{other}"] = {"recurrence": SEMANTICS[other]["recurrence"],
-                                          "path_table": SEMANTICS[other]["table"],
-                                          "fps": 1000.0 / sms, "ms_per_step": sms,
-                                          "frame_alg_roofline_frac": frame_own / (sms / 1000.0) / 1e9 / peak,
-                                          "single_frame": {"fps": 1000.0 / oms, "ms_per_frame": oms},
-                                          "kernel_avg_ms": okern}
             line["reference_literal"] = measure_reference_literal(ctx, dev, dev_frames, flush)
         except Exception as exc:
-            line[f"semantics_{other}"] = {"error": f"{type(exc).__name__}: {exc}"}
+            line["reference_literal"] = {"error": f"{type(exc).__name__}: {exc}"}
         try:
             line["configs"] = measure_configs(ctx, dev, args.semantics)
         except Exception as exc:
