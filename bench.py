@@ -405,6 +405,40 @@ def _event_ms(fn, reps, warm, st):
     return e0.elapsed_time(e1) / reps
 
 
+def batch_trace_summary(tr, shapes, per_sm):
+    """Where one persistent batch run spends its block-time, from the per-item
+    trace (taken, dependency met, ended, smid << 32 | pair * 16 + pass): work,
+    dependency waits (per pass), the gaps a block spends between items, and
+    the tail each SM idles after its last item (per_sm blocks per SM take
+    items in turn; the tail is counted per SM); the time of the items of the
+    pairs below 0.25 Mpixel."""
+    import numpy as np
+    t = tr.numpy().astype(np.int64)
+    take, go, end = t[:, 0], t[:, 1], t[:, 2]
+    ok = (take > 0) & (go >= take) & (end >= go)
+    take, go, end, info = take[ok], go[ok], end[ok], t[ok, 3]
+    sm = info >> 32
+    pp = info & 0xFFFFFFFF
+    pair, ps = pp >> 4, pp & 15
+    t0, t1 = take.min(), end.max()
+    span = float(t1 - t0)
+    slots = len(np.unique(sm)) * per_sm
+    busy = float((end - go).sum())
+    wait = float((go - take).sum())
+    last_end = {}
+    for s_, e_ in zip(sm, end):
+        last_end[s_] = max(last_end.get(s_, 0), e_)
+    tail = float(sum(t1 - e for e in last_end.values())) * per_sm
+    total = span * slots
+    small = np.array([w * h < 250000 for (w, h, d) in shapes])[pair]
+    names = ["prep", "V+", "V-", "D1+", "D1-", "D2+", "D2-", "H+", "H-"]
+    return {"span_ms": span / 1e6, "block_slots": int(slots),
+            "work_frac": busy / total, "dependency_wait_frac": wait / total, "tail_idle_frac": tail / total,
+            "other_frac": max(0.0, 1.0 - (busy + wait + tail) / total),
+            "wait_ms_by_pass": {names[p]: float((go - take)[ps == p].sum()) / 1e6 for p in range(9)},
+            "small_pairs_work_frac": float((end - go)[small].sum()) / max(busy, 1.0)}
+
+
 def measure_batch(ctx, dev, reps=3):
     """Uneven batch: 64 seeded pairs, W ~ U[320,1920], H ~ U[240,1080] (multiples
     of 16), D in {32,64,128,256}; BT + SGM-8 + WTA.  One graph-captured
@@ -480,6 +514,7 @@ def measure_batch(ctx, dev, reps=3):
     b.status()
     equal = all(torch.equal(o["disp"], ref) for o, ref in zip(b.outputs, fused_ref))
     n_items = b.work_queue()[1]
+    trace = batch_trace_summary(b.trace(), shapes, int(tiles.get("ctas_per_sm", 1)) if isinstance(tiles, dict) else 1)
     b.close()
     return {"workload": "64 pairs, W~U[320,1920], H~U[240,1080] (x16), D in {32,64,128,256}, "
                         "BT + SGM-8 + WTA, seed 0",
@@ -494,7 +529,7 @@ def measure_batch(ctx, dev, reps=3):
                          "batch_frac": batch_bytes / (peak * 1e9) / (t_graph / 1000.0),
                          "per_pair_fused_frac": batch_bytes / (peak * 1e9) / (t_pair / 1000.0),
                          "max_speedup_vs_per_pair_fused": t_pair / (batch_bytes / (peak * 1e9) * 1e3)},
-            "bit_identical_to_per_pair": equal and plain_equal}
+            "bit_identical_to_per_pair": equal and plain_equal, "trace": trace}
 
 
 def measure_batch_sharded(ctx, dev, rank, world, reps=3):

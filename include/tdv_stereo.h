@@ -260,6 +260,12 @@ tdv_status tdv_batch_graph_launch(tdv_batch* batch, tdv_stream stream);
 tdv_status tdv_batch_status(tdv_batch* batch, tdv_stream stream);
 /* Bounded-wait limit for the kernel's dependency waits (default 2 s). */
 tdv_status tdv_batch_set_wait_limit(tdv_batch* batch, double seconds);
+/* Diagnostic trace of the runs that follow: `trace` (device memory, at least
+ * 4 * n_items 64-bit words, or NULL to stop) receives per queue item the
+ * global timer (ns) when a block took it, when its dependency was met and
+ * when it ended, and smid << 32 | (pair * 16 + pass).  Where the persistent kernel
+ * waits and where it idles at the end can be read from it. */
+tdv_status tdv_batch_set_trace(tdv_batch* batch, unsigned long long* trace, int64_t capacity_items);
 /* The device work queue (n_items entries of item_bytes: int32 pair*16+pass,
  * int32 block), pass-major, and the per-pass item counts; for inspection and
  * for tests that plant faults in the queue. */

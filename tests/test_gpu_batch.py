@@ -97,6 +97,35 @@ def test_batch_small_pairs_match_oracle(ctx, orc):
     b.close()
 
 
+def test_batch_trace(ctx):
+    """The diagnostic trace: every queue item recorded once, taken before its
+    dependency was met and ended after it, with its own pair and pass; maps
+    unchanged with the trace on; runs after it record nothing."""
+    pairs = _pairs(SHAPES, seed=3)
+    ref = _per_pair(ctx, pairs)
+    b = _batch(ctx, pairs)
+    tr = b.trace().numpy()
+    _same(b.outputs, ref)
+    n = b.work_queue()[1]
+    assert tr.shape == (n, 4)
+    take, go, end = tr[:, 0], tr[:, 1], tr[:, 2]
+    assert (take > 0).all() and (go >= take).all() and (end >= go).all()
+    _, q = _queue(b)
+    pp = tr[:, 3] & 0xFFFFFFFF
+    np.testing.assert_array_equal(pp, q[:, 0])
+    # the first item of a pair's pass never starts before its pass's dependency ended
+    for pair in range(len(pairs)):
+        for ps in range(2, 9):
+            cur = (pp >> 4 == pair) & (pp & 15 == ps)
+            prev = (pp >> 4 == pair) & (pp & 15 == ps - 1)
+            if cur.any() and prev.any():
+                assert go[cur].min() >= end[prev].max() - 1000  # timer granularity
+    b.run()
+    b.status()
+    _same(b.outputs, ref)
+    b.close()
+
+
 def test_batch_graph_replay_video(ctx):
     """Graph replays read the inputs again: rewrite them between replays."""
     shapes = [(160, 96, 64, 1), (320, 48, 128, None), (80, 80, 256, 1)]

@@ -32,7 +32,7 @@ EXPORTS = [
     "tdv_stereo_sgm_static", "tdv_stereo_sgm_frames",
     "tdv_batch_create", "tdv_batch_destroy", "tdv_batch_set_tiles", "tdv_batch_get_tiles",
     "tdv_batch_autotune", "tdv_batch_run", "tdv_batch_graph_launch", "tdv_batch_status",
-    "tdv_batch_set_wait_limit", "tdv_batch_work_queue",
+    "tdv_batch_set_wait_limit", "tdv_batch_set_trace", "tdv_batch_work_queue",
     "tdv_to_gray", "tdv_rectify_maps", "tdv_remap", "tdv_prefilter", "tdv_postfilter", "tdv_subpixel", "tdv_reproject",
     "tdv_write_ply",
 ]
@@ -150,6 +150,7 @@ def _declare(lib):
         "tdv_batch_graph_launch": (st, [vp, vp]),
         "tdv_batch_status": (st, [vp, vp]),
         "tdv_batch_set_wait_limit": (st, [vp, ctypes.c_double]),
+        "tdv_batch_set_trace": (st, [vp, vp, ctypes.c_int64]),
         "tdv_batch_work_queue": (st, [vp, P(vp), P(ctypes.c_int32), P(ctypes.c_int32)]),
         "tdv_to_gray": (st, [vp, P(tdv_raster), vp, vp]),
         "tdv_rectify_maps": (st, [vp, vp, vp, vp, vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp]),

@@ -424,6 +424,21 @@ class Batch:
         self.ctx.check(L.lib().tdv_batch_run(self.handle, _stream()))
         return self.outputs
 
+    def trace(self):
+        """One run with the per-item trace on (tdv_batch_set_trace); returns
+        an (n_items, 4) int64 CPU tensor: global-timer ns when a block took
+        the item, when its dependency was met, when it ended, and
+        smid << 32 | (pair * 16 + pass)."""
+        n = self.work_queue()[1]
+        buf = torch.zeros((n, 4), dtype=torch.int64, device="cuda")
+        self.ctx.check(L.lib().tdv_batch_set_trace(self.handle, buf.data_ptr(), n))
+        try:
+            self.run()
+            self.status()
+        finally:
+            self.ctx.check(L.lib().tdv_batch_set_trace(self.handle, None, 0))
+        return buf.cpu()
+
     def graph_launch(self):
         """The same run replayed from a CUDA graph (captured on first use)."""
         self.ctx.check(L.lib().tdv_batch_graph_launch(self.handle, _stream()))

@@ -973,6 +973,7 @@ struct tdv_batch {
     cudaGraphExec_t gexec = nullptr;
     unsigned long long wait_ns = 2000000000ull;
     int grid = 0;
+    unsigned long long* trace = nullptr;  // caller's device buffer, 4 words per item, or null
 };
 
 namespace {
@@ -1027,7 +1028,7 @@ tdv_status batch_replan(tdv_batch* b, const tdv_batch_tiles& t) {
 tdv_status batch_launch_on(tdv_batch* b, cudaStream_t st) {
     tdv_ctx* ctx = b->ctx;
     TDV_CUDA(tdv::batch_configure(b->plan));
-    TDV_CUDA(tdv::batch_launch(b->plan, (unsigned char*)b->desc, b->wait_ns, b->grid, st));
+    TDV_CUDA(tdv::batch_launch(b->plan, (unsigned char*)b->desc, b->wait_ns, b->grid, st, b->trace));
     return TDV_OK;
 }
 
@@ -1159,7 +1160,8 @@ tdv_status tdv_batch_graph_launch(tdv_batch* b, tdv_stream stream) {
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            const cudaError_t el = tdv::batch_launch(b->plan, (unsigned char*)b->desc, b->wait_ns, b->grid, cs);
+            const cudaError_t el =
+                tdv::batch_launch(b->plan, (unsigned char*)b->desc, b->wait_ns, b->grid, cs, b->trace);
             e = cudaStreamEndCapture(cs, &g);
             if (el != cudaSuccess) e = el;
         }
@@ -1195,6 +1197,16 @@ tdv_status tdv_batch_set_wait_limit(tdv_batch* b, double seconds) {
     if (!(seconds >= 1e-3 && seconds <= 60.0))
         return fail(b->ctx, TDV_ERR_INVALID_ARG, "wait limit must be in [0.001, 60] s");
     b->wait_ns = (unsigned long long)(seconds * 1e9);
+    drop_graph(b);
+    return TDV_OK;
+}
+
+tdv_status tdv_batch_set_trace(tdv_batch* b, unsigned long long* trace, int64_t capacity_items) {
+    if (!b) return TDV_ERR_INVALID_ARG;
+    if (trace && capacity_items < b->plan.n_items)
+        return fail(b->ctx, TDV_ERR_INVALID_ARG, "trace holds %lld items, the queue %d", (long long)capacity_items,
+                    b->plan.n_items);
+    b->trace = trace;
     drop_graph(b);
     return TDV_OK;
 }

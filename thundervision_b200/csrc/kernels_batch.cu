@@ -112,10 +112,11 @@ __device__ __forceinline__ void run_h(const BPair& P, int dx, int blk, unsigned 
 template <int NW>
 __global__ void __launch_bounds__(NW * 32, NW == kBatchWarps ? 1 : 2)
     batch_kernel(const BPair* __restrict__ pairs, int npairs, const BItem* __restrict__ items, int nitems,
-                 int* ctl, unsigned long long wait_ns) {
+                 int* ctl, unsigned long long wait_ns, unsigned long long* trace) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ BPair sp;
-    __shared__ int s_pass, s_blk, s_stop, s_slot;
+    __shared__ int s_pass, s_blk, s_stop, s_slot, s_item, s_pp;
+    __shared__ unsigned long long s_take, s_go;
     int* head = ctl;
     int* err = ctl + 1;
     int* done = ctl + kCtlHeader;
@@ -125,8 +126,11 @@ __global__ void __launch_bounds__(NW * 32, NW == kBatchWarps ? 1 : 2)
             int stop = 1;
             if (ld_volatile(err) == 0) {
                 const int i = atomicAdd(head, 1);
+                s_item = i;
+                if (trace) s_take = global_ns();
                 if (i < nitems) {
                     const BItem it = items[i];
+                    s_pp = it.pp;
                     const unsigned pair = (unsigned)it.pp >> 4;
                     const int pass = it.pp & 15;
                     if (pair >= (unsigned)npairs || pass >= kPasses || it.blk < 0 ||
@@ -140,6 +144,7 @@ __global__ void __launch_bounds__(NW * 32, NW == kBatchWarps ? 1 : 2)
                             s_pass = pass;
                             s_blk = it.blk;
                             s_slot = pair * kPasses + pass;
+                            if (trace) s_go = global_ns();
                         }
                     }
                 }
@@ -179,6 +184,17 @@ __global__ void __launch_bounds__(NW * 32, NW == kBatchWarps ? 1 : 2)
             fence_proxy_async_global();
             __threadfence();
             atomicAdd(done + s_slot, 1);
+            if (trace) {
+                // diagnostic: when the item was taken, when its dependency was
+                // met, when it ended, the SM it ran on and its pair * 16 + pass
+                unsigned smid;
+                asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+                unsigned long long* t = trace + 4 * (size_t)s_item;
+                t[0] = s_take;
+                t[1] = s_go;
+                t[2] = global_ns();
+                t[3] = ((unsigned long long)smid << 32) | (unsigned)s_pp;
+            }
         }
     }
 }
@@ -359,7 +375,7 @@ cudaError_t batch_configure(const BatchPlan& plan) {
 }
 
 cudaError_t batch_launch(const BatchPlan& plan, unsigned char* d_desc, unsigned long long wait_ns, int grid,
-                         cudaStream_t st) {
+                         cudaStream_t st, unsigned long long* trace) {
     cudaError_t e = cudaMemsetAsync(d_desc + plan.ctl_off, 0, batch_ctl_bytes(plan.n_pairs), st);
     if (e != cudaSuccess) return e;
     const BPair* pairs = (const BPair*)(d_desc + plan.pairs_off);
@@ -367,10 +383,10 @@ cudaError_t batch_launch(const BatchPlan& plan, unsigned char* d_desc, unsigned 
     int* ctl = (int*)(d_desc + plan.ctl_off);
     if (plan.ctas_per_sm == 2)
         batch_kernel<kBatchWarps2><<<2 * grid, kBatchWarps2 * 32, plan.smem, st>>>(pairs, plan.n_pairs, items,
-                                                                                   plan.n_items, ctl, wait_ns);
+                                                                                   plan.n_items, ctl, wait_ns, trace);
     else
         batch_kernel<kBatchWarps><<<grid, kBatchWarps * 32, plan.smem, st>>>(pairs, plan.n_pairs, items,
-                                                                             plan.n_items, ctl, wait_ns);
+                                                                             plan.n_items, ctl, wait_ns, trace);
     return cudaGetLastError();
 }
 

@@ -336,8 +336,9 @@ const char* batch_plan(const std::vector<BatchPairArgs>& pairs, int p1h, int p2h
 cudaError_t batch_configure(const BatchPlan& plan);
 // Zeroes the control words and launches the persistent kernel (grid blocks);
 // batch_configure must have run for a plan of at least this shared memory.
+// trace: null, or 4 words per queue item (taken, dependency met, ended, smid << 32 | pair * 16 + pass)
 cudaError_t batch_launch(const BatchPlan& plan, unsigned char* d_desc, unsigned long long wait_ns, int grid,
-                         cudaStream_t st);
+                         cudaStream_t st, unsigned long long* trace = nullptr);
 
 // Differentiable soft-argmin SGM (kernels_soft.cu).
 struct SoftLaunch {
