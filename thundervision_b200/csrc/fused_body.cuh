@@ -731,8 +731,8 @@ __device__ __forceinline__ void vd_body(const FK& k, int s, int dy, int kmin, in
 //     once the loads have passed it, the producer refills the slot with the
 //     chunk 4 places further in walk order.
 // The producer lanes never block: each polls its own row's empty barriers and
-// issues what has become free; the warp sleeps briefly when no lane could
-// issue and gives up (TDV_ERR_TIMEOUT) after kWaitNs without progress.
+// issues what has become free; the warp pauses 256 ns after every round and
+// gives up (TDV_ERR_TIMEOUT) after kWaitNs without progress.
 // The recurrence starts from L = 0, m = 0, which makes the first step L = C
 // without a branch (min(0, 0 + P1, 0 + P2) = 0).
 // TWO: the pass joins two volumes filled by concurrent pass chains, k.S and
@@ -890,8 +890,13 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                     failed = true;
                     break;
                 }
-                __nanosleep(64);
             }
+            // a pause after every round, work or not: with every row releasing a
+            // slot each few hundred ns a busy producer would otherwise poll
+            // without rest, taking issue slots from the two consumer warps of
+            // its SM sub-partition (a slot's refill still lands well before the
+            // slot is needed again)
+            __nanosleep(256);
         }
         // the block must not retire with copies in flight
         if (mine) {
