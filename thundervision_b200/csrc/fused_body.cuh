@@ -1063,6 +1063,12 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                     // a border cell a later walk restarts: the offset alone
 #pragma unroll
                     for (int q = 0; q < PPL; q++) sv[q] += k.OFFOFF;
+                } else if (WTD && !SPEC && (rflags & 1u)) {
+                    // a row that counts nowhere walked by the clean or masked
+                    // step (cheaper than the special one): its path costs are
+                    // computed and dropped, the offset alone is added
+#pragma unroll
+                    for (int q = 0; q < PPL; q++) sv[q] += k.OFFOFF;
                 } else {
 #pragma unroll
                     for (int q = 0; q < PPL; q++) sv[q] += Ln[q];
@@ -1143,7 +1149,7 @@ __device__ __forceinline__ void hp_body(const FK& k, int dx, int R, int blk, uns
                 const unsigned char* slot = wbase + s * SLOT;
                 const int xlo = group_lo(j), xhi = group_hi(j), n = xhi - xlo + 1;
                 const int cxa = (int)(cxs & 0xFFFFu), cxb = (int)(cxs >> 16);
-                const bool special = WTD && ((rflags & 5u) || ((rflags & 2u) && (xlo == 0 || xhi >= W - 1)) ||
+                const bool special = WTD && ((rflags & 4u) || ((rflags & 2u) && (xlo == 0 || xhi >= W - 1)) ||
                                              (cxa >= xlo && cxa <= xhi) || (cxb >= xlo && cxb <= xhi) ||
                                              (k.GSTART && j == 0));
                 if (special) {
