@@ -257,7 +257,7 @@ def _rows_for(seconds_per_step, sem, threads, lo=16):
     return int(max(lo, min(H, seconds_per_step / (t / lo))))
 
 
-def cpu_reference_run(steps, warmup, sem, budget_s=150.0):
+def cpu_reference_run(steps, warmup, sem, budget_s=60.0):
     """Times the restatement on bands of a full-HD frame on every host thread;
     returns (frames/s, seconds per step, rows, threads, description)."""
     threads = os.cpu_count() or 1
